@@ -1,0 +1,321 @@
+#!/usr/bin/env python3
+"""Headline benchmark: exact triangle count of the 34.7M-edge power-law (R-MAT scale 22) graph on one B200.
+
+Workload (seeded synthetic stand-in for the reference's com-LiveJournal measurement, same edge count): R-MAT
+scale 22, (a,b,c,d) = (.57,.19,.19,.05), 8.52 * 2^22 samples symmetrised with self loops and duplicates removed
+(about 34.7M undirected edges), ids permuted from the seed, oriented by (degree, id) into CSR like the reference's
+graph.h. One step = one triangle count of the whole graph with the CSR and its derived index resident in HBM.
+
+Reported (one JSON line, rank 0):
+  value        algorithmic GB/s = B_alg / kernel time, B_alg = 4(n+1) + 8m + 4 * sum over oriented edges (u,v) of
+               (d+(u) + d+(v)) (the bytes a two-list merge streams), whole job over all ranks;
+  e2e          the same metric through the public C ABI from pinned host buffers: ga_graph_create (H2D copy and
+               validation), ga_graph_prepare, ga_tc_count (8-byte D2H) and ga_graph_destroy, every step;
+  roofline     B_alg per launch / CUDA-event launch time vs the measured HBM copy bandwidth;
+  cpu_baseline the reference's own cpu_triangles_omp (oracle/_ref, compiled from its sources) on the host cores.
+``--impl reference`` times the reference's CPU implementation alone with the same metric.
+Multi-GPU (torchrun, one rank per GPU): replicas only - every rank counts its own copy of the graph, no collective
+on the data path; the max over ranks of the device time gives the whole-job value (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "TC ms & GB/s (% HBM peak), 35M-edge power-law; batched vs plain graphs/s, p99"
+SCALE, EDGE_FACTOR, SEED = 22, 8.52, 1
+RMAT = (0.57, 0.19, 0.19)
+L2_FLUSH_BYTES = 256 << 20
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_graph(ga, scale=SCALE, ef=EDGE_FACTOR, seed=SEED):
+    t0 = time.time()
+    pairs = ga.gen_rmat(scale, int(ef * (1 << scale)), *RMAT, seed=seed)
+    g = ga.graph_from_pairs(1 << scale, pairs)
+    log(f"graph: R-MAT scale {scale} ef {ef} seed {seed}: n={g.n} m={g.m} max_out_degree={g.max_out_degree} "
+        f"({time.time() - t0:.1f} s on the host)")
+    return g
+
+
+def algorithmic_bytes(g) -> int:
+    """B_alg = 4(n+1) + 8m + 4 * sum_{(u,v)} (d+(u) + d+(v))."""
+    d = np.diff(g.rowptr.astype(np.int64))
+    s_u = int((d * d).sum())                              # sum over edges of d+(src) = sum_u d+(u)^2
+    s_v = int(d[g.col.astype(np.int64)].sum())            # sum over edges of d+(dst)
+    return 4 * (g.n + 1) + 8 * g.m + 4 * (s_u + s_v)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self) -> dict:
+        rows = []
+        for line in (getattr(self, "out", "") or "").splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def read_peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return {"hbm_gbs": float(p["hbm_gbs"]), "source": "measured"}
+    except (OSError, KeyError, ValueError):
+        return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def read_traffic(workload: str):
+    """DRAM bytes per launch of the count kernel from the committed ncu summary (None if absent)."""
+    path = os.path.join(ROOT, "profiles", f"tc_hash_{workload}.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch:"):
+                return int(float(line.split(":", 1)[1].strip()))
+    except OSError:
+        pass
+    return None
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        return dist, world, rank, local
+    return None, 1, 0, 0
+
+
+def cpu_reference_baseline(g, b_alg: int, steps: int = 1) -> dict:
+    """The reference's cpu_triangles_omp (oracle/_ref) with all host threads, full graph, best of `steps`."""
+    from oracle import Reference
+    ref = Reference()
+    best = None
+    T = None
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        T = ref.triangles_omp(g)
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    return {"value": b_alg / best / 1e9, "unit": "GB/s", "cores": ref.num_threads(), "kind": "reference",
+            "sample": f"whole graph, cpu_triangles_omp (graph.h:123) best of {steps}, {best * 1e3:.1f} ms, "
+                      f"T={T}", "ms": best * 1e3, "triangles": T}
+
+
+def run_reference_arm(args):
+    """--impl reference: the reference's own CPU implementation, same metric and config, on rank 0 only."""
+    dist, world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return 0
+    import graph_analyzer_b200 as ga
+    from oracle import Reference
+    ref = Reference()
+    g = make_graph(ga)
+    b_alg = algorithmic_bytes(g)
+    for _ in range(args.warmup):
+        ref.triangles_omp(g)
+    times = []
+    T = None
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        T = ref.triangles_omp(g)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * sum(times) / len(times)
+    value = b_alg / (ms / 1e3) / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"rmat{SCALE}_tc", "n": g.n, "m": g.m, "edge_factor": EDGE_FACTOR, "seed": SEED,
+                   "triangles": T, "b_alg_bytes": b_alg, "parallelism": "host threads (OpenMP)"},
+        "cpu_baseline": {"value": value, "unit": "GB/s", "cores": ref.num_threads(), "kind": "reference",
+                         "sample": f"whole graph per step, cpu_triangles_omp (graph.h:123), {args.steps} steps"},
+        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    dist, world, rank, local = dist_setup(args)
+    import torch
+    import graph_analyzer_b200 as ga
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    g = make_graph(ga)
+    b_alg = algorithmic_bytes(g)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+    d_out = torch.zeros(1, dtype=torch.int64, device=dev)
+
+    # ---- device-resident: one count per step on the prepared, resident graph ----
+    dg = ga.DeviceGraph(g, device=local, stream=stream.cuda_stream)
+    t0 = time.perf_counter()
+    dg.prepare()
+    torch.cuda.synchronize(dev)
+    prep_ms = (time.perf_counter() - t0) * 1e3
+    T = dg.tc_count()
+    for _ in range(args.warmup):
+        dg.tc_count_async(d_out.data_ptr())
+    torch.cuda.synchronize(dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        for s in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()                                   # L2 flush between steps (not timed)
+            evs[s][0].record(stream)
+            dg.tc_count_async(d_out.data_ptr())
+            evs[s][1].record(stream)
+        torch.cuda.synchronize(dev)
+        time.sleep(0.25)
+    if dist:
+        dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    if int(d_out.item()) != T:
+        raise RuntimeError(f"count changed between launches: {d_out.item()} vs {T}")
+    ms = sum(step_ms) / len(step_ms)
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * b_alg / (ms / 1e3) / 1e9
+
+    # ---- end to end through the public API from pinned host memory ----
+    rp_h = torch.from_numpy(g.rowptr.view(np.int32)).pin_memory()
+    col_h = torch.from_numpy(g.col.view(np.int32)).pin_memory()
+    e2e_times = []
+    for s in range(args.warmup + args.steps):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        h = ga.lib()
+        import ctypes as C
+        hd = C.c_void_p()
+        ga._check(h.ga_graph_create(rp_h.data_ptr(), col_h.data_ptr(), g.n, g.m, local, stream.cuda_stream,
+                                    C.byref(hd)))
+        ga._check(h.ga_graph_prepare(hd))
+        out = C.c_uint64(0)
+        ga._check(h.ga_tc_count(hd, C.byref(out)))
+        ga._check(h.ga_graph_destroy(hd))
+        dt = time.perf_counter() - t0
+        if out.value != T:
+            raise RuntimeError("end-to-end count differs")
+        if s >= args.warmup:
+            e2e_times.append(dt)
+    e2e_ms = 1e3 * sum(e2e_times) / len(e2e_times)
+    if dist:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * b_alg / (e2e_ms / 1e3) / 1e9
+
+    if rank != 0:
+        dg.close()
+        if dist:
+            dist.destroy_process_group()
+        return 0
+    peaks = read_peaks()
+    achieved = b_alg / (ms / 1e3) / 1e9
+    cpu = cpu_reference_baseline(g, b_alg) if world == 1 and not args.no_cpu else None
+    if cpu and cpu["triangles"] != T:
+        raise RuntimeError(f"GPU count {T} differs from the reference CPU count {cpu['triangles']}")
+    line = {
+        "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"rmat{SCALE}_tc", "n": g.n, "m": g.m, "edge_factor": EDGE_FACTOR, "seed": SEED,
+                   "rmat_abc": list(RMAT), "triangles": T, "b_alg_bytes": b_alg, "prep_ms": prep_ms,
+                   "l2": "256 MiB written between steps (untimed); col alone (139 MB) exceeds L2",
+                   "parallelism": f"replicas x{world}", "oriented_edges_per_s": world * g.m / (ms / 1e3)},
+        "e2e": {"value": e2e_value, "unit": "GB/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(rp_h.numel() * 4 + col_h.numel() * 4), "d2h_bytes_per_step": 8,
+                "path": "ga_graph_create + ga_graph_prepare + ga_tc_count + ga_graph_destroy"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": read_traffic(f"rmat{SCALE}"),
+                     "peak_source": peaks["source"], "kernel": "k_tc_hash<COUNT>"},
+        "cpu_baseline": ({k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")} if cpu else None),
+        "clocks": clk.summary(),
+        "gpu_launches": args.steps,
+    }
+    print(json.dumps(line), flush=True)
+    dg.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        log("warm-up raised to 3 steps")
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,440 @@
+"""graph_analyzer_b200 - the triangle path of graph_analyzer on one B200 (sm_100a), Python host layer.
+
+A thin ctypes layer over ``libga_b200.so`` (the C ABI declared in include/graph_analyzer_b200.h). Names follow the
+reference's C++ surface (VijayPraneethSai/graph_analyzer, paths relative to that project):
+
+=====================================  ==========================================================================
+reference                              here
+=====================================  ==========================================================================
+``struct Graph`` (graph.h:19-26)        :class:`Graph`
+``build_graph_from_edges`` (graph.h:38) :func:`build_graph_from_edges`
+``load_graph`` (graph.h:71)             :func:`load_graph`
+``PeelResult`` (densest.h:46-59)        :class:`PeelResult` (``==`` compares like ``operator==``)
+``density_value`` / ``peel_arith_ok``   :func:`density_value`, :func:`peel_arith_ok`, :func:`peel_improves`
+ / ``peel_improves`` (densest.h:62-78)
+count kernels driven by gpu_tc.cu       :meth:`DeviceGraph.tc_count` / :func:`gpu_triangles`
+``tc_per_vertex_alive`` (kernels.cuh)   :meth:`DeviceGraph.participation`
+``triangle_degrees`` (dsg.h:82)         :meth:`DeviceGraph.support_vertices`
+``for_each_triangle`` (dsg.h:67)        :meth:`DeviceGraph.support_edges` (per-edge support)
+``batch_peel_loop`` (densest.h:279)     :meth:`DeviceGraph.batch_peel` / :func:`gpu_batch_peel`
+``core_decomp_loop_inc`` (dsg.h:724)    :meth:`DeviceGraph.core_decomposition` / :func:`gpu_core_decomposition`
+=====================================  ==========================================================================
+
+There is no CPU fallback: every count comes from the CUDA library, and a missing library or device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+__all__ = [
+    "GAError", "Graph", "PeelResult", "CoreResult", "DeviceGraph", "build_graph_from_edges", "load_graph",
+    "canonical_edges", "gen_holme_kim", "gen_rmat", "permute_ids", "density_value", "peel_arith_ok",
+    "peel_improves", "gpu_triangles", "gpu_batch_peel", "gpu_core_decomposition", "lib", "device_count",
+    "OPT_TC_KERNEL", "OPT_LOOP_MODE", "OPT_MAX_ROUNDS", "OPT_ITEM_WORK", "OPT_HEAVY_TABLE_BITS",
+    "OPT_LIGHT_MAX_DEG",
+]
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "_lib", "libga_b200.so")
+
+OPT_TC_KERNEL, OPT_LOOP_MODE, OPT_MAX_ROUNDS, OPT_ITEM_WORK, OPT_HEAVY_TABLE_BITS, OPT_LIGHT_MAX_DEG = 1, 2, 3, 4, 5, 6
+
+STATUS = {
+    0: "GA_OK", 1: "GA_ERR_INVALID_ARGUMENT", 2: "GA_ERR_INVALID_GRAPH", 3: "GA_ERR_CUDA",
+    4: "GA_ERR_OUT_OF_MEMORY", 5: "GA_ERR_ARITH", 6: "GA_ERR_ROUND_LIMIT", 7: "GA_ERR_IO", 8: "GA_ERR_NO_DEVICE",
+    9: "GA_ERR_DEVICE_CHECK", 10: "GA_ERR_BUDGET", 11: "GA_ERR_CAPACITY", 12: "GA_ERR_NOT_READY",
+}
+
+
+class GAError(RuntimeError):
+    """A ga_status other than GA_OK; ``.status`` is the code, ``.name`` its symbol."""
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        self.name = STATUS.get(status, f"status {status}")
+        super().__init__(f"{self.name}: {message}")
+
+
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+_vp = C.c_void_p
+
+
+class _HostGraph(C.Structure):
+    _fields_ = [("n", C.c_uint32), ("m", C.c_uint32), ("max_out_degree", C.c_uint32),
+                ("rowptr", C.POINTER(C.c_uint32)), ("col", C.POINTER(C.c_uint32)), ("src", C.POINTER(C.c_uint32))]
+
+
+class _PeelRes(C.Structure):
+    _fields_ = [("best_num", C.c_uint64), ("best_den", C.c_uint64), ("best_round", C.c_uint32),
+                ("rounds", C.c_uint32)]
+
+
+class _CoreRes(C.Structure):
+    _fields_ = [("kmax", C.c_uint32), ("rounds", C.c_uint32)]
+
+
+# (name, argtypes) of every exported entry point; the library must export all of them.
+SIGNATURES: dict[str, list] = {
+    "ga_status_string": [C.c_int],
+    "ga_last_error": [],
+    "ga_device_count": [C.POINTER(C.c_int)],
+    "ga_canonical_edges": [_u32p, C.c_uint64, C.POINTER(C.c_uint64)],
+    "ga_build_graph_from_edges": [C.c_uint32, _u32p, C.c_uint32, _u32p, _u32p, _u32p, C.POINTER(C.c_uint32)],
+    "ga_host_graph_from_edges": [C.c_uint32, _u32p, C.c_uint64, C.c_int, C.POINTER(C.POINTER(_HostGraph))],
+    "ga_load_graph": [C.c_char_p, C.POINTER(C.POINTER(_HostGraph))],
+    "ga_host_graph_free": [C.POINTER(_HostGraph)],
+    "ga_gen_holme_kim": [C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_uint64, _u32p, C.c_uint64,
+                         C.POINTER(C.c_uint64)],
+    "ga_gen_rmat": [C.c_uint32, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_uint64, _u32p],
+    "ga_permute_ids": [_u32p, C.c_uint64, C.c_uint32, C.c_uint64],
+    "ga_graph_create": [_vp, _vp, C.c_uint32, C.c_uint32, C.c_int, _vp, C.POINTER(_vp)],
+    "ga_graph_create_device": [_vp, _vp, C.c_uint32, C.c_uint32, C.c_int, _vp, C.POINTER(_vp)],
+    "ga_graph_destroy": [_vp],
+    "ga_graph_set_stream": [_vp, _vp],
+    "ga_graph_device_bytes": [_vp, C.POINTER(C.c_uint64)],
+    "ga_graph_prepare": [_vp],
+    "ga_graph_set_option": [_vp, C.c_int, C.c_int64],
+    "ga_tc_count": [_vp, C.POINTER(C.c_uint64)],
+    "ga_tc_count_async": [_vp, _vp],
+    "ga_tc_support_edges": [_vp, _vp, C.POINTER(C.c_uint64)],
+    "ga_tc_support_edges_device": [_vp, _vp, C.POINTER(C.c_uint64)],
+    "ga_tc_support_vertices": [_vp, _vp, C.POINTER(C.c_uint64)],
+    "ga_tc_participation": [_vp, _vp, _vp, C.POINTER(C.c_uint64)],
+    "ga_batch_peel": [_vp, C.c_uint64, C.c_uint64, C.POINTER(_PeelRes), _vp],
+    "ga_core_decomposition": [_vp, _vp, C.POINTER(_CoreRes)],
+}
+_RESTYPE = {"ga_status_string": C.c_char_p, "ga_last_error": C.c_char_p, "ga_host_graph_free": None}
+
+_lib: C.CDLL | None = None
+
+
+def lib() -> C.CDLL:
+    """Loads libga_b200.so (built by ``python -m graph_analyzer_b200.build``); raises if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built: run `python -m graph_analyzer_b200.build` "
+                              "(the CUDA library is required; there is no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = _RESTYPE.get(name, C.c_int)
+        _lib = L
+    return _lib
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        raise GAError(status, lib().ga_last_error().decode(errors="replace"))
+
+
+def device_count() -> int:
+    c = C.c_int(0)
+    _check(lib().ga_device_count(C.byref(c)))
+    return c.value
+
+
+def _ptr(a: np.ndarray | None) -> int | None:
+    return None if a is None else a.ctypes.data
+
+
+# ------------------------------------------------------------------------------------------------------------------
+# graph.h surface
+# ------------------------------------------------------------------------------------------------------------------
+
+@dataclass
+class Graph:
+    """Oriented CSR, the fields of the reference's ``struct Graph`` (graph.h:19-26)."""
+
+    n: int
+    m: int
+    rowptr: np.ndarray            # uint32[n+1]
+    col: np.ndarray               # uint32[m], rows sorted
+    src: np.ndarray               # uint32[m]
+    max_out_degree: int
+
+    def __eq__(self, other) -> bool:
+        return (isinstance(other, Graph) and self.n == other.n and self.m == other.m
+                and self.max_out_degree == other.max_out_degree and np.array_equal(self.rowptr, other.rowptr)
+                and np.array_equal(self.col, other.col) and np.array_equal(self.src, other.src))
+
+
+def canonical_edges(pairs: np.ndarray) -> np.ndarray:
+    """load_graph's clean-up (graph.h:85-92): self loops dropped, (min,max), sorted, unique. Returns (k,2) uint32."""
+    p = np.ascontiguousarray(pairs, dtype=np.uint32).reshape(-1).copy()
+    if p.size == 0:
+        return p.reshape(0, 2)
+    k = C.c_uint64(0)
+    _check(lib().ga_canonical_edges(p, p.size // 2, C.byref(k)))
+    return p[: 2 * k.value].reshape(-1, 2)
+
+
+def build_graph_from_edges(n: int, edges: np.ndarray) -> Graph:
+    """build_graph_from_edges (graph.h:38-67): unique undirected pairs without self loops -> oriented CSR."""
+    p = np.ascontiguousarray(edges, dtype=np.uint32).reshape(-1)
+    m = p.size // 2
+    rowptr = np.zeros(n + 1, np.uint32)
+    col = np.zeros(max(m, 1), np.uint32)
+    src = np.zeros(max(m, 1), np.uint32)
+    mx = C.c_uint32(0)
+    _check(lib().ga_build_graph_from_edges(n, p if m else np.zeros(2, np.uint32), m, rowptr, col, src,
+                                           C.byref(mx)))
+    return Graph(n, m, rowptr, col[:m].copy(), src[:m].copy(), mx.value)
+
+
+def _from_host_graph(hg) -> Graph:
+    h = hg.contents
+    n, m = h.n, h.m
+    rowptr = np.ctypeslib.as_array(h.rowptr, shape=(n + 1,)).copy()
+    col = np.ctypeslib.as_array(h.col, shape=(max(m, 1),))[:m].copy()
+    src = np.ctypeslib.as_array(h.src, shape=(max(m, 1),))[:m].copy()
+    g = Graph(n, m, rowptr, col, src, h.max_out_degree)
+    lib().ga_host_graph_free(hg)
+    return g
+
+
+def load_graph(path: str) -> Graph:
+    """load_graph (graph.h:71-96): SNAP text edge list -> cleaned, oriented CSR with n = max_id + 1."""
+    hg = C.POINTER(_HostGraph)()
+    _check(lib().ga_load_graph(os.fsencode(path), C.byref(hg)))
+    return _from_host_graph(hg)
+
+
+def graph_from_pairs(n: int, pairs: np.ndarray, canonicalize: bool = True) -> Graph:
+    """Cleans (optionally) and orients an arbitrary undirected pair list on vertices 0..n-1."""
+    p = np.ascontiguousarray(pairs, dtype=np.uint32).reshape(-1)
+    hg = C.POINTER(_HostGraph)()
+    _check(lib().ga_host_graph_from_edges(n, p if p.size else np.zeros(2, np.uint32), p.size // 2,
+                                          int(canonicalize), C.byref(hg)))
+    return _from_host_graph(hg)
+
+
+# ------------------------------------------------------------------------------------------------------------------
+# synthetic inputs
+# ------------------------------------------------------------------------------------------------------------------
+
+def gen_holme_kim(n: int, m_lo: int, m_hi: int | None = None, p_hi: float = 0.0, triad_p: float = 0.5,
+                  seed: int = 1, permute: bool = True) -> np.ndarray:
+    """Holme-Kim pairs (unique, no self loops), ids permuted from the seed. m_v = m_hi w.p. p_hi, else m_lo."""
+    m_hi = m_lo if m_hi is None else m_hi
+    cap = n * m_hi
+    out = np.zeros(2 * max(cap, 1), np.uint32)
+    k = C.c_uint64(0)
+    _check(lib().ga_gen_holme_kim(n, m_lo, m_hi, p_hi, triad_p, seed, out, cap, C.byref(k)))
+    pairs = out[: 2 * k.value]
+    if permute:
+        _check(lib().ga_permute_ids(pairs, k.value, n, seed))
+    return pairs.reshape(-1, 2)
+
+
+def gen_rmat(scale: int, nsamples: int, a: float = 0.57, b: float = 0.19, c: float = 0.19, seed: int = 1,
+             permute: bool = True) -> np.ndarray:
+    """Raw R-MAT samples on 2^scale vertices (clean with canonical_edges), ids permuted from the seed."""
+    out = np.zeros(2 * max(nsamples, 1), np.uint32)
+    _check(lib().ga_gen_rmat(scale, nsamples, a, b, c, seed, out))
+    pairs = out[: 2 * nsamples]
+    if permute:
+        _check(lib().ga_permute_ids(pairs, nsamples, 1 << scale, seed))
+    return pairs.reshape(-1, 2)
+
+
+def permute_ids(pairs: np.ndarray, n: int, seed: int) -> np.ndarray:
+    p = np.ascontiguousarray(pairs, dtype=np.uint32).reshape(-1).copy()
+    _check(lib().ga_permute_ids(p, p.size // 2, n, seed))
+    return p.reshape(-1, 2)
+
+
+# ------------------------------------------------------------------------------------------------------------------
+# densest.h helpers (integer arithmetic only; densest.h:62-78)
+# ------------------------------------------------------------------------------------------------------------------
+
+U64 = (1 << 64) - 1
+
+
+def density_value(num: int, den: int) -> float:
+    """Display value only (densest.h:62)."""
+    return float(num) / float(den) if den else 0.0
+
+
+def peel_arith_ok(n: int, T0: int, num: int, den: int) -> tuple[bool, str]:
+    """peel_arith_ok (densest.h:65-72); returns (ok, why)."""
+    if den < 1 or den > (1 << 20) or num > (1 << 20):
+        return False, "eps = num/den needs 1 <= den <= 2^20 and num <= 2^20"
+    if T0 >= (1 << 32):
+        return False, "triangle count >= 2^32: uint32 tri[] counters could overflow"
+    if n > 0 and T0 > U64 // (n * den):
+        return False, "tri*nalive*den could overflow uint64"
+    if T0 > U64 // (3 * (den + num)):
+        return False, "3*(den+num)*T could overflow uint64"
+    return True, ""
+
+
+def peel_improves(T: int, nalive: int, best_num: int, best_den: int) -> bool:
+    """peel_improves (densest.h:76-78): strict improvement; ties keep the earlier, larger set."""
+    return best_den == 0 or T * best_den > best_num * nalive
+
+
+@dataclass
+class PeelResult:
+    """PeelResult (densest.h:46-54); equality as operator== (densest.h:56-59)."""
+
+    best_num: int = 0
+    best_den: int = 0
+    best_round: int = 0
+    rounds: int = 0
+    removed_round: np.ndarray = field(default_factory=lambda: np.zeros(0, np.uint32))
+    ok: bool = True
+    error: str = ""
+
+    def __eq__(self, o) -> bool:
+        return (self.best_num == o.best_num and self.best_den == o.best_den and self.best_round == o.best_round
+                and self.rounds == o.rounds and np.array_equal(self.removed_round, o.removed_round))
+
+    def density(self) -> float:
+        return density_value(self.best_num, self.best_den)
+
+    def peeled_set(self) -> np.ndarray:
+        """{v : removed_round[v] >= best_round} (densest.h:13-14)."""
+        return np.nonzero(self.removed_round >= self.best_round)[0].astype(np.uint32)
+
+
+@dataclass
+class CoreResult:
+    """Core numbers plus the CoreLoopResult fields (dsg.h:687-691)."""
+
+    core: np.ndarray
+    kmax: int
+    rounds: int
+
+
+# ------------------------------------------------------------------------------------------------------------------
+# device-resident graph
+# ------------------------------------------------------------------------------------------------------------------
+
+class DeviceGraph:
+    """A graph resident on one GPU (ga_graph). Use as a context manager or call close()."""
+
+    def __init__(self, g: Graph, device: int = 0, stream: int | None = None):
+        self.n, self.m = g.n, g.m
+        h = _vp()
+        rowptr = np.ascontiguousarray(g.rowptr, np.uint32)
+        col = np.ascontiguousarray(g.col if g.m else np.zeros(1, np.uint32), np.uint32)
+        _check(lib().ga_graph_create(_ptr(rowptr), _ptr(col), g.n, g.m, device, stream, C.byref(h)))
+        self._h = h
+
+    @classmethod
+    def from_device(cls, d_rowptr: int, d_col: int, n: int, m: int, device: int = 0, stream: int | None = None):
+        self = cls.__new__(cls)
+        self.n, self.m = n, m
+        h = _vp()
+        _check(lib().ga_graph_create_device(d_rowptr, d_col, n, m, device, stream, C.byref(h)))
+        self._h = h
+        return self
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().ga_graph_destroy(self._h)
+            self._h = _vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_option(self, opt: int, value: int) -> None:
+        _check(lib().ga_graph_set_option(self._h, opt, value))
+
+    def set_stream(self, stream: int | None) -> None:
+        _check(lib().ga_graph_set_stream(self._h, stream))
+
+    def prepare(self) -> None:
+        _check(lib().ga_graph_prepare(self._h))
+
+    def device_bytes(self) -> int:
+        b = C.c_uint64(0)
+        _check(lib().ga_graph_device_bytes(self._h, C.byref(b)))
+        return b.value
+
+    def tc_count(self) -> int:
+        t = C.c_uint64(0)
+        _check(lib().ga_tc_count(self._h, C.byref(t)))
+        return t.value
+
+    def tc_count_async(self, d_out: int) -> None:
+        """Enqueues the count on the graph's stream; the result lands in 8 bytes of device memory at d_out."""
+        _check(lib().ga_tc_count_async(self._h, d_out))
+
+    def support_edges(self) -> tuple[int, np.ndarray]:
+        sup = np.zeros(max(self.m, 1), np.uint32)
+        t = C.c_uint64(0)
+        _check(lib().ga_tc_support_edges(self._h, _ptr(sup), C.byref(t)))
+        return t.value, sup[: self.m]
+
+    def support_edges_device(self, d_sup: int) -> int:
+        t = C.c_uint64(0)
+        _check(lib().ga_tc_support_edges_device(self._h, d_sup, C.byref(t)))
+        return t.value
+
+    def support_vertices(self) -> tuple[int, np.ndarray]:
+        deg = np.zeros(max(self.n, 1), np.uint64)
+        t = C.c_uint64(0)
+        _check(lib().ga_tc_support_vertices(self._h, _ptr(deg), C.byref(t)))
+        return t.value, deg[: self.n]
+
+    def participation(self, alive: np.ndarray) -> tuple[int, np.ndarray]:
+        a = np.ascontiguousarray(alive, np.uint8)
+        if a.size != self.n:
+            raise ValueError("alive must have n entries")
+        tri = np.zeros(max(self.n, 1), np.uint32)
+        t = C.c_uint64(0)
+        _check(lib().ga_tc_participation(self._h, _ptr(a if self.n else np.zeros(1, np.uint8)), _ptr(tri),
+                                         C.byref(t)))
+        return t.value, tri[: self.n]
+
+    def batch_peel(self, num: int = 1, den: int = 10, want_removed: bool = True) -> PeelResult:
+        r = _PeelRes()
+        rr = np.full(max(self.n, 1), 0xFFFFFFFF, np.uint32) if want_removed else None
+        _check(lib().ga_batch_peel(self._h, num, den, C.byref(r), _ptr(rr)))
+        return PeelResult(r.best_num, r.best_den, r.best_round, r.rounds,
+                          rr[: self.n] if rr is not None else np.zeros(0, np.uint32))
+
+    def core_decomposition(self, want_core: bool = True) -> CoreResult:
+        r = _CoreRes()
+        core = np.zeros(max(self.n, 1), np.uint32) if want_core else None
+        _check(lib().ga_core_decomposition(self._h, _ptr(core), C.byref(r)))
+        return CoreResult(core[: self.n] if core is not None else np.zeros(0, np.uint32), r.kmax, r.rounds)
+
+
+# one-shot helpers with the reference driver's semantics (upload, run, download)
+
+def gpu_triangles(g: Graph, device: int = 0) -> int:
+    with DeviceGraph(g, device) as d:
+        return d.tc_count()
+
+
+def gpu_batch_peel(g: Graph, num: int = 1, den: int = 10, device: int = 0) -> PeelResult:
+    with DeviceGraph(g, device) as d:
+        return d.batch_peel(num, den)
+
+
+def gpu_core_decomposition(g: Graph, device: int = 0) -> CoreResult:
+    with DeviceGraph(g, device) as d:
+        return d.core_decomposition()

@@ -1,0 +1,153 @@
+// ga_device.cuh - device helpers and the ga_graph handle shared by the CUDA translation units of libga_b200.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "ga_internal.h"
+
+#define GA_FULL_MASK 0xFFFFFFFFu
+#define GA_EMPTY 0xFFFFFFFFu
+
+// Returns GA_ERR_CUDA / GA_ERR_OUT_OF_MEMORY with the failing call's text when a CUDA call fails.
+#define GA_CUDA(call)                                                                                          \
+    do {                                                                                                       \
+        cudaError_t e_ = (call);                                                                               \
+        if (e_ != cudaSuccess) {                                                                               \
+            return ::ga::fail(e_ == cudaErrorMemoryAllocation ? GA_ERR_OUT_OF_MEMORY : GA_ERR_CUDA,            \
+                              "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);     \
+        }                                                                                                      \
+    } while (0)
+
+#define GA_TRY(expr)                         \
+    do {                                     \
+        ga_status s_ = (expr);               \
+        if (s_ != GA_OK) return s_;          \
+    } while (0)
+
+namespace ga {
+
+constexpr int kSmCountB200 = 148;
+
+// ---- warp-level helpers --------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, uint32_t lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(GA_FULL_MASK, x, o);
+        if (lane >= (uint32_t)o) x += t;
+    }
+    return x;
+}
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(GA_FULL_MASK, x, o);
+    return x;
+}
+
+// Multiplicative hash onto `bits` bits (Knuth): the high bits of x * 2654435761 mod 2^32.
+__device__ __forceinline__ uint32_t hash_slot(uint32_t x, uint32_t bits) {
+    return (x * 2654435761u) >> (32 - bits);
+}
+
+// First index in sorted a[lo, hi) whose value is >= x.
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* __restrict__ a, uint32_t lo, uint32_t hi,
+                                                    uint32_t x) {
+    while (lo < hi) {
+        const uint32_t mid = lo + ((hi - lo) >> 1);
+        if (a[mid] < x) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// ---- grid sizing ------------------------------------------------------------------------------------------------
+inline unsigned grid_for(uint64_t threads, int block, unsigned cap = 148u * 64u) {
+    uint64_t b = (threads + block - 1) / block;
+    if (b < 1) b = 1;
+    if (b > cap) b = cap;
+    return (unsigned)b;
+}
+
+}  // namespace ga
+
+struct ga_loops;   // round-loop state (ga_loops.cu)
+
+// Work list of one kernel bin: item i covers in-edges [k0[i], k1[i]) of anchor v[i].
+struct ga_items {
+    uint32_t count = 0;
+    uint32_t* v = nullptr;
+    uint32_t* k0 = nullptr;
+    uint32_t* k1 = nullptr;
+    uint32_t max_dv = 0;      // largest anchor out-degree in the bin
+};
+
+struct ga_graph {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    uint32_t n = 0, m = 0, max_out_degree = 0;
+
+    // oriented CSR, the reference's layout (graph.h:19-26)
+    uint32_t* rowptr = nullptr;   // n+1
+    uint32_t* col = nullptr;      // m
+    uint32_t* src = nullptr;      // m (built on the device)
+
+    // transpose of the oriented CSR: in-edges of v are in_src/in_eid[in_ptr[v] .. in_ptr[v+1])
+    uint32_t* in_ptr = nullptr;   // n+1
+    uint32_t* in_src = nullptr;   // m: source u of the in-edge
+    uint32_t* in_eid = nullptr;   // m: index of the edge u->v in col
+
+    ga_items light, heavy;        // degree-binned work lists of the hash-probe kernel
+    bool prepared = false;
+    ga_loops* loops = nullptr;    // peeling / core loop state, allocated on first use
+
+    // small device / pinned host scalars
+    unsigned long long* d_scalars = nullptr;   // 64 slots
+    unsigned long long* h_scalars = nullptr;   // 64 slots, pinned
+    uint32_t* d_queue = nullptr;               // 8 work-queue counters
+
+    // options (ga_option)
+    int64_t opt_tc_kernel = 0, opt_loop_mode = 0, opt_max_rounds = 0;
+    uint32_t item_work = 4096, heavy_bits_cap = 0, light_max_deg = 256;
+
+    // every device allocation, freed by ga_graph_destroy
+    std::vector<std::pair<void*, size_t>> allocations;
+    uint64_t bytes = 0;
+};
+
+namespace ga {
+
+// Device allocation owned by g (freed at destroy) and counted in g->bytes.
+template <class T>
+inline ga_status dalloc(ga_graph* g, T** p, size_t count) {
+    void* q = nullptr;
+    const size_t bytes = (count ? count : 1) * sizeof(T);
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        return fail(GA_ERR_OUT_OF_MEMORY, "cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    }
+    g->allocations.emplace_back(q, bytes);
+    g->bytes += bytes;
+    *p = (T*)q;
+    return GA_OK;
+}
+
+// Releases one allocation made by dalloc early (e.g. a work list that is rebuilt).
+void dfree(ga_graph* g, void* p);
+
+// Makes g's device current for the calling thread.
+ga_status use_device(const ga_graph* g);
+
+// Frees the loop state (CUDA graphs, pinned buffers) of g.
+void destroy_loops(ga_graph* g);
+
+// Builds src, in-lists and work lists (idempotent).
+ga_status prepare(ga_graph* g);
+
+// Device-wide exclusive scan of n uint32 values (in place allowed); out[n] receives the total when out has n+1 slots
+// and `write_total` is set. Uses scratch from g.
+ga_status exclusive_scan_u32(ga_graph* g, const uint32_t* in, uint32_t* out, uint32_t n, bool write_total);
+
+}  // namespace ga

@@ -1,0 +1,512 @@
+// ga_graph.cu - device-resident graph handle: upload, validation, and the derived structures every query shares.
+//
+// Derived structures (built once per handle, on the device, kept resident):
+//   src[m]                 row owner of every edge (the reference builds it on the host, graph.h:64)
+//   in_ptr/in_src/in_eid   transpose of the oriented CSR: for every vertex v the edges u->v (source, edge index)
+//   light / heavy items    degree-binned work lists of the hash-probe kernels: one item = a slice of v's in-edges
+//                          whose probe work (sum of out-degrees of the sources) is bounded; anchors with a large
+//                          out-degree go to the block-wide "heavy" bin, the rest to the per-warp "light" bin.
+#include <algorithm>
+#include <cstring>
+
+#include "ga_device.cuh"
+
+namespace ga {
+
+// ---- scan (reduce-then-scan over tiles of 256 threads x 16 elements) --------------------------------------------
+constexpr int kScanThreads = 256, kScanItems = 16, kScanTile = kScanThreads * kScanItems;
+
+template <class T>
+__global__ void k_tile_reduce(const T* __restrict__ in, uint64_t n, T* __restrict__ sums) {
+    __shared__ T s_w[kScanThreads / 32];
+    const uint64_t base = (uint64_t)blockIdx.x * kScanTile;
+    T acc = 0;
+    for (int i = threadIdx.x; i < kScanTile; i += kScanThreads) {
+        const uint64_t k = base + i;
+        if (k < n) acc += in[k];
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(GA_FULL_MASK, acc, o);
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        T t = 0;
+        for (int w = 0; w < kScanThreads / 32; w++) t += s_w[w];
+        sums[blockIdx.x] = t;
+    }
+}
+
+// Scans one tile; `offsets` (may be null) holds the exclusive prefix of every tile.
+template <class T>
+__global__ void k_tile_scan(const T* __restrict__ in, T* __restrict__ out, uint64_t n, const T* __restrict__ offsets,
+                            int inclusive) {
+    __shared__ T s_tile[kScanTile];
+    __shared__ T s_w[kScanThreads / 32];
+    const uint64_t base = (uint64_t)blockIdx.x * kScanTile;
+    for (int i = threadIdx.x; i < kScanTile; i += kScanThreads) {   // coalesced load through shared memory
+        const uint64_t k = base + i;
+        s_tile[i] = k < n ? in[k] : (T)0;
+    }
+    __syncthreads();
+    T v[kScanItems];
+    T run = 0;
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) { v[j] = s_tile[threadIdx.x * kScanItems + j]; run += v[j]; }
+    // exclusive prefix of the thread totals across the block
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    T x = run;
+    for (int o = 1; o < 32; o <<= 1) {
+        const T t = __shfl_up_sync(GA_FULL_MASK, x, o);
+        if (lane >= (uint32_t)o) x += t;
+    }
+    if (lane == 31) s_w[w] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        T acc = 0;
+        for (int i = 0; i < kScanThreads / 32; i++) { const T t = s_w[i]; s_w[i] = acc; acc += t; }
+    }
+    __syncthreads();
+    T pre = x - run + s_w[w] + (offsets ? offsets[blockIdx.x] : (T)0);
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) {
+        const T val = v[j];
+        s_tile[threadIdx.x * kScanItems + j] = inclusive ? pre + val : pre;
+        pre += val;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kScanTile; i += kScanThreads) {
+        const uint64_t k = base + i;
+        if (k < n) out[k] = s_tile[i];
+    }
+}
+
+template <class T>
+static ga_status scan_impl(cudaStream_t st, const T* in, T* out, uint64_t n, bool inclusive) {
+    if (n == 0) return GA_OK;
+    const uint64_t nb = (n + kScanTile - 1) / kScanTile;
+    if (nb == 1) {
+        k_tile_scan<T><<<1, kScanThreads, 0, st>>>(in, out, n, nullptr, inclusive);
+        GA_CUDA(cudaGetLastError());
+        return GA_OK;
+    }
+    T* sums = nullptr;
+    GA_CUDA(cudaMallocAsync((void**)&sums, nb * sizeof(T), st));
+    k_tile_reduce<T><<<(unsigned)nb, kScanThreads, 0, st>>>(in, n, sums);
+    ga_status s = GA_OK;
+    if (cudaGetLastError() != cudaSuccess) s = fail(GA_ERR_CUDA, "scan reduce launch failed");
+    if (s == GA_OK) s = scan_impl<T>(st, sums, sums, nb, false);
+    if (s == GA_OK) {
+        k_tile_scan<T><<<(unsigned)nb, kScanThreads, 0, st>>>(in, out, n, sums, inclusive);
+        if (cudaGetLastError() != cudaSuccess) s = fail(GA_ERR_CUDA, "scan launch failed");
+    }
+    cudaFreeAsync(sums, st);
+    return s;
+}
+
+ga_status exclusive_scan_u32(ga_graph* g, const uint32_t* in, uint32_t* out, uint32_t n, bool write_total) {
+    GA_TRY(scan_impl<uint32_t>(g->stream, in, out, n, false));
+    (void)write_total;
+    return GA_OK;
+}
+
+// ---- validation and derived structures -------------------------------------------------------------------------
+
+// Flags in *err: 1 rowptr not monotone / beyond m, 2 endpoint >= n, 4 self loop, 8 row not strictly ascending.
+__global__ void k_validate(const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ col, uint32_t n,
+                           uint32_t m, unsigned long long* err) {
+    uint32_t bad = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const uint32_t b = rowptr[v], e = rowptr[v + 1];
+        if (b > e || e > m) { bad |= 1; continue; }
+        for (uint32_t i = b; i < e; i++) {
+            const uint32_t x = col[i];
+            if (x >= n) bad |= 2;
+            if (x == v) bad |= 4;
+            if (i > b && col[i - 1] >= x) bad |= 8;
+        }
+    }
+    if (bad) atomicOr(err, (unsigned long long)bad);
+}
+
+// src[e] = owner row; in-degree histogram.
+__global__ void k_src_and_indeg(const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ col, uint32_t n,
+                                uint32_t* __restrict__ src, uint32_t* __restrict__ indeg) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const uint32_t b = rowptr[v], e = rowptr[v + 1];
+        for (uint32_t i = b; i < e; i++) {
+            src[i] = v;
+            atomicAdd(&indeg[col[i]], 1u);
+        }
+    }
+}
+
+// Scatter every edge u->v into v's in-list; checks the (degree, id) orientation rule of graph.h:43-45 with
+// deg = out + in (flag 16 in *err when an edge points the wrong way).
+__global__ void k_in_scatter(const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ col,
+                             const uint32_t* __restrict__ src, const uint32_t* __restrict__ in_ptr, uint32_t m,
+                             uint32_t* __restrict__ fill, uint32_t* __restrict__ in_src,
+                             uint32_t* __restrict__ in_eid, unsigned long long* err) {
+    uint32_t bad = 0;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
+        const uint32_t u = src[e], v = col[e];
+        const uint32_t du = rowptr[u + 1] - rowptr[u] + in_ptr[u + 1] - in_ptr[u];
+        const uint32_t dv = rowptr[v + 1] - rowptr[v] + in_ptr[v + 1] - in_ptr[v];
+        if (!(du != dv ? du < dv : u < v)) bad |= 16;
+        const uint32_t p = in_ptr[v] + atomicAdd(&fill[v], 1u);
+        in_src[p] = u;
+        in_eid[p] = e;
+    }
+    if (bad) atomicOr(err, (unsigned long long)bad);
+}
+
+// work[k] = out-degree of the source of in-edge k (probe length of that in-edge).
+__global__ void k_in_work(const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ in_src, uint32_t m,
+                          unsigned long long* __restrict__ work) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        const uint32_t u = in_src[k];
+        work[k] = rowptr[u + 1] - rowptr[u];
+    }
+}
+
+// Items per anchor. prefix = inclusive scan of work over in-edges. An anchor with out-degree 0 or no in-edge has no
+// item; otherwise ceil(work / target) items (at least 1), light or heavy by its out-degree.
+__global__ void k_count_items(const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ in_ptr,
+                              const unsigned long long* __restrict__ prefix, uint32_t n, uint32_t light_max_deg,
+                              unsigned long long target, uint32_t* __restrict__ cnt_light,
+                              uint32_t* __restrict__ cnt_heavy, unsigned* max_dv_heavy) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const uint32_t dv = rowptr[v + 1] - rowptr[v];
+        const uint32_t b = in_ptr[v], e = in_ptr[v + 1];
+        uint32_t c = 0;
+        if (dv > 0 && e > b) {
+            const unsigned long long w = prefix[e - 1] - (b ? prefix[b - 1] : 0ull);
+            c = (uint32_t)max(1ull, (w + target - 1) / target);
+            if (c > e - b) c = e - b;
+        }
+        const bool heavy = dv > light_max_deg;
+        cnt_light[v] = heavy ? 0 : c;
+        cnt_heavy[v] = heavy ? c : 0;
+        if (heavy && c) atomicMax(max_dv_heavy, dv);
+    }
+}
+
+// Emits the items of every anchor: chunk c starts at the first in-edge whose local work prefix exceeds c * W / cnt.
+__global__ void k_emit_items(const uint32_t* __restrict__ in_ptr, const unsigned long long* __restrict__ prefix,
+                             const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ off, uint32_t n,
+                             uint32_t* __restrict__ it_v, uint32_t* __restrict__ it_k0, uint32_t* __restrict__ it_k1) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const uint32_t c = cnt[v];
+        if (!c) continue;
+        const uint32_t b = in_ptr[v], e = in_ptr[v + 1], o = off[v];
+        const unsigned long long base = b ? prefix[b - 1] : 0ull, w = prefix[e - 1] - base;
+        uint32_t start = b;
+        for (uint32_t i = 0; i < c; i++) {
+            uint32_t end = e;
+            if (i + 1 < c) {
+                // chunk i ends at the first k with local prefix > (i+1) * w / c; every chunk keeps >= 1 in-edge and
+                // leaves >= 1 for each later chunk (invariant: start <= e - (c - i))
+                const unsigned long long goal = base + (w * (i + 1)) / c;
+                uint32_t lo = start, hi = e;
+                while (lo < hi) {
+                    const uint32_t mid = lo + ((hi - lo) >> 1);
+                    if (prefix[mid] <= goal) lo = mid + 1; else hi = mid;
+                }
+                end = lo > start ? lo : start + 1;
+                if (end > e - (c - 1 - i)) end = e - (c - 1 - i);
+            }
+            it_v[o + i] = v;
+            it_k0[o + i] = start;
+            it_k1[o + i] = end;
+            start = end;
+        }
+    }
+}
+
+void dfree(ga_graph* g, void* p) {
+    if (!p) return;
+    for (size_t i = 0; i < g->allocations.size(); i++)
+        if (g->allocations[i].first == p) {
+            g->bytes -= g->allocations[i].second;
+            g->allocations.erase(g->allocations.begin() + i);
+            break;
+        }
+    cudaFree(p);
+}
+
+ga_status use_device(const ga_graph* g) {
+    GA_CUDA(cudaSetDevice(g->device));
+    return GA_OK;
+}
+
+static ga_status build_items(ga_graph* g, const unsigned long long* prefix, uint32_t* cnt_l, uint32_t* cnt_h,
+                             uint32_t* off_l, uint32_t* off_h, unsigned* d_maxdv) {
+    cudaStream_t st = g->stream;
+    const uint32_t n = g->n;
+    const unsigned grid = grid_for(n, 256);
+    const unsigned long long target = g->item_work;   // probes per item (bounds the tail of the dynamic queue)
+    GA_CUDA(cudaMemsetAsync(d_maxdv, 0, sizeof(unsigned), st));
+    k_count_items<<<grid, 256, 0, st>>>(g->rowptr, g->in_ptr, prefix, n, g->light_max_deg, target, cnt_l, cnt_h,
+                                        d_maxdv);
+    GA_CUDA(cudaGetLastError());
+    GA_TRY(scan_impl<uint32_t>(st, cnt_l, off_l, n, false));
+    GA_TRY(scan_impl<uint32_t>(st, cnt_h, off_h, n, false));
+    uint32_t h[5] = {0, 0, 0, 0, 0};
+    GA_CUDA(cudaMemcpyAsync(&h[0], off_l + n - 1, 4, cudaMemcpyDeviceToHost, st));
+    GA_CUDA(cudaMemcpyAsync(&h[1], cnt_l + n - 1, 4, cudaMemcpyDeviceToHost, st));
+    GA_CUDA(cudaMemcpyAsync(&h[2], off_h + n - 1, 4, cudaMemcpyDeviceToHost, st));
+    GA_CUDA(cudaMemcpyAsync(&h[3], cnt_h + n - 1, 4, cudaMemcpyDeviceToHost, st));
+    GA_CUDA(cudaMemcpyAsync(&h[4], d_maxdv, 4, cudaMemcpyDeviceToHost, st));
+    GA_CUDA(cudaStreamSynchronize(st));
+    ga_items* bins[2] = {&g->light, &g->heavy};
+    const uint32_t totals[2] = {h[0] + h[1], h[2] + h[3]};
+    uint32_t* cnts[2] = {cnt_l, cnt_h};
+    uint32_t* offs[2] = {off_l, off_h};
+    for (int b = 0; b < 2; b++) {
+        ga_items* it = bins[b];
+        dfree(g, it->v); dfree(g, it->k0); dfree(g, it->k1);
+        *it = ga_items{};
+        it->count = totals[b];
+        GA_TRY(dalloc(g, &it->v, totals[b]));
+        GA_TRY(dalloc(g, &it->k0, totals[b]));
+        GA_TRY(dalloc(g, &it->k1, totals[b]));
+        if (totals[b]) {
+            k_emit_items<<<grid, 256, 0, st>>>(g->in_ptr, prefix, cnts[b], offs[b], n, it->v, it->k0, it->k1);
+            GA_CUDA(cudaGetLastError());
+        }
+    }
+    g->light.max_dv = std::min<uint32_t>(g->light_max_deg, g->max_out_degree);
+    g->heavy.max_dv = h[4];
+    return GA_OK;
+}
+
+ga_status prepare(ga_graph* g) {
+    if (g->prepared) return GA_OK;
+    GA_TRY(use_device(g));
+    cudaStream_t st = g->stream;
+    const uint32_t n = g->n, m = g->m;
+    GA_CUDA(cudaStreamSynchronize(st));
+    for (uint32_t** p : {&g->src, &g->in_ptr, &g->in_src, &g->in_eid}) { dfree(g, *p); *p = nullptr; }
+    GA_TRY(dalloc(g, &g->src, m));
+    GA_TRY(dalloc(g, &g->in_ptr, (size_t)n + 1));
+    GA_TRY(dalloc(g, &g->in_src, m));
+    GA_TRY(dalloc(g, &g->in_eid, m));
+    uint32_t *indeg = nullptr, *fill = nullptr;
+    GA_CUDA(cudaMallocAsync((void**)&indeg, ((size_t)n + 1) * 4, st));
+    GA_CUDA(cudaMallocAsync((void**)&fill, ((size_t)n + 1) * 4, st));
+    unsigned long long* err = g->d_scalars + 63;
+    GA_CUDA(cudaMemsetAsync(err, 0, 8, st));
+    GA_CUDA(cudaMemsetAsync(indeg, 0, ((size_t)n + 1) * 4, st));
+    GA_CUDA(cudaMemsetAsync(fill, 0, ((size_t)n + 1) * 4, st));
+    const unsigned gv = grid_for(n, 256), ge = grid_for(m, 256);
+    if (n) {
+        k_src_and_indeg<<<gv, 256, 0, st>>>(g->rowptr, g->col, n, g->src, indeg);
+        GA_CUDA(cudaGetLastError());
+    }
+    GA_TRY(scan_impl<uint32_t>(st, indeg, g->in_ptr, (uint64_t)n + 1, false));   // indeg[n] = 0 -> in_ptr[n] = m
+    if (m) {
+        k_in_scatter<<<ge, 256, 0, st>>>(g->rowptr, g->col, g->src, g->in_ptr, m, fill, g->in_src, g->in_eid, err);
+        GA_CUDA(cudaGetLastError());
+    }
+    // work prefix over in-edges (64-bit: the total probe count can exceed 2^32)
+    unsigned long long* prefix = nullptr;
+    GA_CUDA(cudaMallocAsync((void**)&prefix, ((size_t)m + 1) * 8, st));
+    if (m) {
+        k_in_work<<<ge, 256, 0, st>>>(g->rowptr, g->in_src, m, prefix);
+        GA_CUDA(cudaGetLastError());
+        GA_TRY(scan_impl<unsigned long long>(st, prefix, prefix, m, true));
+    }
+    uint32_t *cnt_l = nullptr, *cnt_h = nullptr, *off_l = nullptr, *off_h = nullptr;
+    GA_CUDA(cudaMallocAsync((void**)&cnt_l, ((size_t)n + 1) * 4, st));
+    GA_CUDA(cudaMallocAsync((void**)&cnt_h, ((size_t)n + 1) * 4, st));
+    GA_CUDA(cudaMallocAsync((void**)&off_l, ((size_t)n + 1) * 4, st));
+    GA_CUDA(cudaMallocAsync((void**)&off_h, ((size_t)n + 1) * 4, st));
+    ga_status s = GA_OK;
+    if (n) s = build_items(g, prefix, cnt_l, cnt_h, off_l, off_h, (unsigned*)(g->d_scalars + 62));
+    cudaFreeAsync(prefix, st);
+    cudaFreeAsync(cnt_l, st);
+    cudaFreeAsync(cnt_h, st);
+    cudaFreeAsync(off_l, st);
+    cudaFreeAsync(off_h, st);
+    cudaFreeAsync(indeg, st);
+    cudaFreeAsync(fill, st);
+    GA_TRY(s);
+    unsigned long long herr = 0;
+    GA_CUDA(cudaMemcpyAsync(&herr, err, 8, cudaMemcpyDeviceToHost, st));
+    GA_CUDA(cudaStreamSynchronize(st));
+    if (herr & 16)
+        return fail(GA_ERR_INVALID_GRAPH, "CSR is not oriented by (degree, id) (graph.h:43-45): an edge points from "
+                                          "the larger to the smaller endpoint, or an undirected edge is stored twice");
+    g->prepared = true;
+    return GA_OK;
+}
+
+static ga_status create_common(const uint32_t* rowptr, const uint32_t* col, uint32_t n, uint32_t m, int device,
+                               void* stream, bool from_device, ga_graph** out) {
+    if (!out) return fail(GA_ERR_INVALID_ARGUMENT, "out is null");
+    *out = nullptr;
+    if (!rowptr || (m && !col)) return fail(GA_ERR_INVALID_ARGUMENT, "null CSR array");
+    if (n == UINT32_MAX) return fail(GA_ERR_INVALID_ARGUMENT, "n must be < 2^32 - 1");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        (void)cudaGetLastError();
+        return fail(GA_ERR_NO_DEVICE, "no CUDA device");
+    }
+    if (device < 0 || device >= count) return fail(GA_ERR_INVALID_ARGUMENT, "device %d out of range", device);
+    if (!from_device && (rowptr[0] != 0 || rowptr[n] != m))
+        return fail(GA_ERR_INVALID_GRAPH, "rowptr[0] must be 0 and rowptr[n] must equal m");
+    ga_graph* g = new ga_graph();
+    g->device = device;
+    g->n = n;
+    g->m = m;
+    auto bail = [&](ga_status s) { ga_graph_destroy(g); return s; };
+    if (cudaSetDevice(device) != cudaSuccess) return bail(fail(GA_ERR_CUDA, "cudaSetDevice(%d) failed", device));
+    cudaDeviceGetAttribute(&g->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (stream) {
+        g->stream = (cudaStream_t)stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess)
+            return bail(fail(GA_ERR_CUDA, "cudaStreamCreate failed"));
+        g->own_stream = true;
+    }
+    ga_status s;
+    if ((s = dalloc(g, &g->rowptr, (size_t)n + 1)) != GA_OK) return bail(s);
+    if ((s = dalloc(g, &g->col, m)) != GA_OK) return bail(s);
+    if ((s = dalloc(g, &g->d_scalars, 64)) != GA_OK) return bail(s);
+    if ((s = dalloc(g, &g->d_queue, 8)) != GA_OK) return bail(s);
+    if (cudaMallocHost((void**)&g->h_scalars, 64 * 8) != cudaSuccess)
+        return bail(fail(GA_ERR_OUT_OF_MEMORY, "cudaMallocHost failed"));
+    const cudaMemcpyKind kind = from_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (cudaMemcpyAsync(g->rowptr, rowptr, ((size_t)n + 1) * 4, kind, g->stream) != cudaSuccess ||
+        (m && cudaMemcpyAsync(g->col, col, (size_t)m * 4, kind, g->stream) != cudaSuccess))
+        return bail(fail(GA_ERR_CUDA, "CSR copy to the device failed"));
+    unsigned long long* err = g->d_scalars + 63;
+    cudaMemsetAsync(err, 0, 8, g->stream);
+    if (n) k_validate<<<grid_for(n, 256), 256, 0, g->stream>>>(g->rowptr, g->col, n, m, err);
+    unsigned long long herr = 0;
+    uint32_t ends[2] = {0, 0};
+    cudaMemcpyAsync(&herr, err, 8, cudaMemcpyDeviceToHost, g->stream);
+    if (from_device) {
+        cudaMemcpyAsync(&ends[0], g->rowptr, 4, cudaMemcpyDeviceToHost, g->stream);
+        cudaMemcpyAsync(&ends[1], g->rowptr + n, 4, cudaMemcpyDeviceToHost, g->stream);
+    }
+    if (cudaStreamSynchronize(g->stream) != cudaSuccess) {
+        const char* why = cudaGetErrorString(cudaGetLastError());
+        return bail(fail(GA_ERR_CUDA, "validation failed: %s", why));
+    }
+    if (from_device && (ends[0] != 0 || ends[1] != m))
+        return bail(fail(GA_ERR_INVALID_GRAPH, "rowptr[0] must be 0 and rowptr[n] must equal m"));
+    if (herr)
+        return bail(fail(GA_ERR_INVALID_GRAPH, "invalid CSR (flags 0x%llx: 1 rowptr, 2 endpoint >= n, 4 self loop, "
+                                               "8 row not strictly ascending)", herr));
+    // max out-degree on the host side of the copy
+    uint32_t mx = 0;
+    if (!from_device) {
+        for (uint32_t v = 0; v < n; v++) mx = std::max(mx, rowptr[v + 1] - rowptr[v]);
+    } else {
+        std::vector<uint32_t> rp((size_t)n + 1);
+        if (cudaMemcpy(rp.data(), g->rowptr, ((size_t)n + 1) * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return bail(fail(GA_ERR_CUDA, "rowptr download failed"));
+        for (uint32_t v = 0; v < n; v++) mx = std::max(mx, rp[v + 1] - rp[v]);
+    }
+    g->max_out_degree = mx;
+    *out = g;
+    return GA_OK;
+}
+
+}  // namespace ga
+
+using namespace ga;
+
+extern "C" {
+
+ga_status ga_device_count(int* count) {
+    if (!count) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    *count = 0;
+    if (cudaGetDeviceCount(count) != cudaSuccess) {
+        (void)cudaGetLastError();
+        *count = 0;
+    }
+    return GA_OK;
+}
+
+ga_status ga_graph_create(const uint32_t* rowptr, const uint32_t* col, uint32_t n, uint32_t m, int device,
+                          void* stream, ga_graph** out) {
+    return create_common(rowptr, col, n, m, device, stream, false, out);
+}
+
+ga_status ga_graph_create_device(const uint32_t* d_rowptr, const uint32_t* d_col, uint32_t n, uint32_t m, int device,
+                                 void* stream, ga_graph** out) {
+    return create_common(d_rowptr, d_col, n, m, device, stream, true, out);
+}
+
+ga_status ga_graph_destroy(ga_graph* g) {
+    if (!g) return GA_OK;
+    cudaSetDevice(g->device);
+    if (g->stream) cudaStreamSynchronize(g->stream);
+    destroy_loops(g);
+    for (auto& a : g->allocations) cudaFree(a.first);
+    if (g->h_scalars) cudaFreeHost(g->h_scalars);
+    if (g->own_stream && g->stream) cudaStreamDestroy(g->stream);
+    delete g;
+    return GA_OK;
+}
+
+ga_status ga_graph_set_stream(ga_graph* g, void* stream) {
+    if (!g) return fail(GA_ERR_INVALID_ARGUMENT, "null graph");
+    GA_TRY(use_device(g));
+    GA_CUDA(cudaStreamSynchronize(g->stream));
+    if (g->own_stream) { cudaStreamDestroy(g->stream); g->own_stream = false; }
+    if (stream) {
+        g->stream = (cudaStream_t)stream;
+    } else {
+        GA_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+        g->own_stream = true;
+    }
+    return GA_OK;
+}
+
+ga_status ga_graph_device_bytes(const ga_graph* g, uint64_t* bytes) {
+    if (!g || !bytes) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    *bytes = g->bytes;
+    return GA_OK;
+}
+
+ga_status ga_graph_prepare(ga_graph* g) {
+    if (!g) return fail(GA_ERR_INVALID_ARGUMENT, "null graph");
+    return prepare(g);
+}
+
+ga_status ga_graph_set_option(ga_graph* g, ga_option opt, int64_t value) {
+    if (!g) return fail(GA_ERR_INVALID_ARGUMENT, "null graph");
+    if (value < 0) return fail(GA_ERR_INVALID_ARGUMENT, "option values are >= 0");
+    switch (opt) {
+        case GA_OPT_TC_KERNEL:
+            if (value > 2) return fail(GA_ERR_INVALID_ARGUMENT, "GA_OPT_TC_KERNEL is 0, 1 or 2");
+            g->opt_tc_kernel = value;
+            return GA_OK;
+        case GA_OPT_LOOP_MODE:
+            if (value > 2) return fail(GA_ERR_INVALID_ARGUMENT, "GA_OPT_LOOP_MODE is 0, 1 or 2");
+            g->opt_loop_mode = value;
+            return GA_OK;
+        case GA_OPT_MAX_ROUNDS:
+            g->opt_max_rounds = value;
+            return GA_OK;
+        case GA_OPT_ITEM_WORK: {
+            const uint32_t v = value ? (uint32_t)std::min<int64_t>(value, 1 << 30) : 4096;
+            if (v != g->item_work) { g->item_work = v; g->prepared = false; }
+            return GA_OK;
+        }
+        case GA_OPT_HEAVY_TABLE_BITS:
+            if (value != 0 && (value < 5 || value > 15))
+                return fail(GA_ERR_INVALID_ARGUMENT, "GA_OPT_HEAVY_TABLE_BITS is 0 or 5..15");
+            g->heavy_bits_cap = (uint32_t)value;
+            return GA_OK;
+        case GA_OPT_LIGHT_MAX_DEG: {
+            const uint32_t v = value ? (uint32_t)std::min<int64_t>(value, 256) : 256;
+            if (v != g->light_max_deg) { g->light_max_deg = v; g->prepared = false; }
+            return GA_OK;
+        }
+    }
+    return fail(GA_ERR_INVALID_ARGUMENT, "unknown option %d", (int)opt);
+}
+
+}  // extern "C"

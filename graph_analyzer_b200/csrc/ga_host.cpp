@@ -1,0 +1,425 @@
+// ga_host.cpp - host side of the C ABI: status strings, the graph.h surface (edge clean-up, (degree,id) orientation,
+// CSR build, text loader) and the seeded synthetic generators.
+//
+// The CSR produced here is the reference's layout exactly (graph.h:15-26, 38-67): edge {a,b} stored once, from the
+// endpoint with the smaller (degree, id); rows sorted ascending; src[e] = row owner. The construction is parallel
+// (OpenMP radix sort and scatter) but its output does not depend on thread count or order, because rows hold unique
+// ids and are sorted at the end.
+#include <omp.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cerrno>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <vector>
+
+#include "ga_internal.h"
+
+namespace ga {
+
+static thread_local std::string t_err;
+
+ga_status fail(ga_status s, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    t_err = buf;
+    return s;
+}
+void clear_error() { t_err.clear(); }
+
+// LSD radix sort of 64-bit keys on the bits [0, key_bits), 11 bits per pass, OpenMP histograms per thread.
+static void radix_sort_u64(std::vector<uint64_t>& a, int key_bits) {
+    const size_t N = a.size();
+    if (N < 2) return;
+    std::vector<uint64_t> tmp(N);
+    const int R = 11, B = 1 << R;
+    const int nthreads = std::max(1, std::min(omp_get_max_threads(), (int)(N / 65536) + 1));
+    std::vector<size_t> hist((size_t)nthreads * B);
+    uint64_t* in = a.data();
+    uint64_t* out = tmp.data();
+    int passes = 0;
+    for (int shift = 0; shift < key_bits; shift += R, passes++) {
+        std::fill(hist.begin(), hist.end(), 0);
+#pragma omp parallel num_threads(nthreads)
+        {
+            const int t = omp_get_thread_num();
+            const size_t lo = N * t / nthreads, hi = N * (t + 1) / nthreads;
+            size_t* h = hist.data() + (size_t)t * B;
+            for (size_t i = lo; i < hi; i++) h[(in[i] >> shift) & (B - 1)]++;
+#pragma omp barrier
+#pragma omp single
+            {
+                size_t sum = 0;
+                for (int d = 0; d < B; d++)
+                    for (int tt = 0; tt < nthreads; tt++) {
+                        size_t c = hist[(size_t)tt * B + d];
+                        hist[(size_t)tt * B + d] = sum;
+                        sum += c;
+                    }
+            }
+            for (size_t i = lo; i < hi; i++) out[h[(in[i] >> shift) & (B - 1)]++] = in[i];
+        }
+        std::swap(in, out);
+    }
+    if (passes & 1) std::memcpy(a.data(), in, N * sizeof(uint64_t));
+}
+
+static int bits_for(uint64_t x) {
+    int b = 0;
+    while (b < 64 && (x >> b)) b++;
+    return b;
+}
+
+// graph.h:85-92 on interleaved pairs.
+static uint64_t canonicalize(uint32_t* pairs, uint64_t npairs) {
+    std::vector<uint64_t> key(npairs);
+    std::atomic<uint64_t> k{0};
+    uint64_t kept = 0;
+    uint32_t maxv = 0;
+#pragma omp parallel for reduction(max : maxv) schedule(static)
+    for (int64_t i = 0; i < (int64_t)npairs; i++) {
+        uint32_t a = pairs[2 * i], b = pairs[2 * i + 1];
+        if (a > b) std::swap(a, b);
+        key[i] = a == b ? UINT64_MAX : ((uint64_t)a << 32) | b;
+        if (a != b) maxv = std::max(maxv, b);
+    }
+    (void)k;
+    // keys without self loops are < 2^(32 + bits(maxv)); self loops (UINT64_MAX) must sort last, so sort all 64 bits
+    // when any is present, else only the used bits.
+    bool any_loop = false;
+    for (uint64_t i = 0; i < npairs && !any_loop; i++) any_loop = key[i] == UINT64_MAX;
+    radix_sort_u64(key, any_loop ? 64 : 32 + bits_for(maxv));
+    for (uint64_t i = 0; i < npairs; i++) {
+        if (key[i] == UINT64_MAX) break;
+        if (kept > 0 && key[i] == key[i - 1]) continue;
+        key[kept++] = key[i];
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)kept; i++) {
+        pairs[2 * i] = (uint32_t)(key[i] >> 32);
+        pairs[2 * i + 1] = (uint32_t)key[i];
+    }
+    return kept;
+}
+
+// graph.h:38-67.
+static ga_status build_csr(uint32_t n, const uint32_t* pairs, uint32_t m, uint32_t* rowptr, uint32_t* col,
+                           uint32_t* src, uint32_t* max_out_degree) {
+    std::unique_ptr<std::atomic<uint32_t>[]> deg(new (std::nothrow) std::atomic<uint32_t>[n ? n : 1]);
+    if (!deg) return fail(GA_ERR_OUT_OF_MEMORY, "host allocation of %u degrees failed", n);
+#pragma omp parallel for schedule(static)
+    for (int64_t v = 0; v < (int64_t)n; v++) deg[v].store(0, std::memory_order_relaxed);
+    bool bad = false;
+#pragma omp parallel for schedule(static) reduction(|| : bad)
+    for (int64_t e = 0; e < (int64_t)m; e++) {
+        const uint32_t a = pairs[2 * e], b = pairs[2 * e + 1];
+        if (a >= n || b >= n || a == b) { bad = true; continue; }
+        deg[a].fetch_add(1, std::memory_order_relaxed);
+        deg[b].fetch_add(1, std::memory_order_relaxed);
+    }
+    if (bad) return fail(GA_ERR_INVALID_GRAPH, "edge list has an endpoint >= n=%u or a self loop", n);
+    auto before = [&](uint32_t a, uint32_t b) {
+        const uint32_t da = deg[a].load(std::memory_order_relaxed), db = deg[b].load(std::memory_order_relaxed);
+        return da != db ? da < db : a < b;
+    };
+    std::unique_ptr<std::atomic<uint32_t>[]> fill(new (std::nothrow) std::atomic<uint32_t>[n ? n : 1]);
+    if (!fill) return fail(GA_ERR_OUT_OF_MEMORY, "host allocation failed");
+#pragma omp parallel for schedule(static)
+    for (int64_t v = 0; v < (int64_t)n; v++) fill[v].store(0, std::memory_order_relaxed);
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < (int64_t)m; e++) {
+        const uint32_t a = pairs[2 * e], b = pairs[2 * e + 1];
+        fill[before(a, b) ? a : b].fetch_add(1, std::memory_order_relaxed);
+    }
+    rowptr[0] = 0;
+    for (uint32_t v = 0; v < n; v++) {
+        rowptr[v + 1] = rowptr[v] + fill[v].load(std::memory_order_relaxed);
+        fill[v].store(rowptr[v], std::memory_order_relaxed);
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t e = 0; e < (int64_t)m; e++) {
+        const uint32_t a = pairs[2 * e], b = pairs[2 * e + 1];
+        const bool fwd = before(a, b);
+        const uint32_t from = fwd ? a : b, to = fwd ? b : a;
+        col[fill[from].fetch_add(1, std::memory_order_relaxed)] = to;
+    }
+    uint32_t mx = 0;
+    bool dup = false;
+#pragma omp parallel for schedule(dynamic, 4096) reduction(max : mx) reduction(|| : dup)
+    for (int64_t u = 0; u < (int64_t)n; u++) {
+        const uint32_t b = rowptr[u], e = rowptr[u + 1];
+        std::sort(col + b, col + e);
+        for (uint32_t i = b; i < e; i++) {
+            src[i] = (uint32_t)u;
+            if (i > b && col[i] == col[i - 1]) dup = true;
+        }
+        mx = std::max(mx, e - b);
+    }
+    if (dup) return fail(GA_ERR_INVALID_GRAPH, "edge list contains duplicate pairs (run ga_canonical_edges first)");
+    *max_out_degree = mx;
+    return GA_OK;
+}
+
+static ga_host_graph* new_host_graph(uint32_t n, uint32_t m) {
+    ga_host_graph* g = (ga_host_graph*)std::calloc(1, sizeof(ga_host_graph));
+    if (!g) return nullptr;
+    g->n = n;
+    g->m = m;
+    g->rowptr = (uint32_t*)std::malloc(((size_t)n + 1) * sizeof(uint32_t));
+    g->col = (uint32_t*)std::malloc(((size_t)m + 1) * sizeof(uint32_t));
+    g->src = (uint32_t*)std::malloc(((size_t)m + 1) * sizeof(uint32_t));
+    if (!g->rowptr || !g->col || !g->src) { ga_host_graph_free(g); return nullptr; }
+    return g;
+}
+
+}  // namespace ga
+
+using namespace ga;
+
+extern "C" {
+
+const char* ga_status_string(ga_status s) {
+    switch (s) {
+        case GA_OK: return "GA_OK";
+        case GA_ERR_INVALID_ARGUMENT: return "GA_ERR_INVALID_ARGUMENT";
+        case GA_ERR_INVALID_GRAPH: return "GA_ERR_INVALID_GRAPH";
+        case GA_ERR_CUDA: return "GA_ERR_CUDA";
+        case GA_ERR_OUT_OF_MEMORY: return "GA_ERR_OUT_OF_MEMORY";
+        case GA_ERR_ARITH: return "GA_ERR_ARITH";
+        case GA_ERR_ROUND_LIMIT: return "GA_ERR_ROUND_LIMIT";
+        case GA_ERR_IO: return "GA_ERR_IO";
+        case GA_ERR_NO_DEVICE: return "GA_ERR_NO_DEVICE";
+        case GA_ERR_DEVICE_CHECK: return "GA_ERR_DEVICE_CHECK";
+        case GA_ERR_BUDGET: return "GA_ERR_BUDGET";
+        case GA_ERR_CAPACITY: return "GA_ERR_CAPACITY";
+        case GA_ERR_NOT_READY: return "GA_ERR_NOT_READY";
+    }
+    return "GA_ERR_UNKNOWN";
+}
+
+const char* ga_last_error(void) { return t_err.c_str(); }
+
+ga_status ga_canonical_edges(uint32_t* pairs, uint64_t npairs, uint64_t* out_npairs) {
+    if ((!pairs && npairs) || !out_npairs) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    try {
+        *out_npairs = canonicalize(pairs, npairs);
+    } catch (const std::bad_alloc&) {
+        return fail(GA_ERR_OUT_OF_MEMORY, "host allocation failed sorting %llu pairs", (unsigned long long)npairs);
+    }
+    return GA_OK;
+}
+
+ga_status ga_build_graph_from_edges(uint32_t n, const uint32_t* pairs, uint32_t m, uint32_t* rowptr, uint32_t* col,
+                                    uint32_t* src, uint32_t* max_out_degree) {
+    if ((!pairs && m) || !rowptr || ((!col || !src) && m) || !max_out_degree)
+        return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    return build_csr(n, pairs, m, rowptr, col, src, max_out_degree);
+}
+
+ga_status ga_host_graph_from_edges(uint32_t n, const uint32_t* pairs, uint64_t npairs, int canonicalize_first,
+                                   ga_host_graph** out) {
+    if ((!pairs && npairs) || !out) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    try {
+        std::vector<uint32_t> copy;
+        const uint32_t* p = pairs;
+        uint64_t m = npairs;
+        if (canonicalize_first) {
+            copy.assign(pairs, pairs + 2 * npairs);
+            m = canonicalize(copy.data(), npairs);
+            p = copy.data();
+        }
+        if (m > UINT32_MAX - 1) return fail(GA_ERR_INVALID_GRAPH, "more than 2^32-2 edges");
+        ga_host_graph* g = new_host_graph(n, (uint32_t)m);
+        if (!g) return fail(GA_ERR_OUT_OF_MEMORY, "host allocation failed");
+        ga_status s = build_csr(n, p, (uint32_t)m, g->rowptr, g->col, g->src, &g->max_out_degree);
+        if (s != GA_OK) { ga_host_graph_free(g); return s; }
+        *out = g;
+    } catch (const std::bad_alloc&) {
+        return fail(GA_ERR_OUT_OF_MEMORY, "host allocation failed");
+    }
+    return GA_OK;
+}
+
+ga_status ga_load_graph(const char* path, ga_host_graph** out) {
+    if (!path || !out) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return fail(GA_ERR_IO, "cannot open %s", path);
+    std::vector<uint32_t> pairs;
+    char line[512];
+    uint32_t max_id = 0;
+    bool big = false;
+    // graph.h:77-89: same line rules (fgets of 512 bytes, '#', '%' and empty lines skipped, two base-10 fields).
+    while (std::fgets(line, sizeof line, f)) {
+        if (line[0] == '#' || line[0] == '%' || line[0] == '\n') continue;
+        char* end;
+        const unsigned long a = std::strtoul(line, &end, 10);
+        if (end == line) continue;
+        char* end2;
+        const unsigned long b = std::strtoul(end, &end2, 10);
+        if (end2 == end) continue;
+        if (a == b) continue;
+        if (a > UINT32_MAX || b > UINT32_MAX) { big = true; break; }
+        const uint32_t u = (uint32_t)std::min(a, b), v = (uint32_t)std::max(a, b);
+        pairs.push_back(u);
+        pairs.push_back(v);
+        max_id = std::max(max_id, v);
+    }
+    std::fclose(f);
+    if (big) return fail(GA_ERR_INVALID_GRAPH, "%s: vertex id does not fit uint32", path);
+    if (max_id == UINT32_MAX) return fail(GA_ERR_INVALID_GRAPH, "%s: n = max_id + 1 overflows uint32", path);
+    return ga_host_graph_from_edges(max_id + 1, pairs.data(), pairs.size() / 2, 1, out);
+}
+
+void ga_host_graph_free(ga_host_graph* g) {
+    if (!g) return;
+    std::free(g->rowptr);
+    std::free(g->col);
+    std::free(g->src);
+    std::free(g);
+}
+
+// ---- generators ------------------------------------------------------------------------------------------------
+
+ga_status ga_gen_holme_kim(uint32_t n, uint32_t m_lo, uint32_t m_hi, double p_hi, double triad_p, uint64_t seed,
+                           uint32_t* pairs, uint64_t cap, uint64_t* npairs) {
+    if (!pairs || !npairs || m_lo == 0 || m_hi < m_lo || n <= m_hi)
+        return fail(GA_ERR_INVALID_ARGUMENT, "holme_kim: need 1 <= m_lo <= m_hi < n and output buffers");
+    Rng rng(seed);
+    std::vector<std::vector<uint32_t>> adj(n);
+    std::vector<uint32_t> repeated;          // every endpoint of every edge, plus the initial vertices
+    repeated.reserve((size_t)2 * n * m_hi + m_hi);
+    for (uint32_t v = 0; v < m_hi; v++) repeated.push_back(v);
+    uint64_t k = 0;
+    std::vector<uint32_t> targets, linked;
+    auto has = [&](uint32_t a, uint32_t b) {       // a is the new vertex: its list is short
+        for (uint32_t x : adj[a]) if (x == b) return true;
+        return false;
+    };
+    auto add = [&](uint32_t a, uint32_t b) -> bool {
+        if (k >= cap) return false;
+        adj[a].push_back(b);
+        adj[b].push_back(a);
+        pairs[2 * k] = a;
+        pairs[2 * k + 1] = b;
+        k++;
+        return true;
+    };
+    for (uint32_t src = m_hi; src < n; src++) {
+        const uint32_t mv = (m_hi != m_lo && rng.uniform() < p_hi) ? m_hi : m_lo;
+        // mv distinct preferential-attachment targets (uniform over the repeated-endpoint list)
+        targets.clear();
+        while (targets.size() < mv) {
+            const uint32_t t = repeated[rng.below(repeated.size())];
+            if (std::find(targets.begin(), targets.end(), t) == targets.end()) targets.push_back(t);
+        }
+        uint32_t last = targets.back();
+        targets.pop_back();
+        if (!add(src, last)) return fail(GA_ERR_CAPACITY, "holme_kim: pair buffer too small");
+        repeated.push_back(last);
+        uint32_t count = 1;
+        while (count < mv) {
+            bool closed = false;
+            if (rng.uniform() < triad_p) {
+                // triad step: a uniformly chosen neighbour of `last` not yet linked to src (rejection sampling over
+                // last's list, then a scan when the tries run out)
+                const auto& nb = adj[last];
+                uint32_t pick = UINT32_MAX;
+                for (int tries = 0; tries < 16 && pick == UINT32_MAX; tries++) {
+                    const uint32_t c = nb[rng.below(nb.size())];
+                    if (c != src && !has(src, c)) pick = c;
+                }
+                if (pick == UINT32_MAX) {
+                    linked.clear();
+                    for (uint32_t c : nb) if (c != src && !has(src, c)) linked.push_back(c);
+                    if (!linked.empty()) pick = linked[rng.below(linked.size())];
+                }
+                if (pick != UINT32_MAX) {
+                    if (!add(src, pick)) return fail(GA_ERR_CAPACITY, "holme_kim: pair buffer too small");
+                    repeated.push_back(pick);
+                    count++;
+                    closed = true;
+                }
+            }
+            if (closed) continue;
+            // preferential-attachment step with the next unused target; a target the triad steps already linked
+            // is replaced by a fresh draw
+            uint32_t t = UINT32_MAX;
+            while (!targets.empty()) {
+                const uint32_t c = targets.back();
+                targets.pop_back();
+                if (!has(src, c)) { t = c; break; }
+            }
+            while (t == UINT32_MAX) {
+                const uint32_t c = repeated[rng.below(repeated.size())];
+                if (c != src && !has(src, c)) t = c;
+            }
+            if (!add(src, t)) return fail(GA_ERR_CAPACITY, "holme_kim: pair buffer too small");
+            repeated.push_back(t);
+            last = t;
+            count++;
+        }
+        for (uint32_t i = 0; i < mv; i++) repeated.push_back(src);
+    }
+    *npairs = k;
+    return GA_OK;
+}
+
+ga_status ga_gen_rmat(uint32_t scale, uint64_t nsamples, double a, double b, double c, uint64_t seed,
+                      uint32_t* pairs) {
+    if (!pairs && nsamples) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    if (scale == 0 || scale > 32 || a < 0 || b < 0 || c < 0 || a + b + c > 1.0)
+        return fail(GA_ERR_INVALID_ARGUMENT, "rmat: need 1 <= scale <= 32 and a, b, c >= 0 with a + b + c <= 1");
+    // thresholds on 32-bit uniforms: quadrant 0 (a) top-left, 1 (b) top-right, 2 (c) bottom-left, 3 (d)
+    const uint64_t ta = (uint64_t)(a * 4294967296.0), tb = (uint64_t)((a + b) * 4294967296.0),
+                   tc = (uint64_t)((a + b + c) * 4294967296.0);
+    const uint64_t CHUNK = 1 << 16;
+    const int64_t nchunks = (int64_t)((nsamples + CHUNK - 1) / CHUNK);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t ch = 0; ch < nchunks; ch++) {
+        Rng rng(mix64(seed ^ mix64((uint64_t)ch + 0x51ed270b27ull)));
+        const uint64_t lo = (uint64_t)ch * CHUNK, hi = std::min<uint64_t>(nsamples, lo + CHUNK);
+        for (uint64_t s = lo; s < hi; s++) {
+            uint32_t u = 0, v = 0;
+            uint64_t bits = 0;
+            int avail = 0;
+            for (uint32_t lvl = 0; lvl < scale; lvl++) {
+                if (avail == 0) { bits = rng.next(); avail = 2; }
+                const uint64_t r = bits & 0xFFFFFFFFull;
+                bits >>= 32;
+                avail--;
+                const uint32_t q = r < ta ? 0 : (r < tb ? 1 : (r < tc ? 2 : 3));
+                u = (u << 1) | (q >> 1);
+                v = (v << 1) | (q & 1);
+            }
+            pairs[2 * s] = u;
+            pairs[2 * s + 1] = v;
+        }
+    }
+    return GA_OK;
+}
+
+ga_status ga_permute_ids(uint32_t* pairs, uint64_t npairs, uint32_t n, uint64_t seed) {
+    if (!pairs && npairs) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    std::vector<uint32_t> perm(n);
+    for (uint32_t i = 0; i < n; i++) perm[i] = i;
+    Rng rng(seed ^ 0x7065726du);
+    for (uint32_t i = n; i > 1; i--) std::swap(perm[i - 1], perm[rng.below(i)]);   // Fisher-Yates
+    bool bad = false;
+#pragma omp parallel for schedule(static) reduction(|| : bad)
+    for (int64_t i = 0; i < (int64_t)(2 * npairs); i++) {
+        if (pairs[i] >= n) { bad = true; continue; }
+        pairs[i] = perm[pairs[i]];
+    }
+    if (bad) return fail(GA_ERR_INVALID_ARGUMENT, "permute: endpoint >= n");
+    return GA_OK;
+}
+
+}  // extern "C"

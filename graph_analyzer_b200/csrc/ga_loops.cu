@@ -1,0 +1,570 @@
+// ga_loops.cu - device-resident round loops: triangle-density batch peeling and the (k, triangle)-core decomposition.
+//
+// Both loops remove a FRONTIER of vertices per round and keep tri[v] (triangles of v inside the alive subgraph)
+// up to date by decrements instead of recounting:
+//   * batch peeling (densest.h:138-160, batch_peel_loop densest.h:279-303): frontier = alive v with
+//     tri[v] * nalive * den <= 3 * (den + num) * T (the integer rule of mark_peel, kernels.cuh:443-459);
+//     the best density is tracked on the device with peel_improves' strict rule (densest.h:76-78);
+//   * cores (core_decomp_loop_inc, dsg.h:724-751): k = max(k, min over alive of tri); frontier = alive v with
+//     tri[v] <= k, core[v] = k (core_find_frontier, kernels.cuh:549-562; level rule and proof dsg.h:666-680).
+// After a frontier F is chosen, exactly the triangles with a corner in F and all corners alive-or-in-F disappear.
+// k_frontier_update enumerates, for every x in F, every triangle through x: with N(x) = N+(x) ∪ In(x) (out-list
+// and in-list of the oriented CSR) the triangles through x are {x, y, w} for y in N(x), w in N+(y) ∩ N(x), each
+// found exactly once from x (x lowest: y = middle; x middle: y = lowest; x highest: y = lowest). The triangle is
+// handled only by its smallest-id frontier corner (the owner rule of core_update_frontier, kernels.cuh:607), which
+// subtracts 1 from tri[] of its alive corners and counts it as destroyed (T -= destroyed). This reproduces the
+// recount of the reference's loops exactly, so rounds, removed_round[], best density and core[] are bit-identical.
+//
+// Round structure (one kernel boundary = one grid-wide barrier, no host sync):
+//   peel : k_peel_mark -> k_frontier_update -> k_retire_tail
+//   core : k_core_min  -> k_core_mark -> k_frontier_update -> k_retire_tail
+// The alive set is kept as a compacted id list (double-buffered, parity on the device), so late rounds scan only the
+// survivors. k_retire_tail's last block advances the round and decides whether to continue. In GA_OPT_LOOP_MODE 2
+// the round is the body of a CUDA graph conditional WHILE node (cudaGraphSetConditional from the tail), so the
+// whole loop is one graph launch; mode 1 launches the same kernels round by round and reads the 100-byte round state
+// back after each (the reference's host loop with its one sync per round).
+#include <algorithm>
+
+#include "ga_device.cuh"
+#include "ga_tc.cuh"
+
+namespace ga {
+
+constexpr uint32_t kChunk = 256;     // neighbours of a frontier vertex per update item
+constexpr int kUpdWarps = 8;
+
+enum LoopKind { LOOP_PEEL = 0, LOOP_CORE = 1 };
+
+// Device round state (one struct, read back whole by the host-driven mode).
+struct LoopScalars {
+    unsigned long long T, nalive, num, den;
+    unsigned long long best_num, best_den, destroyed;
+    uint32_t round, best_round, parity, max_rounds;
+    uint32_t alive_count[2];
+    uint32_t fcount, nitems, kcur, kround, min_tri;
+    uint32_t status, done_blocks, cont;
+    uint32_t iters;   // rounds started, counted independently of the tail (loop bound of last resort)
+};
+
+// status codes written by the device
+enum : uint32_t { LS_OK = 0, LS_NO_PROGRESS = 1, LS_ROUND_LIMIT = 2, LS_LEVEL_DOWN = 3, LS_OVER_REMOVED = 4 };
+
+}  // namespace ga
+
+struct ga_loops {
+    uint32_t* tri = nullptr;          // n
+    uint8_t* state = nullptr;         // n: 0 removed, 1 alive, 2 frontier of this round
+    uint32_t* out = nullptr;          // n: removed_round (peel) or core (core)
+    uint32_t* alive[2] = {nullptr, nullptr};
+    uint32_t* frontier = nullptr;     // n
+    uint32_t* item_x = nullptr;       // item capacity
+    uint32_t* item_c = nullptr;
+    uint64_t item_cap = 0;
+    ga::LoopScalars* sc = nullptr;    // device
+    ga::LoopScalars* h_sc = nullptr;  // pinned host copy
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    cudaGraph_t graph[2] = {nullptr, nullptr};
+    unsigned grid_scan = 1, grid_update = 1, grid_retire = 1;
+};
+
+namespace ga {
+
+__global__ void k_loop_init(uint8_t* __restrict__ state, uint32_t* __restrict__ out, uint32_t* __restrict__ alive0,
+                            uint32_t n) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        state[v] = 1;
+        out[v] = 0xFFFFFFFFu;
+        alive0[v] = v;
+    }
+}
+
+__global__ void k_loop_scalars(LoopScalars* sc, const unsigned long long* total, uint32_t n, unsigned long long num,
+                               unsigned long long den, uint32_t max_rounds) {
+    LoopScalars s = {};
+    s.T = *total;
+    s.nalive = n;
+    s.num = num;
+    s.den = den;
+    s.max_rounds = max_rounds;
+    s.alive_count[0] = n;
+    s.min_tri = 0xFFFFFFFFu;
+    s.cont = n > 0;
+    *sc = s;
+}
+
+// Appends the frontier vertex v (mark kernels): its id to frontier[], and ceil(deg(v) / kChunk) update items.
+// All 32 lanes call it; `take` marks the lanes that append. One atomic per warp for each list.
+__device__ __forceinline__ void append_frontier(bool take, uint32_t v, const uint32_t* __restrict__ rowptr,
+                                                const uint32_t* __restrict__ in_ptr, LoopScalars* sc,
+                                                uint32_t* __restrict__ frontier, uint32_t* __restrict__ item_x,
+                                                uint32_t* __restrict__ item_c, uint32_t lane) {
+    const uint32_t bal = __ballot_sync(GA_FULL_MASK, take);
+    if (!bal) return;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&sc->fcount, (uint32_t)__popc(bal));
+    base = __shfl_sync(GA_FULL_MASK, base, 0);
+    uint32_t nc = 0;
+    if (take) {
+        frontier[base + __popc(bal & ((1u << lane) - 1))] = v;
+        const uint32_t deg = rowptr[v + 1] - rowptr[v] + in_ptr[v + 1] - in_ptr[v];
+        nc = (deg + kChunk - 1) / kChunk;
+    }
+    const uint32_t incl = warp_incl_scan(nc, lane);
+    const uint32_t tot = __shfl_sync(GA_FULL_MASK, incl, 31);
+    uint32_t ib = 0;
+    if (lane == 31 && tot) ib = atomicAdd(&sc->nitems, tot);
+    ib = __shfl_sync(GA_FULL_MASK, ib, 31);
+    for (uint32_t c = 0; c < nc; c++) {
+        item_x[ib + incl - nc + c] = v;
+        item_c[ib + incl - nc + c] = c;
+    }
+}
+
+// Survivors go to the next alive list (one atomic per warp).
+__device__ __forceinline__ void append_survivor(bool keep, uint32_t v, uint32_t* __restrict__ out_list,
+                                                uint32_t* out_count, uint32_t lane) {
+    const uint32_t bal = __ballot_sync(GA_FULL_MASK, keep);
+    if (!bal) return;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(out_count, (uint32_t)__popc(bal));
+    base = __shfl_sync(GA_FULL_MASK, base, 0);
+    if (keep) out_list[base + __popc(bal & ((1u << lane) - 1))] = v;
+}
+
+// Peel round, step 1: best-density bookkeeping (peel_improves, densest.h:297) and the mark_peel rule
+// (kernels.cuh:448-451) over the alive list.
+__global__ void __launch_bounds__(256) k_peel_mark(LoopScalars* sc, const uint32_t* __restrict__ tri,
+                                                   uint8_t* __restrict__ state, uint32_t* __restrict__ removed_round,
+                                                   uint32_t* alive0, uint32_t* alive1,
+                                                   uint32_t* __restrict__ frontier, uint32_t* __restrict__ item_x,
+                                                   uint32_t* __restrict__ item_c, const uint32_t* __restrict__ rowptr,
+                                                   const uint32_t* __restrict__ in_ptr) {
+    const uint32_t p = sc->parity;
+    const uint32_t* in = p ? alive1 : alive0;
+    uint32_t* outl = p ? alive0 : alive1;
+    const uint32_t na = sc->alive_count[p];
+    const unsigned long long T = sc->T, nalive = sc->nalive, num = sc->num, den = sc->den;
+    const unsigned long long rhs = 3ull * (den + num) * T;
+    const uint32_t round = sc->round;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (sc->best_den == 0 || T * sc->best_den > sc->best_num * nalive) {
+            sc->best_num = T;
+            sc->best_den = nalive;
+            sc->best_round = round;
+        }
+    }
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x - lane; i0 < na; i0 += stride) {
+        const uint32_t i = i0 + lane;
+        const bool valid = i < na;
+        const uint32_t v = valid ? in[i] : 0;
+        bool rem = false;
+        if (valid) {
+            rem = (unsigned long long)tri[v] * nalive * den <= rhs;
+            if (rem) {
+                state[v] = 2;
+                removed_round[v] = round;
+            }
+        }
+        append_frontier(rem, v, rowptr, in_ptr, sc, frontier, item_x, item_c, lane);
+        append_survivor(valid && !rem, v, outl, &sc->alive_count[p ^ 1], lane);
+    }
+}
+
+// Core round, step 1: minimum of tri over the alive list (core_min_alive_tri, kernels.cuh:484-491).
+__global__ void __launch_bounds__(256) k_core_min(LoopScalars* sc, const uint32_t* __restrict__ tri,
+                                                  const uint32_t* alive0, const uint32_t* alive1) {
+    const uint32_t p = sc->parity;
+    const uint32_t* in = p ? alive1 : alive0;
+    const uint32_t na = sc->alive_count[p];
+    uint32_t mn = 0xFFFFFFFFu;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x)
+        mn = min(mn, tri[in[i]]);
+    mn = __reduce_min_sync(GA_FULL_MASK, mn);
+    if ((threadIdx.x & 31) == 0 && mn != 0xFFFFFFFFu) atomicMin(&sc->min_tri, mn);
+}
+
+// Core round, step 2: k = max(k, min); frontier = alive with tri <= k, core = k (core_find_frontier,
+// kernels.cuh:549-562).
+__global__ void __launch_bounds__(256) k_core_mark(LoopScalars* sc, const uint32_t* __restrict__ tri,
+                                                   uint8_t* __restrict__ state, uint32_t* __restrict__ core,
+                                                   uint32_t* alive0, uint32_t* alive1,
+                                                   uint32_t* __restrict__ frontier, uint32_t* __restrict__ item_x,
+                                                   uint32_t* __restrict__ item_c, const uint32_t* __restrict__ rowptr,
+                                                   const uint32_t* __restrict__ in_ptr) {
+    const uint32_t p = sc->parity;
+    const uint32_t* in = p ? alive1 : alive0;
+    uint32_t* outl = p ? alive0 : alive1;
+    const uint32_t na = sc->alive_count[p];
+    const uint32_t k = max(sc->kcur, sc->min_tri);
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->kround = k;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x - lane; i0 < na; i0 += stride) {
+        const uint32_t i = i0 + lane;
+        const bool valid = i < na;
+        const uint32_t v = valid ? in[i] : 0;
+        bool rem = false;
+        if (valid) {
+            rem = tri[v] <= k;
+            if (rem) {
+                state[v] = 2;
+                core[v] = k;
+            }
+        }
+        append_frontier(rem, v, rowptr, in_ptr, sc, frontier, item_x, item_c, lane);
+        append_survivor(valid && !rem, v, outl, &sc->alive_count[p ^ 1], lane);
+    }
+}
+
+// Enumerates the triangles through the frontier vertices (see the file comment). One warp per item = up to kChunk
+// consecutive entries of the virtual neighbour list N(x) = [N+(x) | In(x)]. Vertices with deg(x) <= kChunk use a
+// per-warp shared hash set of their live neighbours; larger ones test an edge {x, w} by binary search in the sorted
+// rows N+(x) and N+(w).
+__global__ void __launch_bounds__(kUpdWarps * 32) k_frontier_update(
+    LoopScalars* sc, const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ col,
+    const uint32_t* __restrict__ in_ptr, const uint32_t* __restrict__ in_src, const uint32_t* __restrict__ item_x,
+    const uint32_t* __restrict__ item_c, const uint8_t* __restrict__ state, uint32_t* __restrict__ tri) {
+    constexpr uint32_t kSlots = 2 * kChunk;   // 512 slots, load <= 1/2
+    constexpr uint32_t kBits = 9;
+    __shared__ uint32_t s_key[kUpdWarps][kSlots];
+    __shared__ uint32_t s_incl[kUpdWarps][32], s_rb[kUpdWarps][32], s_y[kUpdWarps][32];
+    __shared__ uint8_t s_sy[kUpdWarps][32];
+    __shared__ unsigned long long s_red[kUpdWarps];
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t* key = s_key[w];
+    const uint32_t nitems = sc->nitems;
+    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long destroyed = 0;
+    for (uint32_t it = gwarp; it < nitems; it += nwarps) {
+        const uint32_t x = item_x[it], c = item_c[it];
+        const uint32_t xb = rowptr[x], dout = rowptr[x + 1] - xb;
+        const uint32_t ib = in_ptr[x], din = in_ptr[x + 1] - ib;
+        const uint32_t deg = dout + din;
+        const bool local = deg <= kChunk;
+        if (local) {
+            for (uint32_t s = lane; s < kSlots; s += 32) key[s] = GA_EMPTY;
+            __syncwarp();
+            for (uint32_t q = lane; q < deg; q += 32) {
+                const uint32_t y = q < dout ? col[xb + q] : in_src[ib + q - dout];
+                if (state[y] == 0) continue;
+                uint32_t h = hash_slot(y, kBits);
+                while (atomicCAS(&key[h], GA_EMPTY, y) != GA_EMPTY) h = (h + 1) & (kSlots - 1);
+            }
+            __syncwarp();
+        }
+        const uint32_t q0 = c * kChunk, q1 = min(deg, q0 + kChunk);
+        for (uint32_t qb = q0; qb < q1; qb += 32) {
+            const uint32_t q = qb + lane;
+            uint32_t d = 0, rb = 0, y = 0;
+            uint8_t sy = 0;
+            if (q < q1) {
+                y = q < dout ? col[xb + q] : in_src[ib + q - dout];
+                sy = state[y];
+                if (sy) {
+                    rb = rowptr[y];
+                    d = rowptr[y + 1] - rb;
+                }
+            }
+            const uint32_t incl = warp_incl_scan(d, lane);
+            const uint32_t tot = __shfl_sync(GA_FULL_MASK, incl, 31);
+            s_incl[w][lane] = incl;
+            s_rb[w][lane] = rb;
+            s_y[w][lane] = y;
+            s_sy[w][lane] = sy;
+            __syncwarp();
+            uint32_t owner = 0;
+            for (uint32_t p = lane; p < tot; p += 32) {
+                while (s_incl[w][owner] <= p) owner++;
+                const uint32_t wv = col[s_rb[w][owner] + (p - (owner ? s_incl[w][owner - 1] : 0u))];
+                bool hit = false;
+                if (local) {
+                    uint32_t h = hash_slot(wv, kBits);
+                    for (;;) {
+                        const uint32_t kk = key[h];
+                        if (kk == wv) { hit = true; break; }
+                        if (kk == GA_EMPTY) break;
+                        h = (h + 1) & (kSlots - 1);
+                    }
+                } else if (wv != x && state[wv] != 0) {
+                    const uint32_t j = lower_bound_u32(col, xb, xb + dout, wv);
+                    hit = j < xb + dout && col[j] == wv;
+                    if (!hit) {
+                        const uint32_t wb = rowptr[wv], we = rowptr[wv + 1];
+                        const uint32_t j2 = lower_bound_u32(col, wb, we, x);
+                        hit = j2 < we && col[j2] == x;
+                    }
+                }
+                if (hit) {
+                    const uint32_t yv = s_y[w][owner];
+                    const uint8_t syv = s_sy[w][owner], sw = state[wv];
+                    const bool owned = !((syv == 2 && yv < x) || (sw == 2 && wv < x));
+                    if (owned) {
+                        destroyed++;
+                        if (syv == 1) atomicSub(&tri[yv], 1u);
+                        if (sw == 1) atomicSub(&tri[wv], 1u);
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+    destroyed = warp_sum_u64(destroyed);
+    if (lane == 0) s_red[w] = destroyed;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int i = 0; i < kUpdWarps; i++) t += s_red[i];
+        if (t) atomicAdd(&sc->destroyed, t);
+    }
+}
+
+// Retires the frontier (state 2 -> 0); the last block to finish closes the round: nalive -= |F|, T -= destroyed,
+// checks (densest.h:298, dsg.h:744), resets the per-round counters, flips the alive-list parity and sets the loop
+// condition (cudaGraphSetConditional when running as a graph body).
+template <int KIND>
+__global__ void __launch_bounds__(256) k_retire_tail(LoopScalars* sc, uint8_t* __restrict__ state,
+                                                     const uint32_t* __restrict__ frontier,
+                                                     cudaGraphConditionalHandle handle, int use_handle) {
+    __shared__ bool s_last;
+    const uint32_t F = sc->fcount;
+    // independent bound: block 0 counts every execution of this kernel; past max_rounds + 1 the loop is forced to
+    // stop even if the round bookkeeping below were broken (a WHILE node keeps its last condition value otherwise)
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const uint32_t it = atomicAdd(&sc->iters, 1u) + 1;
+        if (it > sc->max_rounds + 1) {
+            atomicMax(&sc->status, (uint32_t)LS_ROUND_LIMIT);
+            sc->cont = 0;
+            if (use_handle) cudaGraphSetConditional(handle, 0);
+        }
+    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x)
+        state[frontier[i]] = 0;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(&sc->done_blocks, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last || threadIdx.x != 0) return;
+    __threadfence();
+    LoopScalars s = *sc;   // written by earlier kernels of this round (visible at the kernel boundary)
+    uint32_t status = s.status;
+    if (F == 0 && s.nalive > 0) status = LS_NO_PROGRESS;
+    if (F > s.nalive) status = LS_OVER_REMOVED;
+    if (KIND == LOOP_CORE) {
+        if (s.kround < s.kcur) status = LS_LEVEL_DOWN;
+        s.kcur = s.kround;
+    }
+    if (s.destroyed > s.T) status = LS_OVER_REMOVED;
+    s.nalive -= min((unsigned long long)F, s.nalive);
+    s.T -= min(s.destroyed, s.T);
+    s.round += 1;
+    s.parity ^= 1;
+    s.alive_count[s.parity ^ 1] = 0;   // the next round's output list
+    s.fcount = 0;
+    s.nitems = 0;
+    s.destroyed = 0;
+    s.done_blocks = 0;
+    s.min_tri = 0xFFFFFFFFu;
+    if (status == LS_OK && s.nalive > 0 && s.round >= s.max_rounds) status = LS_ROUND_LIMIT;
+    s.status = status;
+    s.cont = (status == LS_OK && s.nalive > 0 && s.iters <= s.max_rounds) ? 1u : 0u;
+    *sc = s;
+    if (use_handle) cudaGraphSetConditional(handle, s.cont);
+}
+
+// ---- host side --------------------------------------------------------------------------------------------------
+
+static ga_status ensure_loops(ga_graph* g) {
+    if (g->loops) return GA_OK;
+    ga_loops* L = new ga_loops();
+    g->loops = L;
+    const uint32_t n = g->n;
+    GA_TRY(dalloc(g, &L->tri, n));
+    GA_TRY(dalloc(g, &L->state, n));
+    GA_TRY(dalloc(g, &L->out, n));
+    GA_TRY(dalloc(g, &L->alive[0], n));
+    GA_TRY(dalloc(g, &L->alive[1], n));
+    GA_TRY(dalloc(g, &L->frontier, n));
+    // every vertex enters one frontier per run and brings ceil(deg / kChunk) items
+    L->item_cap = (uint64_t)n + (2ull * g->m) / kChunk + 1;
+    GA_TRY(dalloc(g, &L->item_x, L->item_cap));
+    GA_TRY(dalloc(g, &L->item_c, L->item_cap));
+    GA_TRY(dalloc(g, &L->sc, 1));
+    GA_CUDA(cudaMallocHost((void**)&L->h_sc, sizeof(LoopScalars)));
+    // fixed launch shapes (the graph body is captured once): grid-stride scans, persistent update grid
+    int occ = 0;
+    GA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_frontier_update, kUpdWarps * 32, 0));
+    L->grid_scan = (unsigned)g->sm_count * 4;
+    L->grid_update = (unsigned)g->sm_count * (unsigned)std::max(occ, 1);
+    L->grid_retire = (unsigned)g->sm_count;
+    return GA_OK;
+}
+
+void destroy_loops(ga_graph* g) {
+    ga_loops* L = g->loops;
+    if (!L) return;
+    for (int k = 0; k < 2; k++) {
+        if (L->exec[k]) cudaGraphExecDestroy(L->exec[k]);
+        if (L->graph[k]) cudaGraphDestroy(L->graph[k]);
+    }
+    if (L->h_sc) cudaFreeHost(L->h_sc);
+    delete L;   // device buffers belong to g->allocations
+    g->loops = nullptr;
+}
+
+// Enqueues one round on `st` (kernel parameters are fixed, everything per-round lives in *sc).
+template <int KIND>
+static ga_status enqueue_round(ga_graph* g, cudaStream_t st, cudaGraphConditionalHandle h, int use_h) {
+    ga_loops* L = g->loops;
+    if (KIND == LOOP_PEEL) {
+        k_peel_mark<<<L->grid_scan, 256, 0, st>>>(L->sc, L->tri, L->state, L->out, L->alive[0], L->alive[1], L->frontier,
+                                             L->item_x, L->item_c, g->rowptr, g->in_ptr);
+    } else {
+        k_core_min<<<L->grid_scan, 256, 0, st>>>(L->sc, L->tri, L->alive[0], L->alive[1]);
+        k_core_mark<<<L->grid_scan, 256, 0, st>>>(L->sc, L->tri, L->state, L->out, L->alive[0], L->alive[1], L->frontier,
+                                             L->item_x, L->item_c, g->rowptr, g->in_ptr);
+    }
+    k_frontier_update<<<L->grid_update, kUpdWarps * 32, 0, st>>>(L->sc, g->rowptr, g->col, g->in_ptr, g->in_src,
+                                                            L->item_x, L->item_c, L->state, L->tri);
+    k_retire_tail<KIND><<<L->grid_retire, 256, 0, st>>>(L->sc, L->state, L->frontier, h, use_h);
+    GA_CUDA(cudaGetLastError());
+    return GA_OK;
+}
+
+// Builds (once per graph and loop kind) the CUDA graph: a conditional WHILE node whose body is one round.
+template <int KIND>
+static ga_status ensure_graph(ga_graph* g) {
+    ga_loops* L = g->loops;
+    if (L->exec[KIND]) return GA_OK;
+    cudaGraph_t graph;
+    GA_CUDA(cudaGraphCreate(&graph, 0));
+    L->graph[KIND] = graph;
+    cudaGraphConditionalHandle handle;
+    GA_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams params = {};
+    params.type = cudaGraphNodeTypeConditional;
+    params.conditional.handle = handle;
+    params.conditional.type = cudaGraphCondTypeWhile;
+    params.conditional.size = 1;
+    cudaGraphNode_t node;
+    GA_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &params));
+    cudaGraph_t body = params.conditional.phGraph_out[0];
+    cudaStream_t cap;
+    GA_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    ga_status s = GA_OK;
+    if (cudaStreamBeginCaptureToGraph(cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+        cudaSuccess) {
+        s = fail(GA_ERR_CUDA, "cudaStreamBeginCaptureToGraph failed");
+    } else {
+        s = enqueue_round<KIND>(g, cap, handle, 1);
+        cudaGraph_t out = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(cap, &out);
+        if (s == GA_OK && e != cudaSuccess) s = fail(GA_ERR_CUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(e));
+    }
+    cudaStreamDestroy(cap);
+    GA_TRY(s);
+    GA_CUDA(cudaGraphInstantiate(&L->exec[KIND], graph, 0));
+    return GA_OK;
+}
+
+// Common driver: init (full per-vertex count, state), then the round loop in the selected mode.
+template <int KIND>
+static ga_status run_loop(ga_graph* g, uint64_t num, uint64_t den, LoopScalars* result) {
+    GA_TRY(prepare(g));
+    GA_TRY(ensure_loops(g));
+    ga_loops* L = g->loops;
+    cudaStream_t st = g->stream;
+    const uint32_t n = g->n;
+    // tri[] = triangles per vertex on the whole graph (uint32 counters; T < 2^32 is checked below)
+    TcArgs<unsigned int> a{};
+    a.total = g->d_scalars;
+    a.vsup = L->tri;
+    GA_TRY((run_tc<TC_VSUP, false, unsigned int>(g, a, true)));
+    if (n) {
+        k_loop_init<<<grid_for(n, 256), 256, 0, st>>>(L->state, L->out, L->alive[0], n);
+        GA_CUDA(cudaGetLastError());
+    }
+    GA_CUDA(cudaMemcpyAsync(g->h_scalars, g->d_scalars, 8, cudaMemcpyDeviceToHost, st));
+    GA_CUDA(cudaStreamSynchronize(st));
+    const uint64_t T0 = g->h_scalars[0];
+    if (T0 >= (1ull << 32))
+        return fail(GA_ERR_ARITH, "triangle count %llu >= 2^32: uint32 tri[] counters could overflow",
+                    (unsigned long long)T0);
+    if (KIND == LOOP_PEEL) {
+        // peel_arith_ok (densest.h:65-72) with the device count as T0
+        if (n > 0 && T0 > UINT64_MAX / ((uint64_t)n * den))
+            return fail(GA_ERR_ARITH, "tri*nalive*den could overflow uint64");
+        if (T0 > UINT64_MAX / (3ull * (den + num))) return fail(GA_ERR_ARITH, "3*(den+num)*T could overflow uint64");
+    }
+    const uint64_t cap = g->opt_max_rounds ? (uint64_t)g->opt_max_rounds : (uint64_t)n + 1;
+    const uint32_t max_rounds = (uint32_t)std::min<uint64_t>(cap, UINT32_MAX);
+    k_loop_scalars<<<1, 1, 0, st>>>(L->sc, g->d_scalars, n, num, den, max_rounds);
+    GA_CUDA(cudaGetLastError());
+    if (n > 0) {
+        const bool graph_mode = g->opt_loop_mode != 1;
+        if (graph_mode) {
+            GA_TRY(ensure_graph<KIND>(g));
+            GA_CUDA(cudaGraphLaunch(L->exec[KIND], st));
+        } else {
+            for (uint64_t r = 0;; r++) {
+                GA_TRY(enqueue_round<KIND>(g, st, 0, 0));
+                GA_CUDA(cudaMemcpyAsync(L->h_sc, L->sc, sizeof(LoopScalars), cudaMemcpyDeviceToHost, st));
+                GA_CUDA(cudaStreamSynchronize(st));
+                if (!L->h_sc->cont) break;
+                if (r > (uint64_t)max_rounds + 1) return fail(GA_ERR_ROUND_LIMIT, "host loop bound reached");
+            }
+        }
+    }
+    GA_CUDA(cudaMemcpyAsync(L->h_sc, L->sc, sizeof(LoopScalars), cudaMemcpyDeviceToHost, st));
+    GA_CUDA(cudaStreamSynchronize(st));
+    *result = *L->h_sc;
+    switch (result->status) {
+        case LS_OK: break;
+        case LS_ROUND_LIMIT: return fail(GA_ERR_ROUND_LIMIT, "round cap %u reached", result->max_rounds);
+        case LS_NO_PROGRESS: return fail(GA_ERR_DEVICE_CHECK, "no vertex removed in round %u", result->round - 1);
+        case LS_LEVEL_DOWN: return fail(GA_ERR_DEVICE_CHECK, "core level decreased in round %u", result->round - 1);
+        default: return fail(GA_ERR_DEVICE_CHECK, "removed more vertices than alive (round %u)", result->round - 1);
+    }
+    return GA_OK;
+}
+
+}  // namespace ga
+
+using namespace ga;
+
+extern "C" {
+
+ga_status ga_batch_peel(ga_graph* g, uint64_t num, uint64_t den, ga_peel_result* res, uint32_t* removed_round) {
+    if (!g || !res) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    if (den < 1 || den > (1ull << 20) || num > (1ull << 20))
+        return fail(GA_ERR_INVALID_ARGUMENT, "eps = num/den needs 1 <= den <= 2^20 and num <= 2^20");
+    GA_TRY(use_device(g));
+    LoopScalars s;
+    GA_TRY(run_loop<LOOP_PEEL>(g, num, den, &s));
+    res->best_num = s.best_num;
+    res->best_den = s.best_den;
+    res->best_round = s.best_round;
+    res->rounds = s.round;
+    if (removed_round && g->n) {
+        GA_CUDA(cudaMemcpyAsync(removed_round, g->loops->out, (size_t)g->n * 4, cudaMemcpyDeviceToHost, g->stream));
+        GA_CUDA(cudaStreamSynchronize(g->stream));
+    }
+    return GA_OK;
+}
+
+ga_status ga_core_decomposition(ga_graph* g, uint32_t* core, ga_core_result* res) {
+    if (!g || !res) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    GA_TRY(use_device(g));
+    LoopScalars s;
+    GA_TRY(run_loop<LOOP_CORE>(g, 0, 1, &s));
+    res->kmax = s.kcur;
+    res->rounds = s.round;
+    if (core && g->n) {
+        GA_CUDA(cudaMemcpyAsync(core, g->loops->out, (size_t)g->n * 4, cudaMemcpyDeviceToHost, g->stream));
+        GA_CUDA(cudaStreamSynchronize(g->stream));
+    }
+    return GA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,478 @@
+// ga_tc.cu - triangle counting and triangle support on the oriented CSR (sm_100a).
+//
+// What is computed is the reference's sum (graph.h:15-18, kernels.cuh:3): T = sum over oriented edges u->v of
+// |N+(u) ∩ N+(v)|, every triangle {a,b,c} with a->b, a->c, b->c found exactly once. The reference's kernels v1-v9
+// (kernels.cuh:53-358) walk that sum edge by edge. Here it is reorganised around the MIDDLE vertex b of each
+// triangle (the "anchor"):
+//
+//     T = sum over anchors v of sum over in-edges u->v of |N+(u) ∩ N+(v)|
+//
+// N+(v) is loaded ONCE into a shared-memory hash set and every in-neighbour's list N+(u) is streamed past it (probe).
+// Probe work is sum_v sum_{u->v} d+(u) = sum_u d+(u)^2, the smaller of the two sides of the merge sum (the other
+// side, sum_{u->v} d+(v), is about twice as large on power-law graphs), and each probe is one or two shared-memory
+// loads instead of a merge step or a binary search in global memory.
+//
+// Scheduler (degree-binned, one persistent launch):
+//   * work items = slices of an anchor's in-edge list with bounded probe work (built in ga_graph.cu);
+//   * HEAVY bin: anchors with out-degree > light_max_deg. The whole block (8 warps) shares one hash set of N+(v) in
+//     dynamic shared memory and splits the in-edges; anchors whose set does not fit fall back to binary search in
+//     the sorted global row;
+//   * LIGHT bin: every warp owns a 512-slot hash set and takes items on its own;
+//   * blocks drain the heavy queue first, then the light queue (one atomic per item fetch).
+// Inside an item a warp processes 32 in-edges at a time: lane l loads the l-th source, a warp scan of the list
+// lengths flattens the 32 lists into one probe sequence, and lane p takes probes p, p+32, ... so lanes stay busy
+// whatever the list lengths are (load-balanced search: each lane advances its owner index monotonically).
+//
+// Results per triangle (u->v in-edge, x common, x at position e of N+(u) and j of N+(v)):
+//   COUNT: T only, one 64-bit atomic per block at the end.
+//   VSUP : per-vertex counts: x through a per-slot shared counter (flushed once per item), u through a per-in-edge
+//          shared counter (flushed once per 32 in-edges), v through a warp reduction (once per item).
+//   ESUP : per-edge counts indexed like col (for_each_triangle's (e_uv, e_ux, e_vx), dsg.h:67-79): e_uv and e_vx
+//          through shared counters as above, e_ux with one global atomic per triangle.
+//   ALIVE: restricts everything to the subgraph induced by alive[] (tc_per_vertex_alive, kernels.cuh:399-425).
+#include <algorithm>
+
+#include "ga_device.cuh"
+#include "ga_tc.cuh"
+
+namespace ga {
+
+constexpr int kWarps = 8;                 // warps per block of the hash kernel
+constexpr int kThreads = kWarps * 32;
+constexpr int kLightSlots = 512;          // per-warp hash set: anchors with out-degree <= 256 (load <= 1/2)
+
+template <int MODE>
+struct SlotLayout {   // 32-bit words per hash slot: key, +count (VSUP/ESUP), +position (ESUP)
+    static constexpr int words = 1 + (MODE >= TC_VSUP ? 1 : 0) + (MODE == TC_ESUP ? 1 : 0);
+};
+
+// Shared memory of the light phase per warp: slots * words + incl[32] + rb[32] + ecnt[32].
+template <int MODE>
+constexpr int light_warp_words() { return kLightSlots * SlotLayout<MODE>::words + 96; }
+
+template <int MODE, bool ALIVE, class CT>
+__device__ __forceinline__ void on_hit(const TcArgs<CT>& a, uint32_t* cnt, uint32_t h, uint32_t* ecnt,
+                                       uint32_t owner, uint32_t e) {
+    if (MODE >= TC_VSUP) {
+        atomicAdd(&cnt[h], 1u);
+        atomicAdd(&ecnt[owner], 1u);
+    }
+    if (MODE == TC_ESUP) atomicAdd(&a.esup[e], 1u);
+}
+
+// Processes in-edges [kb, k1) of anchor v in batches of 32 (one warp), probing a hash set (key/cnt, 2^bits slots)
+// or, when `global` is set, binary searching the sorted row N+(v) = col[vb, vb + dv). `stride` = 32 * warps that
+// share the item. Returns the hits of this lane.
+template <int MODE, bool ALIVE, class CT>
+__device__ __forceinline__ unsigned long long probe_in_edges(
+    const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ col, const uint32_t* __restrict__ in_src,
+    const uint32_t* __restrict__ in_eid, const TcArgs<CT>& a, uint32_t kb, uint32_t k1, uint32_t stride,
+    const uint32_t* key, uint32_t* cnt, uint32_t bits, bool global, uint32_t vb, uint32_t dv, uint32_t* s_incl,
+    uint32_t* s_rb, uint32_t* s_ecnt, uint32_t lane) {
+    unsigned long long hits = 0;
+    const uint32_t mask = (1u << bits) - 1;
+    for (; kb < k1; kb += stride) {
+        const uint32_t k = kb + lane;
+        uint32_t d = 0, rb = 0, u = 0;
+        if (k < k1) {
+            u = in_src[k];
+            if (!ALIVE || a.alive[u]) {
+                rb = rowptr[u];
+                d = rowptr[u + 1] - rb;
+            }
+        }
+        const uint32_t incl = warp_incl_scan(d, lane);
+        const uint32_t tot = __shfl_sync(GA_FULL_MASK, incl, 31);
+        s_incl[lane] = incl;
+        s_rb[lane] = rb;
+        __syncwarp();
+        uint32_t owner = 0;
+        for (uint32_t p = lane; p < tot; p += 32) {
+            while (s_incl[owner] <= p) owner++;
+            const uint32_t e = s_rb[owner] + (p - (owner ? s_incl[owner - 1] : 0u));
+            const uint32_t x = col[e];
+            if (!global) {
+                uint32_t h = hash_slot(x, bits);
+                for (;;) {
+                    const uint32_t kk = key[h];
+                    if (kk == x) {
+                        hits++;
+                        on_hit<MODE, ALIVE, CT>(a, cnt, h, s_ecnt, owner, e);
+                        break;
+                    }
+                    if (kk == GA_EMPTY) break;
+                    h = (h + 1) & mask;
+                }
+            } else {
+                const uint32_t j = lower_bound_u32(col, vb, vb + dv, x);
+                if (j < vb + dv && col[j] == x && (!ALIVE || a.alive[x])) {
+                    hits++;
+                    if (MODE >= TC_VSUP) atomicAdd(&s_ecnt[owner], 1u);
+                    if (MODE == TC_VSUP) atomicAdd(&a.vsup[x], (CT)1);
+                    if (MODE == TC_ESUP) {
+                        atomicAdd(&a.esup[e], 1u);
+                        atomicAdd(&a.esup[j], 1u);
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        if (MODE >= TC_VSUP) {
+            const uint32_t c = s_ecnt[lane];
+            if (c) {
+                if (MODE == TC_VSUP) atomicAdd(&a.vsup[u], (CT)c);
+                else atomicAdd(&a.esup[in_eid[k]], c);
+                s_ecnt[lane] = 0;
+            }
+        }
+        __syncwarp();
+    }
+    return hits;
+}
+
+// Table size for an anchor with dv out-neighbours: smallest power of two >= 2 dv, at least 32.
+__device__ __forceinline__ uint32_t table_bits(uint32_t dv) {
+    uint32_t b = 5;
+    while ((1u << b) < 2 * dv) b++;
+    return b;
+}
+
+// Clears 2^bits slots and inserts the (alive) members of N+(v); tid/nthr cover the cooperating threads.
+template <int MODE, bool ALIVE, class CT>
+__device__ __forceinline__ void build_table(const uint32_t* __restrict__ col, const TcArgs<CT>& a, uint32_t vb,
+                                            uint32_t dv, uint32_t* key, uint32_t* cnt, uint32_t* pos, uint32_t bits,
+                                            uint32_t tid, uint32_t nthr, bool sync_block) {
+    const uint32_t S = 1u << bits, mask = S - 1;
+    for (uint32_t s = tid; s < S; s += nthr) {
+        key[s] = GA_EMPTY;
+        if (MODE >= TC_VSUP) cnt[s] = 0;
+    }
+    if (sync_block) __syncthreads(); else __syncwarp();
+    for (uint32_t i = tid; i < dv; i += nthr) {
+        const uint32_t x = col[vb + i];
+        if (ALIVE && !a.alive[x]) continue;
+        uint32_t h = hash_slot(x, bits);
+        while (atomicCAS(&key[h], GA_EMPTY, x) != GA_EMPTY) h = (h + 1) & mask;
+        if (MODE == TC_ESUP) pos[h] = i;
+    }
+    if (sync_block) __syncthreads(); else __syncwarp();
+}
+
+// Adds the per-slot counters of an item to the outputs (x's vertex count or edge v->x's count).
+template <int MODE, class CT>
+__device__ __forceinline__ void flush_table(const TcArgs<CT>& a, uint32_t vb, const uint32_t* key,
+                                            const uint32_t* cnt, const uint32_t* pos, uint32_t bits, uint32_t tid,
+                                            uint32_t nthr) {
+    if (MODE < TC_VSUP) return;
+    const uint32_t S = 1u << bits;
+    for (uint32_t s = tid; s < S; s += nthr) {
+        const uint32_t c = cnt[s];
+        if (c) {
+            if (MODE == TC_VSUP) atomicAdd(&a.vsup[key[s]], (CT)c);
+            else atomicAdd(&a.esup[vb + pos[s]], c);
+        }
+    }
+}
+
+template <int MODE, bool ALIVE, class CT>
+__global__ void __launch_bounds__(kThreads) k_tc_hash(const uint32_t* __restrict__ rowptr,
+                                                      const uint32_t* __restrict__ col,
+                                                      const uint32_t* __restrict__ in_src,
+                                                      const uint32_t* __restrict__ in_eid, ga_items heavy,
+                                                      ga_items light, uint32_t heavy_bits_max,
+                                                      uint32_t* __restrict__ queue, TcArgs<CT> a) {
+    extern __shared__ uint32_t smem[];
+    __shared__ uint32_t s_item;
+    __shared__ unsigned long long s_red[kWarps];
+    constexpr int W = SlotLayout<MODE>::words;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long hits = 0;
+
+    // ---- heavy bin: one block per item, table of up to 2^heavy_bits_max slots shared by the block ----
+    {
+        const uint32_t Smax = 1u << heavy_bits_max;
+        uint32_t* key = smem;
+        uint32_t* cnt = key + Smax;
+        uint32_t* pos = cnt + (MODE >= TC_VSUP ? Smax : 0);
+        uint32_t* wbase = smem + (size_t)Smax * W + warp * 96;
+        uint32_t *s_incl = wbase, *s_rb = wbase + 32, *s_ecnt = wbase + 64;
+        s_ecnt[lane] = 0;
+        for (;;) {
+            if (threadIdx.x == 0) s_item = atomicAdd(&queue[0], 1u);
+            __syncthreads();
+            const uint32_t item = s_item;
+            __syncthreads();
+            if (item >= heavy.count) break;
+            const uint32_t v = heavy.v[item];
+            if (ALIVE && !a.alive[v]) continue;
+            const uint32_t vb = rowptr[v], dv = rowptr[v + 1] - vb;
+            const uint32_t bits = table_bits(dv);
+            const bool global = bits > heavy_bits_max;
+            if (!global) build_table<MODE, ALIVE, CT>(col, a, vb, dv, key, cnt, pos, bits, threadIdx.x, kThreads, true);
+            const unsigned long long h = probe_in_edges<MODE, ALIVE, CT>(
+                rowptr, col, in_src, in_eid, a, heavy.k0[item] + warp * 32, heavy.k1[item], kWarps * 32, key, cnt,
+                bits, global, vb, dv, s_incl, s_rb, s_ecnt, lane);
+            hits += h;
+            if (MODE == TC_VSUP) {
+                const unsigned long long t = warp_sum_u64(h);
+                if (lane == 0 && t) atomicAdd(&a.vsup[v], (CT)t);
+            }
+            __syncthreads();
+            if (!global) flush_table<MODE, CT>(a, vb, key, cnt, pos, bits, threadIdx.x, kThreads);
+            __syncthreads();
+        }
+    }
+    // ---- light bin: one warp per item, private 512-slot table ----
+    {
+        constexpr int PW = light_warp_words<MODE>();
+        uint32_t* key = smem + warp * PW;
+        uint32_t* cnt = key + kLightSlots;
+        uint32_t* pos = cnt + (MODE >= TC_VSUP ? kLightSlots : 0);
+        uint32_t* s_incl = key + kLightSlots * W;
+        uint32_t *s_rb = s_incl + 32, *s_ecnt = s_incl + 64;
+        s_ecnt[lane] = 0;
+        __syncwarp();
+        for (;;) {
+            uint32_t item = 0;
+            if (lane == 0) item = atomicAdd(&queue[1], 1u);
+            item = __shfl_sync(GA_FULL_MASK, item, 0);
+            if (item >= light.count) break;
+            const uint32_t v = light.v[item];
+            if (ALIVE && !a.alive[v]) continue;
+            const uint32_t vb = rowptr[v], dv = rowptr[v + 1] - vb;
+            const uint32_t bits = table_bits(dv);   // dv <= 256 -> bits <= 9
+            build_table<MODE, ALIVE, CT>(col, a, vb, dv, key, cnt, pos, bits, lane, 32, false);
+            const unsigned long long h = probe_in_edges<MODE, ALIVE, CT>(rowptr, col, in_src, in_eid, a,
+                                                                          light.k0[item], light.k1[item], 32, key,
+                                                                          cnt, bits, false, vb, dv, s_incl, s_rb,
+                                                                          s_ecnt, lane);
+            hits += h;
+            if (MODE == TC_VSUP) {
+                const unsigned long long t = warp_sum_u64(h);
+                if (lane == 0 && t) atomicAdd(&a.vsup[v], (CT)t);
+            }
+            __syncwarp();
+            flush_table<MODE, CT>(a, vb, key, cnt, pos, bits, lane, 32);
+            __syncwarp();
+        }
+    }
+    // ---- one 64-bit atomic per block ----
+    hits = warp_sum_u64(hits);
+    if (lane == 0) s_red[warp] = hits;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < kWarps; w++) t += s_red[w];
+        if (t) atomicAdd(a.total, t);
+    }
+}
+
+// Plain form (GA_OPT_TC_KERNEL = 1): one thread per oriented edge, two-pointer merge of N+(u) and N+(v), one
+// atomic per triangle and corner - the structure of the reference's v1 / tc_per_vertex_alive (kernels.cuh:53-69,
+// 399-425), kept as the one-kernel-per-launch baseline.
+template <int MODE, bool ALIVE, class CT>
+__global__ void __launch_bounds__(256) k_tc_plain(const uint32_t* __restrict__ rowptr,
+                                                  const uint32_t* __restrict__ col,
+                                                  const uint32_t* __restrict__ src, uint32_t m, TcArgs<CT> a) {
+    unsigned long long local = 0;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
+        const uint32_t u = src[e], v = col[e];
+        if (ALIVE && (!a.alive[u] || !a.alive[v])) continue;
+        uint32_t i = rowptr[u], iend = rowptr[u + 1], j = rowptr[v], jend = rowptr[v + 1];
+        while (i < iend && j < jend) {
+            const uint32_t x = col[i], y = col[j];
+            if (x < y) i++;
+            else if (x > y) j++;
+            else {
+                if (!ALIVE || a.alive[x]) {
+                    local++;
+                    if (MODE == TC_VSUP) {
+                        atomicAdd(&a.vsup[u], (CT)1);
+                        atomicAdd(&a.vsup[v], (CT)1);
+                        atomicAdd(&a.vsup[x], (CT)1);
+                    }
+                    if (MODE == TC_ESUP) {
+                        atomicAdd(&a.esup[e], 1u);
+                        atomicAdd(&a.esup[i], 1u);
+                        atomicAdd(&a.esup[j], 1u);
+                    }
+                }
+                i++;
+                j++;
+            }
+        }
+    }
+    local = warp_sum_u64(local);
+    if ((threadIdx.x & 31) == 0 && local) atomicAdd(a.total, local);
+}
+
+// ---- host launchers ---------------------------------------------------------------------------------------------
+
+template <int MODE>
+static size_t hash_smem_bytes(uint32_t heavy_bits) {
+    const size_t heavy = ((size_t)SlotLayout<MODE>::words << heavy_bits) + kWarps * 96;
+    const size_t light = (size_t)kWarps * light_warp_words<MODE>();
+    return 4 * std::max(heavy, light);
+}
+
+static uint32_t heavy_bits_for(const ga_graph* g, int mode) {
+    // largest table that keeps the block within 200 KB of dynamic shared memory
+    const int words = 1 + (mode >= TC_VSUP) + (mode == TC_ESUP);
+    uint32_t cap = 5;
+    while ((((size_t)words << (cap + 1)) + kWarps * 96) * 4 <= 200 * 1024) cap++;
+    if (g->heavy_bits_cap) cap = std::min(cap, g->heavy_bits_cap);
+    uint32_t need = 5;
+    while ((1u << need) < 2 * g->heavy.max_dv) need++;
+    return std::min(need, cap);
+}
+
+template <int MODE, bool ALIVE, class CT>
+static ga_status launch_hash(ga_graph* g, const TcArgs<CT>& a) {
+    const uint32_t hb = heavy_bits_for(g, MODE);
+    const size_t smem = hash_smem_bytes<MODE>(hb);
+    auto kern = k_tc_hash<MODE, ALIVE, CT>;
+    GA_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 0;
+    GA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, smem));
+    occ = std::max(occ, 1);
+    const uint64_t want = std::max<uint64_t>(g->heavy.count, (g->light.count + kWarps - 1) / kWarps);
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)g->sm_count * occ, want));
+    GA_CUDA(cudaMemsetAsync(g->d_queue, 0, 8 * sizeof(uint32_t), g->stream));
+    kern<<<grid, kThreads, smem, g->stream>>>(g->rowptr, g->col, g->in_src, g->in_eid, g->heavy, g->light, hb,
+                                              g->d_queue, a);
+    GA_CUDA(cudaGetLastError());
+    return GA_OK;
+}
+
+template <int MODE, bool ALIVE, class CT>
+static ga_status launch_plain(ga_graph* g, const TcArgs<CT>& a) {
+    if (!g->m) return GA_OK;
+    int occ = 0;
+    GA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tc_plain<MODE, ALIVE, CT>, 256, 0));
+    const unsigned grid = grid_for(g->m, 256, (unsigned)g->sm_count * std::max(occ, 1) * 4);
+    k_tc_plain<MODE, ALIVE, CT><<<grid, 256, 0, g->stream>>>(g->rowptr, g->col, g->src, g->m, a);
+    GA_CUDA(cudaGetLastError());
+    return GA_OK;
+}
+
+template <int MODE, bool ALIVE, class CT>
+ga_status run_tc(ga_graph* g, const TcArgs<CT>& a, bool zero_outputs) {
+    GA_TRY(prepare(g));
+    cudaStream_t st = g->stream;
+    if (zero_outputs) {
+        GA_CUDA(cudaMemsetAsync(a.total, 0, sizeof(unsigned long long), st));
+        if (MODE == TC_VSUP && g->n) GA_CUDA(cudaMemsetAsync(a.vsup, 0, (size_t)g->n * sizeof(CT), st));
+        if (MODE == TC_ESUP && g->m) GA_CUDA(cudaMemsetAsync(a.esup, 0, (size_t)g->m * sizeof(uint32_t), st));
+    }
+    if (g->opt_tc_kernel == 1) return launch_plain<MODE, ALIVE, CT>(g, a);
+    if (g->heavy.count == 0 && g->light.count == 0) return GA_OK;
+    return launch_hash<MODE, ALIVE, CT>(g, a);
+}
+
+template ga_status run_tc<TC_COUNT, false, unsigned int>(ga_graph*, const TcArgs<unsigned int>&, bool);
+template ga_status run_tc<TC_VSUP, false, unsigned long long>(ga_graph*, const TcArgs<unsigned long long>&, bool);
+template ga_status run_tc<TC_VSUP, false, unsigned int>(ga_graph*, const TcArgs<unsigned int>&, bool);
+template ga_status run_tc<TC_VSUP, true, unsigned int>(ga_graph*, const TcArgs<unsigned int>&, bool);
+template ga_status run_tc<TC_ESUP, false, unsigned int>(ga_graph*, const TcArgs<unsigned int>&, bool);
+
+}  // namespace ga
+
+using namespace ga;
+
+namespace {
+
+// Device buffer released at scope exit (stream-ordered).
+struct Scratch {
+    void* p = nullptr;
+    cudaStream_t st = nullptr;
+    ~Scratch() { if (p) cudaFreeAsync(p, st); }
+};
+
+ga_status read_total(ga_graph* g, const unsigned long long* d_total, uint64_t* out) {
+    GA_CUDA(cudaMemcpyAsync(g->h_scalars, d_total, 8, cudaMemcpyDeviceToHost, g->stream));
+    GA_CUDA(cudaStreamSynchronize(g->stream));
+    if (out) *out = g->h_scalars[0];
+    return GA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+ga_status ga_tc_count(ga_graph* g, uint64_t* triangles) {
+    if (!g || !triangles) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    GA_TRY(use_device(g));
+    TcArgs<unsigned int> a{};
+    a.total = g->d_scalars;
+    GA_TRY((run_tc<TC_COUNT, false, unsigned int>(g, a, true)));
+    return read_total(g, a.total, triangles);
+}
+
+ga_status ga_tc_count_async(ga_graph* g, uint64_t* d_triangles) {
+    if (!g || !d_triangles) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    GA_TRY(use_device(g));
+    TcArgs<unsigned int> a{};
+    a.total = (unsigned long long*)d_triangles;
+    return run_tc<TC_COUNT, false, unsigned int>(g, a, true);
+}
+
+ga_status ga_tc_support_edges_device(ga_graph* g, uint32_t* d_sup, uint64_t* triangles) {
+    if (!g || (!d_sup && g->m)) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    GA_TRY(use_device(g));
+    TcArgs<unsigned int> a{};
+    a.total = g->d_scalars;
+    a.esup = d_sup;
+    GA_TRY((run_tc<TC_ESUP, false, unsigned int>(g, a, true)));
+    return read_total(g, a.total, triangles);
+}
+
+ga_status ga_tc_support_edges(ga_graph* g, uint32_t* sup, uint64_t* triangles) {
+    if (!g || (!sup && g->m)) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    GA_TRY(use_device(g));
+    Scratch s;
+    s.st = g->stream;
+    GA_CUDA(cudaMallocAsync(&s.p, ((size_t)g->m + 1) * 4, g->stream));
+    GA_TRY(ga_tc_support_edges_device(g, (uint32_t*)s.p, triangles));
+    if (g->m) GA_CUDA(cudaMemcpyAsync(sup, s.p, (size_t)g->m * 4, cudaMemcpyDeviceToHost, g->stream));
+    GA_CUDA(cudaStreamSynchronize(g->stream));
+    return GA_OK;
+}
+
+ga_status ga_tc_support_vertices(ga_graph* g, uint64_t* deg, uint64_t* triangles) {
+    if (!g || (!deg && g->n)) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    GA_TRY(use_device(g));
+    Scratch s;
+    s.st = g->stream;
+    GA_CUDA(cudaMallocAsync(&s.p, ((size_t)g->n + 1) * 8, g->stream));
+    TcArgs<unsigned long long> a{};
+    a.total = g->d_scalars;
+    a.vsup = (unsigned long long*)s.p;
+    GA_TRY((run_tc<TC_VSUP, false, unsigned long long>(g, a, true)));
+    if (g->n) GA_CUDA(cudaMemcpyAsync(deg, s.p, (size_t)g->n * 8, cudaMemcpyDeviceToHost, g->stream));
+    return read_total(g, a.total, triangles);
+}
+
+ga_status ga_tc_participation(ga_graph* g, const uint8_t* alive, uint32_t* tri, uint64_t* triangles) {
+    if (!g || ((!alive || !tri) && g->n)) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    GA_TRY(use_device(g));
+    // T of the alive subgraph is at most T of the graph; refuse when uint32 counters could overflow (densest.h:68)
+    uint64_t T_full = 0;
+    GA_TRY(ga_tc_count(g, &T_full));
+    if (T_full >= (1ull << 32))
+        return fail(GA_ERR_ARITH, "triangle count >= 2^32: uint32 tri[] counters could overflow");
+    Scratch s;
+    s.st = g->stream;
+    GA_CUDA(cudaMallocAsync(&s.p, ((size_t)g->n + 1) * 5, g->stream));
+    uint32_t* d_tri = (uint32_t*)s.p;
+    uint8_t* d_alive = (uint8_t*)(d_tri + g->n + 1);
+    if (g->n) GA_CUDA(cudaMemcpyAsync(d_alive, alive, g->n, cudaMemcpyHostToDevice, g->stream));
+    TcArgs<unsigned int> a{};
+    a.total = g->d_scalars;
+    a.vsup = d_tri;
+    a.alive = d_alive;
+    GA_TRY((run_tc<TC_VSUP, true, unsigned int>(g, a, true)));
+    if (g->n) GA_CUDA(cudaMemcpyAsync(tri, d_tri, (size_t)g->n * 4, cudaMemcpyDeviceToHost, g->stream));
+    return read_total(g, a.total, triangles);
+}
+
+}  // extern "C"

@@ -1,0 +1,195 @@
+/* graph_analyzer_b200.h - C ABI of the B200 (sm_100a) triangle path.
+ *
+ * Drop-in boundary for the triangle hot path of VijayPraneethSai/graph_analyzer (paths below are relative to that
+ * project). The reference has no C ABI: its surface is header-only C++ (src/graph.h, src/densest.h, src/dsg.h),
+ * raw-pointer __global__ kernels (src/kernels.cuh) driven by src/gpu_tc.cu, src/gpu_densest.cu and src/gpu_dsg.cu,
+ * and duck-typed backends for the host loops batch_peel_loop (densest.h:279-303) and core_decomp_loop[_inc]
+ * (dsg.h:693-751). Each entry point below names the reference interface it replaces. The C++ surface with the
+ * reference's own names (Graph, build_graph_from_edges, load_graph, PeelResult, ...) is include/ga/graph_analyzer.hpp,
+ * a header-only layer over these functions.
+ *
+ * Conventions
+ *  - Plain pointers and sizes; no CUDA or torch types. `stream` arguments are cudaStream_t passed as void*.
+ *  - Pointers documented as "host" are host memory (pageable or pinned); "device" pointers are device memory of the
+ *    graph's device.
+ *  - Every function returns a ga_status. On failure ga_last_error() returns a message for the calling thread.
+ *    Nothing calls exit() or traps on the device (the reference's CUDA_CHECK -> exit(1), gpu_tc.cu:29-37, becomes
+ *    GA_ERR_CUDA).
+ *  - The library owns the device memory behind a ga_graph handle (the reference's backends leak theirs,
+ *    gpu_densest.cu:82-96); ga_graph_destroy frees it.
+ *  - A ga_graph is used by one host thread at a time; different handles may be used from different threads.
+ */
+#ifndef GRAPH_ANALYZER_B200_H
+#define GRAPH_ANALYZER_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GA_API_VERSION 1
+
+typedef enum ga_status {
+    GA_OK = 0,
+    GA_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad size, eps out of range (densest.h:67)                      */
+    GA_ERR_INVALID_GRAPH = 2,    /* CSR not valid: rowptr not monotone, endpoint >= n, self loop, unsorted row     */
+    GA_ERR_CUDA = 3,             /* a CUDA call failed (the reference's CUDA_CHECK, gpu_tc.cu:29-37)              */
+    GA_ERR_OUT_OF_MEMORY = 4,    /* device or host allocation failed                                                */
+    GA_ERR_ARITH = 5,            /* refused by the overflow guards: peel_arith_ok (densest.h:65-72), T >= 2^32 for
+                                    uint32 counters (dsg.h:696,727)                                                 */
+    GA_ERR_ROUND_LIMIT = 6,      /* a device-resident loop hit its round cap                                        */
+    GA_ERR_IO = 7,               /* file could not be read (load_graph, graph.h:72-73)                             */
+    GA_ERR_NO_DEVICE = 8,        /* no CUDA device                                                                  */
+    GA_ERR_DEVICE_CHECK = 9,     /* the device reported an impossible state (densest.h:298, dsg.h:710: removed 0
+                                    or more than alive, level decreased)                                           */
+    GA_ERR_BUDGET = 10,          /* serving admission: request does not fit the HBM budget                          */
+    GA_ERR_CAPACITY = 11,        /* a fixed-capacity variant was given a size beyond its stated maximum            */
+    GA_ERR_NOT_READY = 12        /* serving: result not available yet                                                */
+} ga_status;
+
+/* Human-readable name of a status code. */
+const char* ga_status_string(ga_status s);
+/* Message of the last failing call made by this thread ("" if none). */
+const char* ga_last_error(void);
+/* Number of CUDA devices visible (0 without a GPU). */
+ga_status ga_device_count(int* count);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Host-side graph construction: the reference's Graph / load_graph / build_graph_from_edges (graph.h:19-96).
+ * ------------------------------------------------------------------------------------------------------------- */
+
+/* Oriented CSR owned by the library (fields of struct Graph, graph.h:19-26). */
+typedef struct ga_host_graph {
+    uint32_t n;              /* vertices 0..n-1                                                   */
+    uint32_t m;              /* oriented edges == undirected edges after clean-up                 */
+    uint32_t max_out_degree;
+    uint32_t* rowptr;        /* n+1                                                               */
+    uint32_t* col;           /* m, each row sorted ascending                                      */
+    uint32_t* src;           /* m, src[e] = row owning edge e                                     */
+} ga_host_graph;
+
+/* load_graph's clean-up of an undirected pair list (graph.h:85-92): drops self loops, stores (min,max), sorts and
+ * removes duplicates. In place on `pairs` (2*npairs interleaved uint32); *out_npairs = pairs kept. */
+ga_status ga_canonical_edges(uint32_t* pairs, uint64_t npairs, uint64_t* out_npairs);
+
+/* build_graph_from_edges (graph.h:38-67) into caller arrays: rowptr[n+1], col[m], src[m]. `pairs` must hold m unique
+ * undirected pairs without self loops (the reference's precondition); endpoints >= n give GA_ERR_INVALID_GRAPH.
+ * Orientation from the endpoint with the smaller (degree, id) to the other; rows sorted. */
+ga_status ga_build_graph_from_edges(uint32_t n, const uint32_t* pairs, uint32_t m, uint32_t* rowptr, uint32_t* col,
+                                    uint32_t* src, uint32_t* max_out_degree);
+
+/* Library-allocated variant: canonicalises a copy of `pairs` first when `canonicalize` != 0. */
+ga_status ga_host_graph_from_edges(uint32_t n, const uint32_t* pairs, uint64_t npairs, int canonicalize,
+                                   ga_host_graph** out);
+
+/* load_graph (graph.h:71-96): SNAP text edge list, '#'/'%' comment lines, n = max_id + 1. Ids must fit uint32
+ * (the reference truncates larger ids silently; this returns GA_ERR_INVALID_GRAPH). */
+ga_status ga_load_graph(const char* path, ga_host_graph** out);
+
+void ga_host_graph_free(ga_host_graph* g);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Seeded synthetic inputs (no counterpart in the reference's C++; its generators are scripts/gen_*.py).
+ * ------------------------------------------------------------------------------------------------------------- */
+
+/* Holme-Kim power-law cluster graph: each new vertex attaches m_v edges (m_v = m_hi with probability p_hi, else
+ * m_lo) by preferential attachment, each later edge closing a triangle with probability triad_p. Writes unique
+ * undirected pairs without self loops; `cap` = capacity in pairs (n*m_hi suffices). */
+ga_status ga_gen_holme_kim(uint32_t n, uint32_t m_lo, uint32_t m_hi, double p_hi, double triad_p, uint64_t seed,
+                           uint32_t* pairs, uint64_t cap, uint64_t* npairs);
+/* R-MAT samples on 2^scale vertices with quadrant probabilities (a, b, c, 1-a-b-c). Writes `nsamples` raw pairs
+ * (self loops and duplicates included; ga_canonical_edges symmetrises and cleans them). */
+ga_status ga_gen_rmat(uint32_t scale, uint64_t nsamples, double a, double b, double c, uint64_t seed,
+                      uint32_t* pairs);
+/* Relabels every endpoint through a seeded uniform permutation of 0..n-1. */
+ga_status ga_permute_ids(uint32_t* pairs, uint64_t npairs, uint32_t n, uint64_t seed);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Device-resident graph (replaces the upload() + cudaMalloc pattern of gpu_tc.cu:43-62, gpu_densest.cu:48-96 and
+ * gpu_dsg.cu:61-80). The CSR stays resident for repeated queries; derived device structures (src, in-lists,
+ * work lists) are built on the device on first use and kept.
+ * ------------------------------------------------------------------------------------------------------------- */
+typedef struct ga_graph ga_graph;
+
+/* Copies rowptr[n+1] and col[m] (host memory) to `device` and validates them on the device. stream may be NULL
+ * (the library then creates its own non-blocking stream). */
+ga_status ga_graph_create(const uint32_t* rowptr, const uint32_t* col, uint32_t n, uint32_t m, int device,
+                          void* stream, ga_graph** out);
+/* Same from device memory of `device` (copied device-to-device; the caller keeps ownership of its buffers). */
+ga_status ga_graph_create_device(const uint32_t* d_rowptr, const uint32_t* d_col, uint32_t n, uint32_t m,
+                                 int device, void* stream, ga_graph** out);
+ga_status ga_graph_destroy(ga_graph* g);
+/* Stream used by the graph's calls (cudaStream_t as void*). */
+ga_status ga_graph_set_stream(ga_graph* g, void* stream);
+/* Device bytes held by the graph (CSR plus derived structures and scratch). */
+ga_status ga_graph_device_bytes(const ga_graph* g, uint64_t* bytes);
+/* Builds the derived structures now (otherwise the first query does it). */
+ga_status ga_graph_prepare(ga_graph* g);
+
+/* Tuning knobs (the reference's compile-time macros SM_CAP / HASH_SLOTS / TASK_CHUNK, kernels.cuh:23-34, become
+ * run-time options; GA_OPT_*_AUTO lets the autotuner choose). */
+typedef enum ga_option {
+    GA_OPT_TC_KERNEL = 1,     /* 0 auto, 1 plain merge (one thread per oriented edge), 2 degree-binned hash probe */
+    GA_OPT_LOOP_MODE = 2,     /* 0 auto, 1 host-driven rounds (one sync per round), 2 CUDA graph with a device
+                                 while-node (no host sync inside the loop)                                          */
+    GA_OPT_MAX_ROUNDS = 3,    /* round cap of device-resident loops (0 = n + 1)                                    */
+    GA_OPT_ITEM_WORK = 4,     /* probe work (list elements) per work item of the hash kernel (0 = 4096)            */
+    GA_OPT_HEAVY_TABLE_BITS = 5, /* log2 slots of the block-wide hash set; anchors that need more binary-search the
+                                    global row (0 = as large as shared memory allows, 5..15)                        */
+    GA_OPT_LIGHT_MAX_DEG = 6  /* anchors with out-degree <= this use per-warp tables (0 = 256, at most 256)        */
+} ga_option;
+ga_status ga_graph_set_option(ga_graph* g, ga_option opt, int64_t value);
+
+/* ---- triangle counting: replaces kernels v1-v9 (kernels.cuh:53-358) as launched by gpu_tc.cu:165-229 ---- */
+
+/* Sum over oriented edges (u,v) of |N+(u) ∩ N+(v)| = cpu_triangles_serial (graph.h:110-121). */
+ga_status ga_tc_count(ga_graph* g, uint64_t* triangles);
+/* Same, asynchronous: enqueues the count on the graph's stream and writes it to device memory d_triangles
+ * (8 bytes) without a host sync (kernels.cuh's "unsigned long long* total" output). Call ga_graph_prepare first if
+ * the launch must not include the one-time preparation. */
+ga_status ga_tc_count_async(ga_graph* g, uint64_t* d_triangles);
+
+/* Per-oriented-edge support, indexed like col: sup[e] = triangles containing edge e (for_each_triangle's
+ * (e, i, j), dsg.h:67-79). `sup` is host memory of m entries. *triangles may be NULL. */
+ga_status ga_tc_support_edges(ga_graph* g, uint32_t* sup, uint64_t* triangles);
+/* Same, writing to device memory of m entries on the graph's stream. */
+ga_status ga_tc_support_edges_device(ga_graph* g, uint32_t* d_sup, uint64_t* triangles);
+
+/* Per-vertex triangle degree = triangle_degrees (dsg.h:82-87). `deg` is host memory of n entries. */
+ga_status ga_tc_support_vertices(ga_graph* g, uint64_t* deg, uint64_t* triangles);
+
+/* Triangles of the subgraph induced by alive[] and tri[v] per vertex = tc_per_vertex_alive (kernels.cuh:399-425),
+ * cpu_triangle_participation (densest.h:81-101). alive and tri are host memory of n entries. Refuses T >= 2^32
+ * (uint32 counters) with GA_ERR_ARITH. */
+ga_status ga_tc_participation(ga_graph* g, const uint8_t* alive, uint32_t* tri, uint64_t* triangles);
+
+/* ---- triangle-density batch peeling: replaces batch_peel_loop<GpuBackend> (densest.h:279-303,
+ *      gpu_densest.cu:70-126) with a device-resident loop ---- */
+typedef struct ga_peel_result {
+    uint64_t best_num;    /* triangles of the best subgraph                            */
+    uint64_t best_den;    /* vertices of the best subgraph                             */
+    uint32_t best_round;  /* best subgraph = { v : removed_round[v] >= best_round }    */
+    uint32_t rounds;      /* rounds executed                                           */
+} ga_peel_result;          /* the integer fields of PeelResult (densest.h:46-54)        */
+
+/* eps = num/den. removed_round: host memory of n entries (UINT32_MAX = never removed), may be NULL.
+ * Refusals follow peel_arith_ok (densest.h:65-72): GA_ERR_INVALID_ARGUMENT for eps out of range, GA_ERR_ARITH for
+ * the overflow bounds. */
+ga_status ga_batch_peel(ga_graph* g, uint64_t num, uint64_t den, ga_peel_result* res, uint32_t* removed_round);
+
+/* ---- (k, triangle)-core decomposition: replaces core_decomp_loop_inc<GpuCoreBackendInc> (dsg.h:724-751,
+ *      gpu_dsg.cu:138-199) ---- */
+typedef struct ga_core_result {
+    uint32_t kmax;    /* maximum core number                         */
+    uint32_t rounds;  /* level-synchronous rounds (CoreLoopResult)   */
+} ga_core_result;
+
+/* core: host memory of n entries (core numbers of core_decomposition, dsg.h:125-166), may be NULL.
+ * Refuses T >= 2^32 with GA_ERR_ARITH (dsg.h:727). */
+ga_status ga_core_decomposition(ga_graph* g, uint32_t* core, ga_core_result* res);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GRAPH_ANALYZER_B200_H */

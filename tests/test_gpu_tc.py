@@ -1,0 +1,150 @@
+"""GPU parity: triangle count, per-edge and per-vertex support, alive-subgraph participation (through the C ABI)
+against the oracle and the reference's golden outputs. Integer work: bit-exact equality everywhere."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import FIXTURES, fixture_path, golden_arrays, hub_pairs, random_pairs
+
+pytestmark = pytest.mark.gpu
+
+# kernel configurations that force every path: default (light + heavy bins), plain merge kernel, tiny light bin with
+# a small heavy table (heavy anchors and the global binary-search fallback), small work items (many items/anchor)
+CONFIGS = {
+    "auto": {},
+    "plain": {1: 1},
+    "heavy_global": {6: 8, 5: 5},
+    "heavy_table": {6: 4, 5: 12},
+    "small_items": {4: 16},
+}
+
+
+def _dev(ga, g, cfg):
+    d = ga.DeviceGraph(g)
+    for opt, val in CONFIGS[cfg].items():
+        d.set_option(opt, val)
+    return d
+
+
+def _check_all(ga, oracle, g, cfg, rng):
+    T = oracle.triangles_serial(g)
+    _, sup = oracle.edge_support(g)
+    _, deg = oracle.triangle_degrees(g)
+    with _dev(ga, g, cfg) as d:
+        assert d.tc_count() == T
+        assert d.tc_count() == T                                  # repeat launches are identical
+        Ts, gsup = d.support_edges()
+        assert Ts == T and np.array_equal(gsup, sup)
+        Tv, gdeg = d.support_vertices()
+        assert Tv == T and np.array_equal(gdeg, deg)
+        for pa in (1.0, 0.9, 0.6, 0.3, 0.05, 0.0):                 # emu_densest.cpp:97-114 masks
+            alive = (rng.random(g.n) < pa).astype(np.uint8)
+            Ta, tri = d.participation(alive)
+            To, trio = oracle.participation(g, alive)
+            assert Ta == To and np.array_equal(tri, trio)
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+@pytest.mark.parametrize("cfg", list(CONFIGS))
+def test_fixtures(ga, oracle, golden, cuda_ok, name, cfg):
+    g = ga.load_graph(fixture_path(name))
+    arr = golden_arrays(name)
+    with _dev(ga, g, cfg) as d:
+        assert d.tc_count() == golden[name]["brute_force_triangles"]
+        assert np.array_equal(d.support_edges()[1], arr["sup"])
+        assert np.array_equal(d.support_vertices()[1], arr["deg"])
+    _check_all(ga, oracle, g, cfg, np.random.default_rng(7))
+
+
+@pytest.mark.parametrize("seed", range(4))
+@pytest.mark.parametrize("cfg", list(CONFIGS))
+def test_random_graphs(ga, oracle, cuda_ok, seed, cfg):
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(50, 700))
+    g = ga.build_graph_from_edges(n, ga.canonical_edges(random_pairs(rng, n, float(rng.choice([0.02, 0.1, 0.3])))))
+    _check_all(ga, oracle, g, cfg, rng)
+
+
+@pytest.mark.parametrize("cfg", ["auto", "heavy_global", "plain"])
+def test_hub_graphs(ga, oracle, cuda_ok, cfg):
+    rng = np.random.default_rng(11)
+    for _ in range(4):
+        n, raw = hub_pairs(rng, int(rng.integers(1, 4)), int(rng.integers(40, 400)), int(rng.integers(8, 40)))
+        g = ga.build_graph_from_edges(n, ga.canonical_edges(raw))
+        _check_all(ga, oracle, g, cfg, rng)
+
+
+@pytest.mark.parametrize("cfg", list(CONFIGS))
+def test_clique_uses_heavy_bin(ga, oracle, cuda_ok, cfg):
+    n = 640                                                       # out-degrees up to 639 > 256: heavy anchors
+    iu, iv = np.triu_indices(n, 1)
+    g = ga.build_graph_from_edges(n, np.stack([iu, iv], 1).astype(np.uint32))
+    with _dev(ga, g, cfg) as d:
+        assert d.tc_count() == n * (n - 1) * (n - 2) // 6
+        T, deg = d.support_vertices()
+        assert np.all(deg == (n - 1) * (n - 2) // 2)
+        T, sup = d.support_edges()
+        assert np.all(sup == n - 2)
+
+
+def test_holme_kim_c1_shape(ga, oracle, cuda_ok):
+    """The 8,298-vertex Holme-Kim graph (12 edges per new vertex, p = 0.5), ids permuted from the seed."""
+    g = ga.graph_from_pairs(8298, ga.gen_holme_kim(8298, 12, 12, 0.0, 0.5, seed=1))
+    _check_all(ga, oracle, g, "auto", np.random.default_rng(3))
+    _check_all(ga, oracle, g, "plain", np.random.default_rng(3))
+
+
+def test_rmat_skewed(ga, oracle, cuda_ok):
+    g = ga.graph_from_pairs(1 << 14, ga.gen_rmat(14, 9 * (1 << 14), seed=2))
+    _check_all(ga, oracle, g, "auto", np.random.default_rng(4))
+
+
+def test_edge_cases(ga, oracle, cuda_ok):
+    cases = [
+        (0, np.zeros((0, 2), np.uint32)),
+        (1, np.zeros((0, 2), np.uint32)),
+        (7, np.zeros((0, 2), np.uint32)),
+        (3, np.array([[0, 1], [1, 2], [0, 2]], np.uint32)),
+        (5, np.array([[0, 1], [1, 2], [2, 3], [3, 4]], np.uint32)),          # a path: no triangle
+        (300, np.array([[0, i] for i in range(1, 300)], np.uint32)),        # a star: no triangle
+    ]
+    for n, p in cases:
+        g = ga.build_graph_from_edges(n, p)
+        with ga.DeviceGraph(g) as d:
+            assert d.tc_count() == oracle.triangles_serial(g)
+            assert np.array_equal(d.support_edges()[1], oracle.edge_support(g)[1])
+            assert np.array_equal(d.support_vertices()[1], oracle.triangle_degrees(g)[1])
+
+
+def test_invalid_csr_rejected(ga, cuda_ok):
+    good = ga.build_graph_from_edges(4, np.array([[0, 1], [1, 2], [0, 2], [2, 3]], np.uint32))
+    bad = ga.Graph(good.n, good.m, good.rowptr.copy(), good.col.copy(), good.src, good.max_out_degree)
+    bad.col[0] = 9                                                   # endpoint >= n
+    with pytest.raises(ga.GAError) as e:
+        ga.DeviceGraph(bad)
+    assert e.value.name == "GA_ERR_INVALID_GRAPH"
+    # both directions of an undirected edge: valid rows, but not a (degree, id) orientation
+    rp = np.array([0, 1, 2], np.uint32)
+    col = np.array([1, 0], np.uint32)
+    d = ga.DeviceGraph(ga.Graph(2, 2, rp, col, np.array([0, 1], np.uint32), 1))
+    with pytest.raises(ga.GAError) as e:
+        d.tc_count()
+    assert e.value.name == "GA_ERR_INVALID_GRAPH"
+    d.close()
+
+
+def test_device_create_and_streams(ga, oracle, cuda_ok):
+    import torch
+    g = ga.graph_from_pairs(2000, ga.gen_holme_kim(2000, 5, 5, 0.0, 0.5, seed=9))
+    rp = torch.from_numpy(g.rowptr.astype(np.int32)).cuda()
+    col = torch.from_numpy(g.col.astype(np.int32)).cuda()
+    s = torch.cuda.Stream()
+    with ga.DeviceGraph.from_device(rp.data_ptr(), col.data_ptr(), g.n, g.m, 0, s.cuda_stream) as d:
+        assert d.tc_count() == oracle.triangles_serial(g)
+        d.set_stream(None)
+        assert d.tc_count() == oracle.triangles_serial(g)
+        sup = torch.zeros(g.m, dtype=torch.int32, device="cuda")
+        assert d.support_edges_device(sup.data_ptr()) == oracle.triangles_serial(g)
+        assert np.array_equal(sup.cpu().numpy().view(np.uint32), oracle.edge_support(g)[1])
+        assert d.device_bytes() > 0
