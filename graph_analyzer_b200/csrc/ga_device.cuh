@@ -109,7 +109,7 @@ struct ga_graph {
 
     // options (ga_option)
     int64_t opt_tc_kernel = 0, opt_loop_mode = 0, opt_max_rounds = 0;
-    uint32_t item_work = 4096, heavy_bits_cap = 0, light_max_deg = 256;
+    uint32_t item_work = 4096, heavy_bits_cap = 0, light_max_deg = 128;
 
     // every device allocation, freed by ga_graph_destroy
     std::vector<std::pair<void*, size_t>> allocations;

@@ -15,6 +15,7 @@ namespace ga {
 
 // ---- scan (reduce-then-scan over tiles of 256 threads x 16 elements) --------------------------------------------
 constexpr int kScanThreads = 256, kScanItems = 16, kScanTile = kScanThreads * kScanItems;
+constexpr unsigned long long kHeavyItemFactor = 64;   // heavy items carry 64x the probe work of light items
 
 template <class T>
 __global__ void k_tile_reduce(const T* __restrict__ in, uint64_t n, T* __restrict__ sums) {
@@ -168,56 +169,64 @@ __global__ void k_in_work(const uint32_t* __restrict__ rowptr, const uint32_t* _
 }
 
 // Items per anchor. prefix = inclusive scan of work over in-edges. An anchor with out-degree 0 or no in-edge has no
-// item; otherwise ceil(work / target) items (at least 1), light or heavy by its out-degree.
+// item; otherwise ceil(work / target) items (at least 1, at most one per in-edge), light or heavy by its out-degree
+// (heavy items are `heavy_factor` times larger: the block-wide table is built once per item).
 __global__ void k_count_items(const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ in_ptr,
                               const unsigned long long* __restrict__ prefix, uint32_t n, uint32_t light_max_deg,
-                              unsigned long long target, uint32_t* __restrict__ cnt_light,
-                              uint32_t* __restrict__ cnt_heavy, unsigned* max_dv_heavy) {
+                              unsigned long long target, unsigned long long heavy_target,
+                              uint32_t* __restrict__ cnt_light, uint32_t* __restrict__ cnt_heavy,
+                              unsigned* max_dv_heavy) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
         const uint32_t dv = rowptr[v + 1] - rowptr[v];
         const uint32_t b = in_ptr[v], e = in_ptr[v + 1];
+        const bool heavy = dv > light_max_deg;
         uint32_t c = 0;
         if (dv > 0 && e > b) {
             const unsigned long long w = prefix[e - 1] - (b ? prefix[b - 1] : 0ull);
-            c = (uint32_t)max(1ull, (w + target - 1) / target);
+            const unsigned long long t = heavy ? heavy_target : target;
+            c = (uint32_t)max(1ull, (w + t - 1) / t);
             if (c > e - b) c = e - b;
         }
-        const bool heavy = dv > light_max_deg;
         cnt_light[v] = heavy ? 0 : c;
         cnt_heavy[v] = heavy ? c : 0;
         if (heavy && c) atomicMax(max_dv_heavy, dv);
     }
 }
 
-// Emits the items of every anchor: chunk c starts at the first in-edge whose local work prefix exceeds c * W / cnt.
+// One thread per item: finds its anchor by binary search over the item offsets, then the item's in-edge range:
+// chunk j of c covers the in-edges whose local inclusive work prefix lies in (j*w/c, (j+1)*w/c] (chunks can be
+// empty; together they cover the anchor's in-edges exactly once).
 __global__ void k_emit_items(const uint32_t* __restrict__ in_ptr, const unsigned long long* __restrict__ prefix,
                              const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ off, uint32_t n,
-                             uint32_t* __restrict__ it_v, uint32_t* __restrict__ it_k0, uint32_t* __restrict__ it_k1) {
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-        const uint32_t c = cnt[v];
-        if (!c) continue;
-        const uint32_t b = in_ptr[v], e = in_ptr[v + 1], o = off[v];
-        const unsigned long long base = b ? prefix[b - 1] : 0ull, w = prefix[e - 1] - base;
-        uint32_t start = b;
-        for (uint32_t i = 0; i < c; i++) {
-            uint32_t end = e;
-            if (i + 1 < c) {
-                // chunk i ends at the first k with local prefix > (i+1) * w / c; every chunk keeps >= 1 in-edge and
-                // leaves >= 1 for each later chunk (invariant: start <= e - (c - i))
-                const unsigned long long goal = base + (w * (i + 1)) / c;
-                uint32_t lo = start, hi = e;
-                while (lo < hi) {
-                    const uint32_t mid = lo + ((hi - lo) >> 1);
-                    if (prefix[mid] <= goal) lo = mid + 1; else hi = mid;
-                }
-                end = lo > start ? lo : start + 1;
-                if (end > e - (c - 1 - i)) end = e - (c - 1 - i);
-            }
-            it_v[o + i] = v;
-            it_k0[o + i] = start;
-            it_k1[o + i] = end;
-            start = end;
+                             uint32_t total, uint32_t* __restrict__ it_v, uint32_t* __restrict__ it_k0,
+                             uint32_t* __restrict__ it_k1) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        // anchor = last v with off[v] <= i and cnt[v] > 0  (off is the exclusive scan of cnt)
+        uint32_t lo = 0, hi = n;
+        while (lo < hi) {
+            const uint32_t mid = lo + ((hi - lo) >> 1);
+            if (off[mid] <= i) lo = mid + 1; else hi = mid;
         }
+        const uint32_t v = lo - 1;   // an anchor without items shares its offset with the next, so the last match has items
+        const uint32_t c = cnt[v], j = i - off[v];
+        const uint32_t b = in_ptr[v], e = in_ptr[v + 1];
+        const unsigned long long base = b ? prefix[b - 1] : 0ull, w = prefix[e - 1] - base;
+        uint32_t bound[2];
+        for (int q = 0; q < 2; q++) {
+            const uint32_t jj = j + q;
+            if (jj == 0) { bound[q] = b; continue; }
+            if (jj == c) { bound[q] = e; continue; }
+            const unsigned long long goal = base + (w * jj) / c;
+            uint32_t l2 = b, h2 = e;                   // first k with prefix[k] > goal
+            while (l2 < h2) {
+                const uint32_t mid = l2 + ((h2 - l2) >> 1);
+                if (prefix[mid] <= goal) l2 = mid + 1; else h2 = mid;
+            }
+            bound[q] = l2;
+        }
+        it_v[i] = v;
+        it_k0[i] = bound[0];
+        it_k1[i] = bound[1];
     }
 }
 
@@ -244,8 +253,8 @@ static ga_status build_items(ga_graph* g, const unsigned long long* prefix, uint
     const unsigned grid = grid_for(n, 256);
     const unsigned long long target = g->item_work;   // probes per item (bounds the tail of the dynamic queue)
     GA_CUDA(cudaMemsetAsync(d_maxdv, 0, sizeof(unsigned), st));
-    k_count_items<<<grid, 256, 0, st>>>(g->rowptr, g->in_ptr, prefix, n, g->light_max_deg, target, cnt_l, cnt_h,
-                                        d_maxdv);
+    k_count_items<<<grid, 256, 0, st>>>(g->rowptr, g->in_ptr, prefix, n, g->light_max_deg, target,
+                                        target * kHeavyItemFactor, cnt_l, cnt_h, d_maxdv);
     GA_CUDA(cudaGetLastError());
     GA_TRY(scan_impl<uint32_t>(st, cnt_l, off_l, n, false));
     GA_TRY(scan_impl<uint32_t>(st, cnt_h, off_h, n, false));
@@ -269,7 +278,8 @@ static ga_status build_items(ga_graph* g, const unsigned long long* prefix, uint
         GA_TRY(dalloc(g, &it->k0, totals[b]));
         GA_TRY(dalloc(g, &it->k1, totals[b]));
         if (totals[b]) {
-            k_emit_items<<<grid, 256, 0, st>>>(g->in_ptr, prefix, cnts[b], offs[b], n, it->v, it->k0, it->k1);
+            k_emit_items<<<grid_for(totals[b], 256), 256, 0, st>>>(g->in_ptr, prefix, cnts[b], offs[b], n,
+                                                                    totals[b], it->v, it->k0, it->k1);
             GA_CUDA(cudaGetLastError());
         }
     }
@@ -501,7 +511,7 @@ ga_status ga_graph_set_option(ga_graph* g, ga_option opt, int64_t value) {
             g->heavy_bits_cap = (uint32_t)value;
             return GA_OK;
         case GA_OPT_LIGHT_MAX_DEG: {
-            const uint32_t v = value ? (uint32_t)std::min<int64_t>(value, 256) : 256;
+            const uint32_t v = value ? (uint32_t)std::min<int64_t>(value, 256) : 128;
             if (v != g->light_max_deg) { g->light_max_deg = v; g->prepared = false; }
             return GA_OK;
         }

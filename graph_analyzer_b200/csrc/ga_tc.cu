@@ -39,7 +39,8 @@ namespace ga {
 
 constexpr int kWarps = 8;                 // warps per block of the hash kernel
 constexpr int kThreads = kWarps * 32;
-constexpr int kLightSlots = 512;          // per-warp hash set: anchors with out-degree <= 256 (load <= 1/2)
+constexpr int kLightSlots = 512;          // per-warp hash set: anchors with out-degree <= 128 (load <= 1/4)
+constexpr uint32_t kLightBits = 9;
 
 template <int MODE>
 struct SlotLayout {   // 32-bit words per hash slot: key, +count (VSUP/ESUP), +position (ESUP)
@@ -60,81 +61,82 @@ __device__ __forceinline__ void on_hit(const TcArgs<CT>& a, uint32_t* cnt, uint3
     if (MODE == TC_ESUP) atomicAdd(&a.esup[e], 1u);
 }
 
-// Processes in-edges [kb, k1) of anchor v in batches of 32 (one warp), probing a hash set (key/cnt, 2^bits slots)
-// or, when `global` is set, binary searching the sorted row N+(v) = col[vb, vb + dv). `stride` = 32 * warps that
-// share the item. Returns the hits of this lane.
+// Probes one batch of up to 32 in-edges [kb, kend) of anchor v (one warp): lane l loads the l-th source u, a warp
+// scan of the list lengths flattens the lists N+(u) into one probe sequence and lane p takes probes p, p+32, ...
+// (each lane advances its owner index monotonically). A probe looks x up in the hash set (key, 2^bits slots) or, when
+// `global` is set, binary searches the sorted row N+(v) = col[vb, vb + dv). Returns this lane's hits.
 template <int MODE, bool ALIVE, class CT>
-__device__ __forceinline__ unsigned long long probe_in_edges(
+__device__ __forceinline__ unsigned long long probe_batch(
     const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ col, const uint32_t* __restrict__ in_src,
-    const uint32_t* __restrict__ in_eid, const TcArgs<CT>& a, uint32_t kb, uint32_t k1, uint32_t stride,
-    const uint32_t* key, uint32_t* cnt, uint32_t bits, bool global, uint32_t vb, uint32_t dv, uint32_t* s_incl,
-    uint32_t* s_rb, uint32_t* s_ecnt, uint32_t lane) {
+    const uint32_t* __restrict__ in_eid, const TcArgs<CT>& a, uint32_t kb, uint32_t kend, const uint32_t* key,
+    uint32_t* cnt, uint32_t bits, bool global, uint32_t vb, uint32_t dv, uint32_t* s_incl, uint32_t* s_rb,
+    uint32_t* s_ecnt, uint32_t lane) {
     unsigned long long hits = 0;
     const uint32_t mask = (1u << bits) - 1;
-    for (; kb < k1; kb += stride) {
-        const uint32_t k = kb + lane;
-        uint32_t d = 0, rb = 0, u = 0;
-        if (k < k1) {
-            u = in_src[k];
-            if (!ALIVE || a.alive[u]) {
-                rb = rowptr[u];
-                d = rowptr[u + 1] - rb;
-            }
+    const uint32_t k = kb + lane;
+    uint32_t d = 0, rb = 0, u = 0;
+    if (k < kend) {
+        u = in_src[k];
+        if (!ALIVE || a.alive[u]) {
+            rb = rowptr[u];
+            d = rowptr[u + 1] - rb;
         }
-        const uint32_t incl = warp_incl_scan(d, lane);
-        const uint32_t tot = __shfl_sync(GA_FULL_MASK, incl, 31);
-        s_incl[lane] = incl;
-        s_rb[lane] = rb;
-        __syncwarp();
-        uint32_t owner = 0;
-        for (uint32_t p = lane; p < tot; p += 32) {
-            while (s_incl[owner] <= p) owner++;
-            const uint32_t e = s_rb[owner] + (p - (owner ? s_incl[owner - 1] : 0u));
-            const uint32_t x = col[e];
-            if (!global) {
-                uint32_t h = hash_slot(x, bits);
-                for (;;) {
-                    const uint32_t kk = key[h];
-                    if (kk == x) {
-                        hits++;
-                        on_hit<MODE, ALIVE, CT>(a, cnt, h, s_ecnt, owner, e);
-                        break;
-                    }
-                    if (kk == GA_EMPTY) break;
-                    h = (h + 1) & mask;
-                }
-            } else {
-                const uint32_t j = lower_bound_u32(col, vb, vb + dv, x);
-                if (j < vb + dv && col[j] == x && (!ALIVE || a.alive[x])) {
-                    hits++;
-                    if (MODE >= TC_VSUP) atomicAdd(&s_ecnt[owner], 1u);
-                    if (MODE == TC_VSUP) atomicAdd(&a.vsup[x], (CT)1);
-                    if (MODE == TC_ESUP) {
-                        atomicAdd(&a.esup[e], 1u);
-                        atomicAdd(&a.esup[j], 1u);
-                    }
-                }
-            }
-        }
-        __syncwarp();
-        if (MODE >= TC_VSUP) {
-            const uint32_t c = s_ecnt[lane];
-            if (c) {
-                if (MODE == TC_VSUP) atomicAdd(&a.vsup[u], (CT)c);
-                else atomicAdd(&a.esup[in_eid[k]], c);
-                s_ecnt[lane] = 0;
-            }
-        }
-        __syncwarp();
     }
+    const uint32_t incl = warp_incl_scan(d, lane);
+    const uint32_t tot = __shfl_sync(GA_FULL_MASK, incl, 31);
+    s_incl[lane] = incl;
+    s_rb[lane] = rb;
+    __syncwarp();
+    uint32_t owner = 0;
+    for (uint32_t p = lane; p < tot; p += 32) {
+        while (s_incl[owner] <= p) owner++;
+        const uint32_t e = s_rb[owner] + (p - (owner ? s_incl[owner - 1] : 0u));
+        const uint32_t x = col[e];
+        if (!global) {
+            uint32_t h = hash_slot(x, bits);
+            for (;;) {
+                const uint32_t kk = key[h];
+                if (kk == x) {
+                    hits++;
+                    on_hit<MODE, ALIVE, CT>(a, cnt, h, s_ecnt, owner, e);
+                    break;
+                }
+                if (kk == GA_EMPTY) break;
+                h = (h + 1) & mask;
+            }
+        } else {
+            const uint32_t j = lower_bound_u32(col, vb, vb + dv, x);
+            if (j < vb + dv && col[j] == x && (!ALIVE || a.alive[x])) {
+                hits++;
+                if (MODE >= TC_VSUP) atomicAdd(&s_ecnt[owner], 1u);
+                if (MODE == TC_VSUP) atomicAdd(&a.vsup[x], (CT)1);
+                if (MODE == TC_ESUP) {
+                    atomicAdd(&a.esup[e], 1u);
+                    atomicAdd(&a.esup[j], 1u);
+                }
+            }
+        }
+    }
+    __syncwarp();
+    if (MODE >= TC_VSUP) {
+        const uint32_t c = s_ecnt[lane];
+        if (c) {
+            if (MODE == TC_VSUP) atomicAdd(&a.vsup[u], (CT)c);
+            else atomicAdd(&a.esup[in_eid[k]], c);
+            s_ecnt[lane] = 0;
+        }
+    }
+    __syncwarp();
     return hits;
 }
 
-// Table size for an anchor with dv out-neighbours: smallest power of two >= 2 dv, at least 32.
-__device__ __forceinline__ uint32_t table_bits(uint32_t dv) {
+// Table size for an anchor with dv out-neighbours: smallest power of two >= 4 dv (load <= 1/4, short miss probes),
+// at least 32; `cap` bits at most, where a load up to 1/2 is accepted. Returns 0 when even that does not fit.
+__device__ __forceinline__ uint32_t table_bits(uint32_t dv, uint32_t cap) {
     uint32_t b = 5;
-    while ((1u << b) < 2 * dv) b++;
-    return b;
+    while ((1u << b) < 4 * dv) b++;
+    if (b <= cap) return b;
+    return (1u << cap) >= 2 * dv ? cap : 0;
 }
 
 // Clears 2^bits slots and inserts the (alive) members of N+(v); tid/nthr cover the cooperating threads.
@@ -182,13 +184,14 @@ __global__ void __launch_bounds__(kThreads) k_tc_hash(const uint32_t* __restrict
                                                       ga_items light, uint32_t heavy_bits_max,
                                                       uint32_t* __restrict__ queue, TcArgs<CT> a) {
     extern __shared__ uint32_t smem[];
-    __shared__ uint32_t s_item;
+    __shared__ uint32_t s_item, s_next;
     __shared__ unsigned long long s_red[kWarps];
     constexpr int W = SlotLayout<MODE>::words;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned long long hits = 0;
 
-    // ---- heavy bin: one block per item, table of up to 2^heavy_bits_max slots shared by the block ----
+    // ---- heavy bin: the block shares one hash set of N+(v) per item; its warps pull 32-in-edge batches from a
+    //      shared counter, so no warp waits for another until the item is exhausted ----
     {
         const uint32_t Smax = 1u << heavy_bits_max;
         uint32_t* key = smem;
@@ -201,17 +204,28 @@ __global__ void __launch_bounds__(kThreads) k_tc_hash(const uint32_t* __restrict
             if (threadIdx.x == 0) s_item = atomicAdd(&queue[0], 1u);
             __syncthreads();
             const uint32_t item = s_item;
-            __syncthreads();
             if (item >= heavy.count) break;
             const uint32_t v = heavy.v[item];
-            if (ALIVE && !a.alive[v]) continue;
+            if (ALIVE && !a.alive[v]) {
+                __syncthreads();          // everyone has read s_item before thread 0 overwrites it
+                continue;
+            }
             const uint32_t vb = rowptr[v], dv = rowptr[v + 1] - vb;
-            const uint32_t bits = table_bits(dv);
-            const bool global = bits > heavy_bits_max;
+            const uint32_t k0 = heavy.k0[item], k1 = heavy.k1[item];
+            const uint32_t bits = table_bits(dv, heavy_bits_max);
+            const bool global = bits == 0;
+            if (threadIdx.x == 0) s_next = k0;
             if (!global) build_table<MODE, ALIVE, CT>(col, a, vb, dv, key, cnt, pos, bits, threadIdx.x, kThreads, true);
-            const unsigned long long h = probe_in_edges<MODE, ALIVE, CT>(
-                rowptr, col, in_src, in_eid, a, heavy.k0[item] + warp * 32, heavy.k1[item], kWarps * 32, key, cnt,
-                bits, global, vb, dv, s_incl, s_rb, s_ecnt, lane);
+            else __syncthreads();
+            unsigned long long h = 0;
+            for (;;) {
+                uint32_t kb = 0;
+                if (lane == 0) kb = atomicAdd(&s_next, 32u);
+                kb = __shfl_sync(GA_FULL_MASK, kb, 0);
+                if (kb >= k1) break;
+                h += probe_batch<MODE, ALIVE, CT>(rowptr, col, in_src, in_eid, a, kb, min(kb + 32, k1), key, cnt,
+                                                  bits, global, vb, dv, s_incl, s_rb, s_ecnt, lane);
+            }
             hits += h;
             if (MODE == TC_VSUP) {
                 const unsigned long long t = warp_sum_u64(h);
@@ -222,7 +236,7 @@ __global__ void __launch_bounds__(kThreads) k_tc_hash(const uint32_t* __restrict
             __syncthreads();
         }
     }
-    // ---- light bin: one warp per item, private 512-slot table ----
+    // ---- light bin: one warp per item, private hash set of kLightSlots slots ----
     {
         constexpr int PW = light_warp_words<MODE>();
         uint32_t* key = smem + warp * PW;
@@ -240,12 +254,13 @@ __global__ void __launch_bounds__(kThreads) k_tc_hash(const uint32_t* __restrict
             const uint32_t v = light.v[item];
             if (ALIVE && !a.alive[v]) continue;
             const uint32_t vb = rowptr[v], dv = rowptr[v + 1] - vb;
-            const uint32_t bits = table_bits(dv);   // dv <= 256 -> bits <= 9
+            const uint32_t bits = table_bits(dv, kLightBits);   // dv <= light_max_deg: always a table
             build_table<MODE, ALIVE, CT>(col, a, vb, dv, key, cnt, pos, bits, lane, 32, false);
-            const unsigned long long h = probe_in_edges<MODE, ALIVE, CT>(rowptr, col, in_src, in_eid, a,
-                                                                          light.k0[item], light.k1[item], 32, key,
-                                                                          cnt, bits, false, vb, dv, s_incl, s_rb,
-                                                                          s_ecnt, lane);
+            unsigned long long h = 0;
+            const uint32_t k1 = light.k1[item];
+            for (uint32_t kb = light.k0[item]; kb < k1; kb += 32)
+                h += probe_batch<MODE, ALIVE, CT>(rowptr, col, in_src, in_eid, a, kb, min(kb + 32, k1), key, cnt,
+                                                  bits, false, vb, dv, s_incl, s_rb, s_ecnt, lane);
             hits += h;
             if (MODE == TC_VSUP) {
                 const unsigned long long t = warp_sum_u64(h);
@@ -322,7 +337,7 @@ static uint32_t heavy_bits_for(const ga_graph* g, int mode) {
     while ((((size_t)words << (cap + 1)) + kWarps * 96) * 4 <= 200 * 1024) cap++;
     if (g->heavy_bits_cap) cap = std::min(cap, g->heavy_bits_cap);
     uint32_t need = 5;
-    while ((1u << need) < 2 * g->heavy.max_dv) need++;
+    while ((1u << need) < 4 * g->heavy.max_dv) need++;
     return std::min(need, cap);
 }
 

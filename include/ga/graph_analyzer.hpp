@@ -1,0 +1,217 @@
+// graph_analyzer.hpp - C++ surface of the B200 triangle path with the reference's names, header-only over the C ABI
+// (graph_analyzer_b200.h). It mirrors VijayPraneethSai/graph_analyzer's src/graph.h, src/densest.h and src/dsg.h
+// for the GPU path (paths relative to that project):
+//
+//   Graph, build_graph_from_edges, load_graph            graph.h:19-96    (host CSR, same layout and orientation)
+//   PeelResult, operator==, density_value,               densest.h:46-78
+//     peel_arith_ok, peel_improves
+//   CoreLoopResult                                       dsg.h:687-691
+//   gpu_triangles                                        the counts gpu_tc.cu:165-229 obtains from kernels v1-v9
+//   gpu_edge_support / gpu_triangle_degrees              for_each_triangle / triangle_degrees (dsg.h:67-87)
+//   gpu_triangle_participation                           tc_per_vertex_alive (kernels.cuh:399) /
+//                                                        cpu_triangle_participation (densest.h:81)
+//   batch_peel_loop(n, T_full, num, den, DeviceGraph&)   batch_peel_loop (densest.h:279-303) + GpuBackend
+//   core_decomp_loop_inc(n, T_full, DeviceGraph&, core)  core_decomp_loop_inc (dsg.h:724-751) + GpuCoreBackendInc
+//
+// Everything lives in namespace ga; define GA_B200_GLOBAL_NAMES before including to also get the reference's
+// unqualified names. Errors follow the reference: functions that returned bool return false (load_graph), results
+// carry ok/error like PeelResult/CoreLoopResult, and the rest throw ga::Error (where the reference would exit(1)).
+#pragma once
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../graph_analyzer_b200.h"
+
+namespace ga {
+
+struct Error : std::runtime_error {
+    ga_status status;
+    Error(ga_status s, const std::string& what) : std::runtime_error(what), status(s) {}
+};
+
+inline void check(ga_status s) {
+    if (s != GA_OK) throw Error(s, std::string(ga_status_string(s)) + ": " + ga_last_error());
+}
+
+// ---- graph.h ----------------------------------------------------------------------------------------------------
+struct Graph {
+    uint32_t n = 0;
+    uint32_t m = 0;
+    std::vector<uint32_t> rowptr;
+    std::vector<uint32_t> col;
+    std::vector<uint32_t> src;
+    uint32_t max_out_degree = 0;
+};
+
+inline bool graphs_equal(const Graph& a, const Graph& b) {
+    return a.n == b.n && a.m == b.m && a.rowptr == b.rowptr && a.col == b.col && a.src == b.src &&
+           a.max_out_degree == b.max_out_degree;
+}
+
+// graph.h:38-67: unique undirected pairs without self loops -> oriented CSR.
+inline void build_graph_from_edges(uint32_t n, const std::vector<std::pair<uint32_t, uint32_t>>& edges, Graph& g) {
+    std::vector<uint32_t> flat(2 * edges.size());
+    for (size_t i = 0; i < edges.size(); i++) { flat[2 * i] = edges[i].first; flat[2 * i + 1] = edges[i].second; }
+    g.n = n;
+    g.m = (uint32_t)edges.size();
+    g.rowptr.assign((size_t)n + 1, 0);
+    g.col.assign(g.m, 0);
+    g.src.assign(g.m, 0);
+    check(ga_build_graph_from_edges(n, flat.data(), g.m, g.rowptr.data(), g.col.data(), g.src.data(),
+                                    &g.max_out_degree));
+}
+
+// graph.h:71-96: SNAP text edge list; prints the reason and returns false when the file cannot be used.
+inline bool load_graph(const char* path, Graph& g) {
+    ga_host_graph* h = nullptr;
+    const ga_status s = ga_load_graph(path, &h);
+    if (s != GA_OK) {
+        std::fprintf(stderr, "%s\n", ga_last_error());
+        return false;
+    }
+    g.n = h->n;
+    g.m = h->m;
+    g.max_out_degree = h->max_out_degree;
+    g.rowptr.assign(h->rowptr, h->rowptr + h->n + 1);
+    g.col.assign(h->col, h->col + h->m);
+    g.src.assign(h->src, h->src + h->m);
+    ga_host_graph_free(h);
+    return true;
+}
+
+// ---- densest.h helpers (integer decisions; densest.h:62-78) ----------------------------------------------------
+struct PeelResult {
+    uint64_t best_num = 0;
+    uint64_t best_den = 0;
+    uint32_t best_round = 0;
+    uint32_t rounds = 0;
+    std::vector<uint32_t> removed_round;
+    bool ok = true;
+    std::string error;
+};
+inline bool operator==(const PeelResult& a, const PeelResult& b) {
+    return a.best_num == b.best_num && a.best_den == b.best_den && a.best_round == b.best_round &&
+           a.rounds == b.rounds && a.removed_round == b.removed_round;
+}
+inline double density_value(uint64_t num, uint64_t den) { return den ? (double)num / (double)den : 0.0; }
+inline bool peel_arith_ok(uint32_t n, uint64_t T0, uint64_t num, uint64_t den, std::string* why = nullptr) {
+    auto fail = [&](const char* msg) { if (why) *why = msg; return false; };
+    if (den < 1 || den > (1ull << 20) || num > (1ull << 20)) return fail("eps = num/den needs 1 <= den <= 2^20 and num <= 2^20");
+    if (T0 >= (1ull << 32)) return fail("triangle count >= 2^32: uint32 tri[] counters could overflow");
+    if (n > 0 && T0 > UINT64_MAX / ((uint64_t)n * den)) return fail("tri*nalive*den could overflow uint64");
+    if (T0 > UINT64_MAX / (3ull * (den + num))) return fail("3*(den+num)*T could overflow uint64");
+    return true;
+}
+inline bool peel_improves(uint64_t T, uint64_t nalive, uint64_t best_num, uint64_t best_den) {
+    return best_den == 0 || T * best_den > best_num * nalive;
+}
+
+struct CoreLoopResult {
+    uint32_t rounds = 0, kmax = 0;
+    bool ok = true;
+    std::string error;
+};
+
+// ---- device-resident graph ---------------------------------------------------------------------------------------
+class DeviceGraph {
+  public:
+    explicit DeviceGraph(const Graph& g, int device = 0, void* stream = nullptr) : n_(g.n), m_(g.m) {
+        check(ga_graph_create(g.rowptr.data(), g.m ? g.col.data() : nullptr, g.n, g.m, device, stream, &h_));
+    }
+    ~DeviceGraph() { if (h_) ga_graph_destroy(h_); }
+    DeviceGraph(const DeviceGraph&) = delete;
+    DeviceGraph& operator=(const DeviceGraph&) = delete;
+
+    ga_graph* handle() const { return h_; }
+    uint32_t n() const { return n_; }
+    uint32_t m() const { return m_; }
+    void set_option(ga_option o, int64_t v) { check(ga_graph_set_option(h_, o, v)); }
+
+    uint64_t triangles() {
+        uint64_t t = 0;
+        check(ga_tc_count(h_, &t));
+        return t;
+    }
+    uint64_t edge_support(std::vector<uint32_t>& sup) {
+        sup.assign(m_, 0);
+        uint64_t t = 0;
+        check(ga_tc_support_edges(h_, sup.data(), &t));
+        return t;
+    }
+    uint64_t triangle_degrees(std::vector<uint64_t>& deg) {
+        deg.assign(n_, 0);
+        uint64_t t = 0;
+        check(ga_tc_support_vertices(h_, deg.data(), &t));
+        return t;
+    }
+    uint64_t triangle_participation(const std::vector<uint8_t>& alive, std::vector<uint32_t>& tri) {
+        tri.assign(n_, 0);
+        uint64_t t = 0;
+        check(ga_tc_participation(h_, alive.data(), tri.data(), &t));
+        return t;
+    }
+
+  private:
+    ga_graph* h_ = nullptr;
+    uint32_t n_, m_;
+};
+
+inline uint64_t gpu_triangles(const Graph& g, int device = 0) {
+    DeviceGraph d(g, device);
+    return d.triangles();
+}
+
+// batch_peel_loop (densest.h:279-303) on the device-resident loop. Same refusals (peel_arith_ok with T_full), same
+// round-0 cross-check of the device count against T_full, same PeelResult including removed_round.
+inline PeelResult batch_peel_loop(uint32_t n, uint64_t T_full, uint64_t num, uint64_t den, DeviceGraph& d) {
+    PeelResult r;
+    std::string why;
+    if (n != d.n()) { r.ok = false; r.error = "n differs from the device graph"; return r; }
+    if (!peel_arith_ok(n, T_full, num, den, &why)) { r.ok = false; r.error = why; return r; }
+    const uint64_t T0 = d.triangles();
+    if (T0 != T_full) { r.ok = false; r.error = "device triangle count in round 0 differs from CPU count"; return r; }
+    ga_peel_result res{};
+    r.removed_round.assign(n, UINT32_MAX);
+    const ga_status s = ga_batch_peel(d.handle(), num, den, &res, r.removed_round.data());
+    if (s != GA_OK) { r.ok = false; r.error = ga_last_error(); r.removed_round.clear(); return r; }
+    r.best_num = res.best_num;
+    r.best_den = res.best_den;
+    r.best_round = res.best_round;
+    r.rounds = res.rounds;
+    return r;
+}
+
+// core_decomp_loop_inc (dsg.h:724-751): core numbers (core_decomposition's, dsg.h:125) plus rounds and kmax.
+inline CoreLoopResult core_decomp_loop_inc(uint32_t n, uint64_t T_full, DeviceGraph& d, std::vector<uint32_t>& core) {
+    CoreLoopResult r;
+    if (T_full >= (1ull << 32)) { r.ok = false; r.error = "triangle count >= 2^32: uint32 tri[] counters could overflow"; return r; }
+    if (n != d.n()) { r.ok = false; r.error = "n differs from the device graph"; return r; }
+    if (d.triangles() != T_full) { r.ok = false; r.error = "device triangle count differs from CPU count"; return r; }
+    core.assign(n, 0);
+    ga_core_result res{};
+    const ga_status s = ga_core_decomposition(d.handle(), core.data(), &res);
+    if (s != GA_OK) { r.ok = false; r.error = ga_last_error(); return r; }
+    r.rounds = res.rounds;
+    r.kmax = res.kmax;
+    return r;
+}
+
+}  // namespace ga
+
+#ifdef GA_B200_GLOBAL_NAMES
+using ga::batch_peel_loop;
+using ga::build_graph_from_edges;
+using ga::core_decomp_loop_inc;
+using ga::CoreLoopResult;
+using ga::density_value;
+using ga::Graph;
+using ga::load_graph;
+using ga::peel_arith_ok;
+using ga::peel_improves;
+using ga::PeelResult;
+#endif
