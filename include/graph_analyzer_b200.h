@@ -150,6 +150,24 @@ ga_status ga_tc_count(ga_graph* g, uint64_t* triangles);
  * the launch must not include the one-time preparation. */
 ga_status ga_tc_count_async(ga_graph* g, uint64_t* d_triangles);
 
+/* Triangle count that allocates no memory at all. It has no counterpart in the reference; it exists for callers that
+ * cannot call cudaMalloc: a process whose device memory is entirely claimed by another allocator (for example a
+ * framework's caching pool that reserved the free HBM up front), or a latency-critical path that must not pay for
+ * cudaMalloc's implicit device synchronisation. The caller passes the oriented CSR in device memory of `device`
+ * (rowptr[n+1], col[m], the reference's layout) and receives the count in host memory; the only scratch the call
+ * uses (row owners and a few status words, 4 * GA_NOALLOC_MAX_EDGES bytes) is a fixed array compiled into the
+ * library, which every GPU that loads the library holds until the process exits.
+ *  - m > GA_NOALLOC_MAX_EDGES gives GA_ERR_CAPACITY; an invalid CSR gives GA_ERR_INVALID_GRAPH (checked on the
+ *    device before any row is followed).
+ *  - The first call on a device looks up the array's device address; make that first call before starting any
+ *    stream capture on that device.
+ *  - All calls share the one array per device: calls that overlap on the GPU (different streams or threads at the
+ *    same time) race and give wrong counts. Serialise them.
+ *  - Synchronous: returns after the count has been read back. */
+#define GA_NOALLOC_MAX_EDGES 4194304u
+ga_status ga_tc_count_noalloc(const uint32_t* d_rowptr, const uint32_t* d_col, uint32_t n, uint32_t m, int device,
+                              void* stream, uint64_t* triangles);
+
 /* Per-oriented-edge support, indexed like col: sup[e] = triangles containing edge e (for_each_triangle's
  * (e, i, j), dsg.h:67-79). `sup` is host memory of m entries. *triangles may be NULL. */
 ga_status ga_tc_support_edges(ga_graph* g, uint32_t* sup, uint64_t* triangles);
