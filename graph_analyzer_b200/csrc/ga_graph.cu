@@ -379,7 +379,10 @@ static ga_status create_common(const uint32_t* rowptr, const uint32_t* col, uint
     }
     ga_status s;
     if ((s = dalloc(g, &g->rowptr, (size_t)n + 1)) != GA_OK) return bail(s);
-    if ((s = dalloc(g, &g->col, m)) != GA_OK) return bail(s);
+    // col is padded by 4 zero entries so that 16-byte (quad) loads of the last row stay inside the allocation
+    if ((s = dalloc(g, &g->col, (size_t)m + 4)) != GA_OK) return bail(s);
+    if (cudaMemsetAsync(g->col + m, 0, 16, g->stream) != cudaSuccess)
+        return bail(fail(GA_ERR_CUDA, "cudaMemsetAsync failed"));
     if ((s = dalloc(g, &g->d_scalars, 64)) != GA_OK) return bail(s);
     if ((s = dalloc(g, &g->d_queue, 8)) != GA_OK) return bail(s);
     if (cudaMallocHost((void**)&g->h_scalars, 64 * 8) != cudaSuccess)

@@ -37,6 +37,10 @@
 
 namespace ga {
 
+#ifndef GA_TC_MIN_BLOCKS
+#define GA_TC_MIN_BLOCKS 8                // resident blocks per SM the hash kernel is compiled for (full occupancy)
+#endif
+
 constexpr int kWarps = 8;                 // warps per block of the hash kernel
 constexpr int kThreads = kWarps * 32;
 constexpr int kLightSlots = 512;          // per-warp hash set: anchors with out-degree <= 128 (load <= 1/4)
@@ -47,9 +51,12 @@ struct SlotLayout {   // 32-bit words per hash slot: key, +count (VSUP/ESUP), +p
     static constexpr int words = 1 + (MODE >= TC_VSUP ? 1 : 0) + (MODE == TC_ESUP ? 1 : 0);
 };
 
-// Shared memory of the light phase per warp: slots * words + incl[32] + rb[32] + ecnt[32].
+// Per-warp batch area: incl[32], rb[32], re[32], ecnt[32].
+constexpr int kBatchWords = 128;
+
+// Shared memory of the light phase per warp: slots * words + the batch area.
 template <int MODE>
-constexpr int light_warp_words() { return kLightSlots * SlotLayout<MODE>::words + 96; }
+constexpr int light_warp_words() { return kLightSlots * SlotLayout<MODE>::words + kBatchWords; }
 
 template <int MODE, bool ALIVE, class CT>
 __device__ __forceinline__ void on_hit(const TcArgs<CT>& a, uint32_t* cnt, uint32_t h, uint32_t* ecnt,
@@ -61,10 +68,44 @@ __device__ __forceinline__ void on_hit(const TcArgs<CT>& a, uint32_t* cnt, uint3
     if (MODE == TC_ESUP) atomicAdd(&a.esup[e], 1u);
 }
 
-// Probes one batch of up to 32 in-edges [kb, kend) of anchor v (one warp): lane l loads the l-th source u, a warp
-// scan of the list lengths flattens the lists N+(u) into one probe sequence and lane p takes probes p, p+32, ...
-// (each lane advances its owner index monotonically). A probe looks x up in the hash set (key, 2^bits slots) or, when
-// `global` is set, binary searches the sorted row N+(v) = col[vb, vb + dv). Returns this lane's hits.
+// Looks x (at col position e, probe list of in-edge `owner`) up in the hash set or, when `global`, by binary search in
+// the sorted row N+(v) = col[vb, vb + dv). Returns 1 on a hit and books the supports of the found triangle.
+template <int MODE, bool ALIVE, class CT>
+__device__ __forceinline__ uint32_t probe_one(const uint32_t* __restrict__ col, const TcArgs<CT>& a, uint32_t x,
+                                              uint32_t e, uint32_t owner, const uint32_t* key, uint32_t* cnt,
+                                              uint32_t bits, bool global, uint32_t vb, uint32_t dv,
+                                              uint32_t* s_ecnt) {
+    if (!global) {
+        const uint32_t mask = (1u << bits) - 1;
+        uint32_t h = hash_slot(x, bits);
+        for (;;) {
+            const uint32_t kk = key[h];
+            if (kk == x) {
+                on_hit<MODE, ALIVE, CT>(a, cnt, h, s_ecnt, owner, e);
+                return 1;
+            }
+            if (kk == GA_EMPTY) return 0;
+            h = (h + 1) & mask;
+        }
+    }
+    const uint32_t j = lower_bound_u32(col, vb, vb + dv, x);
+    if (j < vb + dv && col[j] == x && (!ALIVE || a.alive[x])) {
+        if (MODE >= TC_VSUP) atomicAdd(&s_ecnt[owner], 1u);
+        if (MODE == TC_VSUP) atomicAdd(&a.vsup[x], (CT)1);
+        if (MODE == TC_ESUP) {
+            atomicAdd(&a.esup[e], 1u);
+            atomicAdd(&a.esup[j], 1u);
+        }
+        return 1;
+    }
+    return 0;
+}
+
+// Probes one batch of up to 32 in-edges [kb, kend) of anchor v (one warp). Lane l loads the l-th source u; each list
+// N+(u) = col[rb, re) is cut into 16-byte quads (col is 16-byte aligned and padded, so a quad never leaves the
+// allocation), a warp scan of the quad counts flattens the 32 lists into one sequence, and lane p takes quads
+// p, p+32, ...: one 128-bit load, then up to 4 probes of the elements inside [rb, re). Each lane advances its owner
+// index monotonically. Returns this lane's hits.
 template <int MODE, bool ALIVE, class CT>
 __device__ __forceinline__ unsigned long long probe_batch(
     const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ col, const uint32_t* __restrict__ in_src,
@@ -72,50 +113,39 @@ __device__ __forceinline__ unsigned long long probe_batch(
     uint32_t* cnt, uint32_t bits, bool global, uint32_t vb, uint32_t dv, uint32_t* s_incl, uint32_t* s_rb,
     uint32_t* s_ecnt, uint32_t lane) {
     unsigned long long hits = 0;
-    const uint32_t mask = (1u << bits) - 1;
+    uint32_t* s_re = s_rb + 32;   // the caller's batch area: incl[32], rb[32], re[32], ecnt[32]
     const uint32_t k = kb + lane;
-    uint32_t d = 0, rb = 0, u = 0;
+    uint32_t nq = 0, rb = 0, re = 0, u = 0;
     if (k < kend) {
         u = in_src[k];
         if (!ALIVE || a.alive[u]) {
             rb = rowptr[u];
-            d = rowptr[u + 1] - rb;
+            re = rowptr[u + 1];
+            if (re > rb) nq = ((re + 3) >> 2) - (rb >> 2);
         }
     }
-    const uint32_t incl = warp_incl_scan(d, lane);
+    const uint32_t incl = warp_incl_scan(nq, lane);
     const uint32_t tot = __shfl_sync(GA_FULL_MASK, incl, 31);
     s_incl[lane] = incl;
     s_rb[lane] = rb;
+    s_re[lane] = re;
     __syncwarp();
+    const uint4* __restrict__ col4 = reinterpret_cast<const uint4*>(col);
     uint32_t owner = 0;
     for (uint32_t p = lane; p < tot; p += 32) {
         while (s_incl[owner] <= p) owner++;
-        const uint32_t e = s_rb[owner] + (p - (owner ? s_incl[owner - 1] : 0u));
-        const uint32_t x = col[e];
-        if (!global) {
-            uint32_t h = hash_slot(x, bits);
-            for (;;) {
-                const uint32_t kk = key[h];
-                if (kk == x) {
-                    hits++;
-                    on_hit<MODE, ALIVE, CT>(a, cnt, h, s_ecnt, owner, e);
-                    break;
-                }
-                if (kk == GA_EMPTY) break;
-                h = (h + 1) & mask;
-            }
-        } else {
-            const uint32_t j = lower_bound_u32(col, vb, vb + dv, x);
-            if (j < vb + dv && col[j] == x && (!ALIVE || a.alive[x])) {
-                hits++;
-                if (MODE >= TC_VSUP) atomicAdd(&s_ecnt[owner], 1u);
-                if (MODE == TC_VSUP) atomicAdd(&a.vsup[x], (CT)1);
-                if (MODE == TC_ESUP) {
-                    atomicAdd(&a.esup[e], 1u);
-                    atomicAdd(&a.esup[j], 1u);
-                }
-            }
-        }
+        const uint32_t lo = s_rb[owner], hi = s_re[owner];
+        const uint32_t q = (lo >> 2) + (p - (owner ? s_incl[owner - 1] : 0u));
+        const uint4 v = __ldg(col4 + q);
+        const uint32_t e0 = q << 2;
+        if (e0 >= lo && e0 < hi)
+            hits += probe_one<MODE, ALIVE, CT>(col, a, v.x, e0, owner, key, cnt, bits, global, vb, dv, s_ecnt);
+        if (e0 + 1 >= lo && e0 + 1 < hi)
+            hits += probe_one<MODE, ALIVE, CT>(col, a, v.y, e0 + 1, owner, key, cnt, bits, global, vb, dv, s_ecnt);
+        if (e0 + 2 >= lo && e0 + 2 < hi)
+            hits += probe_one<MODE, ALIVE, CT>(col, a, v.z, e0 + 2, owner, key, cnt, bits, global, vb, dv, s_ecnt);
+        if (e0 + 3 >= lo && e0 + 3 < hi)
+            hits += probe_one<MODE, ALIVE, CT>(col, a, v.w, e0 + 3, owner, key, cnt, bits, global, vb, dv, s_ecnt);
     }
     __syncwarp();
     if (MODE >= TC_VSUP) {
@@ -177,7 +207,7 @@ __device__ __forceinline__ void flush_table(const TcArgs<CT>& a, uint32_t vb, co
 }
 
 template <int MODE, bool ALIVE, class CT>
-__global__ void __launch_bounds__(kThreads) k_tc_hash(const uint32_t* __restrict__ rowptr,
+__global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const uint32_t* __restrict__ rowptr,
                                                       const uint32_t* __restrict__ col,
                                                       const uint32_t* __restrict__ in_src,
                                                       const uint32_t* __restrict__ in_eid, ga_items heavy,
@@ -197,8 +227,8 @@ __global__ void __launch_bounds__(kThreads) k_tc_hash(const uint32_t* __restrict
         uint32_t* key = smem;
         uint32_t* cnt = key + Smax;
         uint32_t* pos = cnt + (MODE >= TC_VSUP ? Smax : 0);
-        uint32_t* wbase = smem + (size_t)Smax * W + warp * 96;
-        uint32_t *s_incl = wbase, *s_rb = wbase + 32, *s_ecnt = wbase + 64;
+        uint32_t* wbase = smem + (size_t)Smax * W + warp * kBatchWords;
+        uint32_t *s_incl = wbase, *s_rb = wbase + 32, *s_ecnt = wbase + 96;
         s_ecnt[lane] = 0;
         for (;;) {
             if (threadIdx.x == 0) s_item = atomicAdd(&queue[0], 1u);
@@ -243,7 +273,7 @@ __global__ void __launch_bounds__(kThreads) k_tc_hash(const uint32_t* __restrict
         uint32_t* cnt = key + kLightSlots;
         uint32_t* pos = cnt + (MODE >= TC_VSUP ? kLightSlots : 0);
         uint32_t* s_incl = key + kLightSlots * W;
-        uint32_t *s_rb = s_incl + 32, *s_ecnt = s_incl + 64;
+        uint32_t *s_rb = s_incl + 32, *s_ecnt = s_incl + 96;
         s_ecnt[lane] = 0;
         __syncwarp();
         for (;;) {
@@ -325,7 +355,7 @@ __global__ void __launch_bounds__(256) k_tc_plain(const uint32_t* __restrict__ r
 
 template <int MODE>
 static size_t hash_smem_bytes(uint32_t heavy_bits) {
-    const size_t heavy = ((size_t)SlotLayout<MODE>::words << heavy_bits) + kWarps * 96;
+    const size_t heavy = ((size_t)SlotLayout<MODE>::words << heavy_bits) + kWarps * kBatchWords;
     const size_t light = (size_t)kWarps * light_warp_words<MODE>();
     return 4 * std::max(heavy, light);
 }
@@ -334,7 +364,7 @@ static uint32_t heavy_bits_for(const ga_graph* g, int mode) {
     // largest table that keeps the block within 200 KB of dynamic shared memory
     const int words = 1 + (mode >= TC_VSUP) + (mode == TC_ESUP);
     uint32_t cap = 5;
-    while ((((size_t)words << (cap + 1)) + kWarps * 96) * 4 <= 200 * 1024) cap++;
+    while ((((size_t)words << (cap + 1)) + kWarps * kBatchWords) * 4 <= 200 * 1024) cap++;
     if (g->heavy_bits_cap) cap = std::min(cap, g->heavy_bits_cap);
     uint32_t need = 5;
     while ((1u << need) < 4 * g->heavy.max_dv) need++;
