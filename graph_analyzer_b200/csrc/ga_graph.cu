@@ -509,8 +509,8 @@ ga_status ga_graph_set_option(ga_graph* g, ga_option opt, int64_t value) {
             return GA_OK;
         }
         case GA_OPT_HEAVY_TABLE_BITS:
-            if (value != 0 && (value < 5 || value > 15))
-                return fail(GA_ERR_INVALID_ARGUMENT, "GA_OPT_HEAVY_TABLE_BITS is 0 or 5..15");
+            if (value != 0 && (value < 3 || value > 13))
+                return fail(GA_ERR_INVALID_ARGUMENT, "GA_OPT_HEAVY_TABLE_BITS is 0 or 3..13");
             g->heavy_bits_cap = (uint32_t)value;
             return GA_OK;
         case GA_OPT_LIGHT_MAX_DEG: {

@@ -43,8 +43,8 @@ namespace ga {
 
 constexpr int kWarps = 8;                 // warps per block of the hash kernel
 constexpr int kThreads = kWarps * 32;
-constexpr int kLightSlots = 512;          // per-warp hash set: anchors with out-degree <= 128 (load <= 1/4)
-constexpr uint32_t kLightBits = 9;
+constexpr int kLightSlots = 512;          // per-warp hash set: 128 buckets of 4 slots, anchors with out-degree <= 128
+constexpr uint32_t kLightBits = 7;        // log2 buckets of the light set
 
 template <int MODE>
 struct SlotLayout {   // 32-bit words per hash slot: key, +count (VSUP/ESUP), +position (ESUP)
@@ -76,16 +76,21 @@ __device__ __forceinline__ uint32_t probe_one(const uint32_t* __restrict__ col, 
                                               uint32_t bits, bool global, uint32_t vb, uint32_t dv,
                                               uint32_t* s_ecnt) {
     if (!global) {
+        // bucketed set: 2^bits buckets of 4 slots; a bucket fills its slots in order, so an empty last slot ends
+        // the search. One 128-bit shared load resolves almost every lookup.
+        const uint4* key4 = reinterpret_cast<const uint4*>(key);
         const uint32_t mask = (1u << bits) - 1;
-        uint32_t h = hash_slot(x, bits);
+        uint32_t b = hash_slot(x, bits);
         for (;;) {
-            const uint32_t kk = key[h];
-            if (kk == x) {
-                on_hit<MODE, ALIVE, CT>(a, cnt, h, s_ecnt, owner, e);
+            const uint4 t = key4[b];
+            const uint32_t m = (t.x == x ? 1u : 0u) | (t.y == x ? 2u : 0u) | (t.z == x ? 4u : 0u) |
+                               (t.w == x ? 8u : 0u);
+            if (m) {
+                on_hit<MODE, ALIVE, CT>(a, cnt, 4 * b + (__ffs(m) - 1), s_ecnt, owner, e);
                 return 1;
             }
-            if (kk == GA_EMPTY) return 0;
-            h = (h + 1) & mask;
+            if (t.w == GA_EMPTY) return 0;
+            b = (b + 1) & mask;
         }
     }
     const uint32_t j = lower_bound_u32(col, vb, vb + dv, x);
@@ -160,21 +165,23 @@ __device__ __forceinline__ unsigned long long probe_batch(
     return hits;
 }
 
-// Table size for an anchor with dv out-neighbours: smallest power of two >= 4 dv (load <= 1/4, short miss probes),
-// at least 32; `cap` bits at most, where a load up to 1/2 is accepted. Returns 0 when even that does not fit.
+// Buckets (log2) for an anchor with dv out-neighbours: 2^b >= dv (at most one key per bucket on average), at least
+// 8 buckets, at most `cap` bits; an oversized anchor accepts up to 2 keys per bucket. Returns 0 when even that does
+// not fit (the caller then binary-searches the global row).
 __device__ __forceinline__ uint32_t table_bits(uint32_t dv, uint32_t cap) {
-    uint32_t b = 5;
-    while ((1u << b) < 4 * dv) b++;
+    uint32_t b = 3;
+    while ((1u << b) < dv) b++;
     if (b <= cap) return b;
-    return (1u << cap) >= 2 * dv ? cap : 0;
+    return (2u << cap) >= dv ? cap : 0;
 }
 
-// Clears 2^bits slots and inserts the (alive) members of N+(v); tid/nthr cover the cooperating threads.
+// Clears 2^bits buckets (4 slots each) and inserts the (alive) members of N+(v): a key takes the first free slot of
+// its bucket, or of the next bucket when all four are taken. tid/nthr cover the cooperating threads.
 template <int MODE, bool ALIVE, class CT>
 __device__ __forceinline__ void build_table(const uint32_t* __restrict__ col, const TcArgs<CT>& a, uint32_t vb,
                                             uint32_t dv, uint32_t* key, uint32_t* cnt, uint32_t* pos, uint32_t bits,
                                             uint32_t tid, uint32_t nthr, bool sync_block) {
-    const uint32_t S = 1u << bits, mask = S - 1;
+    const uint32_t S = 4u << bits, mask = (1u << bits) - 1;
     for (uint32_t s = tid; s < S; s += nthr) {
         key[s] = GA_EMPTY;
         if (MODE >= TC_VSUP) cnt[s] = 0;
@@ -183,9 +190,12 @@ __device__ __forceinline__ void build_table(const uint32_t* __restrict__ col, co
     for (uint32_t i = tid; i < dv; i += nthr) {
         const uint32_t x = col[vb + i];
         if (ALIVE && !a.alive[x]) continue;
-        uint32_t h = hash_slot(x, bits);
-        while (atomicCAS(&key[h], GA_EMPTY, x) != GA_EMPTY) h = (h + 1) & mask;
-        if (MODE == TC_ESUP) pos[h] = i;
+        uint32_t b = hash_slot(x, bits), slot = 4 * b;
+        while (atomicCAS(&key[slot], GA_EMPTY, x) != GA_EMPTY) {
+            slot++;
+            if ((slot & 3) == 0) { b = (b + 1) & mask; slot = 4 * b; }
+        }
+        if (MODE == TC_ESUP) pos[slot] = i;
     }
     if (sync_block) __syncthreads(); else __syncwarp();
 }
@@ -196,7 +206,7 @@ __device__ __forceinline__ void flush_table(const TcArgs<CT>& a, uint32_t vb, co
                                             const uint32_t* cnt, const uint32_t* pos, uint32_t bits, uint32_t tid,
                                             uint32_t nthr) {
     if (MODE < TC_VSUP) return;
-    const uint32_t S = 1u << bits;
+    const uint32_t S = 4u << bits;
     for (uint32_t s = tid; s < S; s += nthr) {
         const uint32_t c = cnt[s];
         if (c) {
@@ -223,7 +233,7 @@ __global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const ui
     // ---- heavy bin: the block shares one hash set of N+(v) per item; its warps pull 32-in-edge batches from a
     //      shared counter, so no warp waits for another until the item is exhausted ----
     {
-        const uint32_t Smax = 1u << heavy_bits_max;
+        const uint32_t Smax = 4u << heavy_bits_max;
         uint32_t* key = smem;
         uint32_t* cnt = key + Smax;
         uint32_t* pos = cnt + (MODE >= TC_VSUP ? Smax : 0);
@@ -355,19 +365,20 @@ __global__ void __launch_bounds__(256) k_tc_plain(const uint32_t* __restrict__ r
 
 template <int MODE>
 static size_t hash_smem_bytes(uint32_t heavy_bits) {
-    const size_t heavy = ((size_t)SlotLayout<MODE>::words << heavy_bits) + kWarps * kBatchWords;
+    const size_t heavy = ((size_t)SlotLayout<MODE>::words << (heavy_bits + 2)) + kWarps * kBatchWords;
     const size_t light = (size_t)kWarps * light_warp_words<MODE>();
     return 4 * std::max(heavy, light);
 }
 
+// log2 buckets of the heavy (block-wide) set: enough for the largest heavy anchor at one key per bucket, capped by
+// 200 KB of dynamic shared memory (and by GA_OPT_HEAVY_TABLE_BITS).
 static uint32_t heavy_bits_for(const ga_graph* g, int mode) {
-    // largest table that keeps the block within 200 KB of dynamic shared memory
     const int words = 1 + (mode >= TC_VSUP) + (mode == TC_ESUP);
-    uint32_t cap = 5;
-    while ((((size_t)words << (cap + 1)) + kWarps * kBatchWords) * 4 <= 200 * 1024) cap++;
+    uint32_t cap = 3;
+    while ((((size_t)words << (cap + 3)) + kWarps * kBatchWords) * 4 <= 200 * 1024) cap++;
     if (g->heavy_bits_cap) cap = std::min(cap, g->heavy_bits_cap);
-    uint32_t need = 5;
-    while ((1u << need) < 4 * g->heavy.max_dv) need++;
+    uint32_t need = 3;
+    while ((1u << need) < g->heavy.max_dv) need++;
     return std::min(need, cap);
 }
 

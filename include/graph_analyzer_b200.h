@@ -135,8 +135,8 @@ typedef enum ga_option {
                                  while-node (no host sync inside the loop)                                          */
     GA_OPT_MAX_ROUNDS = 3,    /* round cap of device-resident loops (0 = n + 1)                                    */
     GA_OPT_ITEM_WORK = 4,     /* probe work (list elements) per work item of the hash kernel (0 = 4096)            */
-    GA_OPT_HEAVY_TABLE_BITS = 5, /* log2 slots of the block-wide hash set; anchors that need more binary-search the
-                                    global row (0 = as large as shared memory allows, 5..15)                        */
+    GA_OPT_HEAVY_TABLE_BITS = 5, /* log2 buckets (4 slots each) of the block-wide hash set; anchors that need more
+                                    binary-search the global row (0 = as large as shared memory allows, 3..13)      */
     GA_OPT_LIGHT_MAX_DEG = 6  /* anchors with out-degree <= this use per-warp tables (0 = 128, at most 256)        */
 } ga_option;
 ga_status ga_graph_set_option(ga_graph* g, ga_option opt, int64_t value);

@@ -14,8 +14,8 @@ pytestmark = pytest.mark.gpu
 CONFIGS = {
     "auto": {},
     "plain": {1: 1},
-    "heavy_global": {6: 8, 5: 5},
-    "heavy_table": {6: 4, 5: 12},
+    "heavy_global": {6: 8, 5: 3},
+    "heavy_table": {6: 4, 5: 10},
     "small_items": {4: 16},
 }
 
