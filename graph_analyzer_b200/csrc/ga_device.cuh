@@ -104,7 +104,7 @@ struct ga_graph {
 
     // small device / pinned host scalars
     unsigned long long* d_scalars = nullptr;   // 64 slots
-    unsigned long long* h_scalars = nullptr;   // 64 slots, pinned
+    unsigned long long h_scalars[64] = {};     // host copies of small results
     uint32_t* d_queue = nullptr;               // 8 work-queue counters
 
     // options (ga_option)
@@ -118,12 +118,16 @@ struct ga_graph {
 
 namespace ga {
 
-// Device allocation owned by g (freed at destroy) and counted in g->bytes.
+// Configures the device's default memory pool once per process and device: freed blocks stay cached (up to
+// 8 GiB) so that graphs created and destroyed repeatedly reuse memory instead of returning it to the driver.
+ga_status init_pool(int device);
+
+// Device allocation owned by g (stream-ordered from the pool on g's stream, freed at destroy), counted in g->bytes.
 template <class T>
 inline ga_status dalloc(ga_graph* g, T** p, size_t count) {
     void* q = nullptr;
     const size_t bytes = (count ? count : 1) * sizeof(T);
-    cudaError_t e = cudaMalloc(&q, bytes);
+    cudaError_t e = cudaMallocAsync(&q, bytes, g->stream);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
         return fail(GA_ERR_OUT_OF_MEMORY, "cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));

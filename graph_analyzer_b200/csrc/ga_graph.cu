@@ -8,6 +8,7 @@
 //                          out-degree go to the block-wide "heavy" bin, the rest to the per-warp "light" bin.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 #include "ga_device.cuh"
 
@@ -115,9 +116,11 @@ ga_status exclusive_scan_u32(ga_graph* g, const uint32_t* in, uint32_t* out, uin
 __global__ void k_validate(const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ col, uint32_t n,
                            uint32_t m, unsigned long long* err) {
     uint32_t bad = 0;
+    uint32_t maxdeg = 0;
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
         const uint32_t b = rowptr[v], e = rowptr[v + 1];
         if (b > e || e > m) { bad |= 1; continue; }
+        maxdeg = max(maxdeg, e - b);
         for (uint32_t i = b; i < e; i++) {
             const uint32_t x = col[i];
             if (x >= n) bad |= 2;
@@ -126,6 +129,8 @@ __global__ void k_validate(const uint32_t* __restrict__ rowptr, const uint32_t* 
         }
     }
     if (bad) atomicOr(err, (unsigned long long)bad);
+    maxdeg = __reduce_max_sync(GA_FULL_MASK, maxdeg);
+    if ((threadIdx.x & 31) == 0 && maxdeg) atomicMax(err - 1, (unsigned long long)maxdeg);   // max out-degree
 }
 
 // src[e] = owner row; in-degree histogram.
@@ -238,11 +243,24 @@ void dfree(ga_graph* g, void* p) {
             g->allocations.erase(g->allocations.begin() + i);
             break;
         }
-    cudaFree(p);
+    cudaFreeAsync(p, g->stream);
 }
 
 ga_status use_device(const ga_graph* g) {
     GA_CUDA(cudaSetDevice(g->device));
+    return GA_OK;
+}
+
+ga_status init_pool(int device) {
+    static std::mutex mu;
+    static bool done[64] = {};
+    std::lock_guard<std::mutex> lock(mu);
+    if (device < 64 && done[device]) return GA_OK;
+    cudaMemPool_t pool;
+    GA_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t keep = 8ull << 30;
+    GA_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    if (device < 64) done[device] = true;
     return GA_OK;
 }
 
@@ -378,6 +396,7 @@ static ga_status create_common(const uint32_t* rowptr, const uint32_t* col, uint
         g->own_stream = true;
     }
     ga_status s;
+    if ((s = init_pool(device)) != GA_OK) return bail(s);
     if ((s = dalloc(g, &g->rowptr, (size_t)n + 1)) != GA_OK) return bail(s);
     // col is padded by 4 zero entries so that 16-byte (quad) loads of the last row stay inside the allocation
     if ((s = dalloc(g, &g->col, (size_t)m + 4)) != GA_OK) return bail(s);
@@ -385,18 +404,16 @@ static ga_status create_common(const uint32_t* rowptr, const uint32_t* col, uint
         return bail(fail(GA_ERR_CUDA, "cudaMemsetAsync failed"));
     if ((s = dalloc(g, &g->d_scalars, 64)) != GA_OK) return bail(s);
     if ((s = dalloc(g, &g->d_queue, 8)) != GA_OK) return bail(s);
-    if (cudaMallocHost((void**)&g->h_scalars, 64 * 8) != cudaSuccess)
-        return bail(fail(GA_ERR_OUT_OF_MEMORY, "cudaMallocHost failed"));
     const cudaMemcpyKind kind = from_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     if (cudaMemcpyAsync(g->rowptr, rowptr, ((size_t)n + 1) * 4, kind, g->stream) != cudaSuccess ||
         (m && cudaMemcpyAsync(g->col, col, (size_t)m * 4, kind, g->stream) != cudaSuccess))
         return bail(fail(GA_ERR_CUDA, "CSR copy to the device failed"));
+    // validation flags in d_scalars[63], max out-degree in d_scalars[62]
     unsigned long long* err = g->d_scalars + 63;
-    cudaMemsetAsync(err, 0, 8, g->stream);
+    cudaMemsetAsync(g->d_scalars + 62, 0, 16, g->stream);
     if (n) k_validate<<<grid_for(n, 256), 256, 0, g->stream>>>(g->rowptr, g->col, n, m, err);
-    unsigned long long herr = 0;
     uint32_t ends[2] = {0, 0};
-    cudaMemcpyAsync(&herr, err, 8, cudaMemcpyDeviceToHost, g->stream);
+    cudaMemcpyAsync(g->h_scalars + 62, g->d_scalars + 62, 16, cudaMemcpyDeviceToHost, g->stream);
     if (from_device) {
         cudaMemcpyAsync(&ends[0], g->rowptr, 4, cudaMemcpyDeviceToHost, g->stream);
         cudaMemcpyAsync(&ends[1], g->rowptr + n, 4, cudaMemcpyDeviceToHost, g->stream);
@@ -407,20 +424,10 @@ static ga_status create_common(const uint32_t* rowptr, const uint32_t* col, uint
     }
     if (from_device && (ends[0] != 0 || ends[1] != m))
         return bail(fail(GA_ERR_INVALID_GRAPH, "rowptr[0] must be 0 and rowptr[n] must equal m"));
-    if (herr)
+    if (g->h_scalars[63])
         return bail(fail(GA_ERR_INVALID_GRAPH, "invalid CSR (flags 0x%llx: 1 rowptr, 2 endpoint >= n, 4 self loop, "
-                                               "8 row not strictly ascending)", herr));
-    // max out-degree on the host side of the copy
-    uint32_t mx = 0;
-    if (!from_device) {
-        for (uint32_t v = 0; v < n; v++) mx = std::max(mx, rowptr[v + 1] - rowptr[v]);
-    } else {
-        std::vector<uint32_t> rp((size_t)n + 1);
-        if (cudaMemcpy(rp.data(), g->rowptr, ((size_t)n + 1) * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
-            return bail(fail(GA_ERR_CUDA, "rowptr download failed"));
-        for (uint32_t v = 0; v < n; v++) mx = std::max(mx, rp[v + 1] - rp[v]);
-    }
-    g->max_out_degree = mx;
+                                               "8 row not strictly ascending)", g->h_scalars[63]));
+    g->max_out_degree = (uint32_t)g->h_scalars[62];
     *out = g;
     return GA_OK;
 }
@@ -456,8 +463,8 @@ ga_status ga_graph_destroy(ga_graph* g) {
     cudaSetDevice(g->device);
     if (g->stream) cudaStreamSynchronize(g->stream);
     destroy_loops(g);
-    for (auto& a : g->allocations) cudaFree(a.first);
-    if (g->h_scalars) cudaFreeHost(g->h_scalars);
+    for (auto& a : g->allocations) cudaFreeAsync(a.first, g->stream);
+    if (g->stream) cudaStreamSynchronize(g->stream);
     if (g->own_stream && g->stream) cudaStreamDestroy(g->stream);
     delete g;
     return GA_OK;

@@ -61,7 +61,7 @@ struct ga_loops {
     uint32_t* item_c = nullptr;
     uint64_t item_cap = 0;
     ga::LoopScalars* sc = nullptr;    // device
-    ga::LoopScalars* h_sc = nullptr;  // pinned host copy
+    ga::LoopScalars h_sc = {};         // host copy of the round state
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     cudaGraph_t graph[2] = {nullptr, nullptr};
     unsigned grid_scan = 1, grid_update = 1, grid_retire = 1;
@@ -391,7 +391,6 @@ static ga_status ensure_loops(ga_graph* g) {
     GA_TRY(dalloc(g, &L->item_x, L->item_cap));
     GA_TRY(dalloc(g, &L->item_c, L->item_cap));
     GA_TRY(dalloc(g, &L->sc, 1));
-    GA_CUDA(cudaMallocHost((void**)&L->h_sc, sizeof(LoopScalars)));
     // fixed launch shapes (the graph body is captured once): grid-stride scans, persistent update grid
     int occ = 0;
     GA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_frontier_update, kUpdWarps * 32, 0));
@@ -408,7 +407,6 @@ void destroy_loops(ga_graph* g) {
         if (L->exec[k]) cudaGraphExecDestroy(L->exec[k]);
         if (L->graph[k]) cudaGraphDestroy(L->graph[k]);
     }
-    if (L->h_sc) cudaFreeHost(L->h_sc);
     delete L;   // device buffers belong to g->allocations
     g->loops = nullptr;
 }
@@ -509,16 +507,16 @@ static ga_status run_loop(ga_graph* g, uint64_t num, uint64_t den, LoopScalars* 
         } else {
             for (uint64_t r = 0;; r++) {
                 GA_TRY(enqueue_round<KIND>(g, st, 0, 0));
-                GA_CUDA(cudaMemcpyAsync(L->h_sc, L->sc, sizeof(LoopScalars), cudaMemcpyDeviceToHost, st));
+                GA_CUDA(cudaMemcpyAsync(&L->h_sc, L->sc, sizeof(LoopScalars), cudaMemcpyDeviceToHost, st));
                 GA_CUDA(cudaStreamSynchronize(st));
-                if (!L->h_sc->cont) break;
+                if (!L->h_sc.cont) break;
                 if (r > (uint64_t)max_rounds + 1) return fail(GA_ERR_ROUND_LIMIT, "host loop bound reached");
             }
         }
     }
-    GA_CUDA(cudaMemcpyAsync(L->h_sc, L->sc, sizeof(LoopScalars), cudaMemcpyDeviceToHost, st));
+    GA_CUDA(cudaMemcpyAsync(&L->h_sc, L->sc, sizeof(LoopScalars), cudaMemcpyDeviceToHost, st));
     GA_CUDA(cudaStreamSynchronize(st));
-    *result = *L->h_sc;
+    *result = L->h_sc;
     switch (result->status) {
         case LS_OK: break;
         case LS_ROUND_LIMIT: return fail(GA_ERR_ROUND_LIMIT, "round cap %u reached", result->max_rounds);
