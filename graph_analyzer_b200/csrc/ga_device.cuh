@@ -108,7 +108,7 @@ struct ga_graph {
     uint32_t* d_queue = nullptr;               // 8 work-queue counters
 
     // options (ga_option)
-    int64_t opt_tc_kernel = 0, opt_loop_mode = 0, opt_max_rounds = 0;
+    int64_t opt_tc_kernel = 0, opt_loop_mode = 0, opt_max_rounds = 0, opt_update_mode = 0;
     uint32_t item_work = 4096, heavy_bits_cap = 0, light_max_deg = 128;
 
     // every device allocation, freed by ga_graph_destroy
@@ -150,8 +150,12 @@ void destroy_loops(ga_graph* g);
 // Builds src, in-lists and work lists (idempotent).
 ga_status prepare(ga_graph* g);
 
-// Device-wide exclusive scan of n uint32 values (in place allowed); out[n] receives the total when out has n+1 slots
-// and `write_total` is set. Uses scratch from g.
+// Device-wide exclusive scan of n uint32 values (in place allowed) on g's stream.
 ga_status exclusive_scan_u32(ga_graph* g, const uint32_t* in, uint32_t* out, uint32_t n, bool write_total);
+// In-place exclusive scan of n uint64 values on g's stream.
+ga_status scan_u64(ga_graph* g, unsigned long long* data, uint64_t n);
+
+// Frees the loop state and its device buffers (the next loop call rebuilds them).
+void reset_loops(ga_graph* g);
 
 }  // namespace ga

@@ -110,6 +110,10 @@ ga_status exclusive_scan_u32(ga_graph* g, const uint32_t* in, uint32_t* out, uin
     return GA_OK;
 }
 
+ga_status scan_u64(ga_graph* g, unsigned long long* data, uint64_t n) {
+    return scan_impl<unsigned long long>(g->stream, data, data, n, false);
+}
+
 // ---- validation and derived structures -------------------------------------------------------------------------
 
 // Flags in *err: 1 rowptr not monotone / beyond m, 2 endpoint >= n, 4 self loop, 8 row not strictly ascending.
@@ -509,6 +513,14 @@ ga_status ga_graph_set_option(ga_graph* g, ga_option opt, int64_t value) {
             return GA_OK;
         case GA_OPT_MAX_ROUNDS:
             g->opt_max_rounds = value;
+            return GA_OK;
+        case GA_OPT_UPDATE_MODE:
+            if (value > 2) return fail(GA_ERR_INVALID_ARGUMENT, "GA_OPT_UPDATE_MODE is 0, 1 or 2");
+            if (value != g->opt_update_mode) {
+                GA_TRY(use_device(g));
+                reset_loops(g);
+                g->opt_update_mode = value;
+            }
             return GA_OK;
         case GA_OPT_ITEM_WORK: {
             const uint32_t v = value ? (uint32_t)std::min<int64_t>(value, 1 << 30) : 4096;

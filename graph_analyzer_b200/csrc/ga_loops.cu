@@ -30,7 +30,8 @@
 
 namespace ga {
 
-constexpr uint32_t kChunk = 256;     // neighbours of a frontier vertex per update item
+constexpr uint32_t kChunk = 256;     // neighbours of a frontier vertex per update item (enumeration update)
+constexpr uint32_t kListChunk = 1024;   // incidence entries of a frontier vertex per update item (list update)
 constexpr int kUpdWarps = 8;
 
 enum LoopKind { LOOP_PEEL = 0, LOOP_CORE = 1 };
@@ -65,6 +66,11 @@ struct ga_loops {
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     cudaGraph_t graph[2] = {nullptr, nullptr};
     unsigned grid_scan = 1, grid_update = 1, grid_retire = 1;
+    // triangle incidence lists (built once per graph when memory allows): for every vertex v the other two corners
+    // of each triangle through v, in inc[inc_ptr[v] .. inc_ptr[v+1])
+    int lists = -1;                    // -1 undecided, 0 enumeration update, 1 incidence-list update
+    uint2* inc = nullptr;
+    unsigned long long* inc_ptr = nullptr;   // n+1
 };
 
 namespace ga {
@@ -94,8 +100,10 @@ __global__ void k_loop_scalars(LoopScalars* sc, const unsigned long long* total,
 
 // Appends the frontier vertex v (mark kernels): its id to frontier[], and ceil(deg(v) / kChunk) update items.
 // All 32 lanes call it; `take` marks the lanes that append. One atomic per warp for each list.
+// With incidence lists (inc_ptr != null) the items are ceil(|Tri(v)| / kListChunk) slices of v's list instead.
 __device__ __forceinline__ void append_frontier(bool take, uint32_t v, const uint32_t* __restrict__ rowptr,
-                                                const uint32_t* __restrict__ in_ptr, LoopScalars* sc,
+                                                const uint32_t* __restrict__ in_ptr,
+                                                const unsigned long long* __restrict__ inc_ptr, LoopScalars* sc,
                                                 uint32_t* __restrict__ frontier, uint32_t* __restrict__ item_x,
                                                 uint32_t* __restrict__ item_c, uint32_t lane) {
     const uint32_t bal = __ballot_sync(GA_FULL_MASK, take);
@@ -106,8 +114,12 @@ __device__ __forceinline__ void append_frontier(bool take, uint32_t v, const uin
     uint32_t nc = 0;
     if (take) {
         frontier[base + __popc(bal & ((1u << lane) - 1))] = v;
-        const uint32_t deg = rowptr[v + 1] - rowptr[v] + in_ptr[v + 1] - in_ptr[v];
-        nc = (deg + kChunk - 1) / kChunk;
+        if (inc_ptr) {
+            nc = (uint32_t)((inc_ptr[v + 1] - inc_ptr[v] + kListChunk - 1) / kListChunk);
+        } else {
+            const uint32_t deg = rowptr[v + 1] - rowptr[v] + in_ptr[v + 1] - in_ptr[v];
+            nc = (deg + kChunk - 1) / kChunk;
+        }
     }
     const uint32_t incl = warp_incl_scan(nc, lane);
     const uint32_t tot = __shfl_sync(GA_FULL_MASK, incl, 31);
@@ -138,7 +150,8 @@ __global__ void __launch_bounds__(256) k_peel_mark(LoopScalars* sc, const uint32
                                                    uint32_t* alive0, uint32_t* alive1,
                                                    uint32_t* __restrict__ frontier, uint32_t* __restrict__ item_x,
                                                    uint32_t* __restrict__ item_c, const uint32_t* __restrict__ rowptr,
-                                                   const uint32_t* __restrict__ in_ptr) {
+                                                   const uint32_t* __restrict__ in_ptr,
+                                                   const unsigned long long* __restrict__ inc_ptr) {
     const uint32_t p = sc->parity;
     const uint32_t* in = p ? alive1 : alive0;
     uint32_t* outl = p ? alive0 : alive1;
@@ -167,7 +180,7 @@ __global__ void __launch_bounds__(256) k_peel_mark(LoopScalars* sc, const uint32
                 removed_round[v] = round;
             }
         }
-        append_frontier(rem, v, rowptr, in_ptr, sc, frontier, item_x, item_c, lane);
+        append_frontier(rem, v, rowptr, in_ptr, inc_ptr, sc, frontier, item_x, item_c, lane);
         append_survivor(valid && !rem, v, outl, &sc->alive_count[p ^ 1], lane);
     }
 }
@@ -192,7 +205,8 @@ __global__ void __launch_bounds__(256) k_core_mark(LoopScalars* sc, const uint32
                                                    uint32_t* alive0, uint32_t* alive1,
                                                    uint32_t* __restrict__ frontier, uint32_t* __restrict__ item_x,
                                                    uint32_t* __restrict__ item_c, const uint32_t* __restrict__ rowptr,
-                                                   const uint32_t* __restrict__ in_ptr) {
+                                                   const uint32_t* __restrict__ in_ptr,
+                                                   const unsigned long long* __restrict__ inc_ptr) {
     const uint32_t p = sc->parity;
     const uint32_t* in = p ? alive1 : alive0;
     uint32_t* outl = p ? alive0 : alive1;
@@ -213,7 +227,7 @@ __global__ void __launch_bounds__(256) k_core_mark(LoopScalars* sc, const uint32
                 core[v] = k;
             }
         }
-        append_frontier(rem, v, rowptr, in_ptr, sc, frontier, item_x, item_c, lane);
+        append_frontier(rem, v, rowptr, in_ptr, inc_ptr, sc, frontier, item_x, item_c, lane);
         append_survivor(valid && !rem, v, outl, &sc->alive_count[p ^ 1], lane);
     }
 }
@@ -320,6 +334,45 @@ __global__ void __launch_bounds__(kUpdWarps * 32) k_frontier_update(
     }
 }
 
+// Incidence-list update: one warp per item = up to kListChunk entries (y, w) of frontier vertex x's list, read
+// coalesced. The triangle {x, y, w} still exists iff y and w are alive or in the frontier; it is handled by its
+// smallest-id frontier corner (kernels.cuh:607), which subtracts 1 from tri[] of its alive corners and counts it as
+// destroyed. Over a whole run every triangle is read at most three times (once per corner).
+__global__ void __launch_bounds__(256) k_frontier_update_list(LoopScalars* sc, const uint2* __restrict__ inc,
+                                                              const unsigned long long* __restrict__ inc_ptr,
+                                                              const uint32_t* __restrict__ item_x,
+                                                              const uint32_t* __restrict__ item_c,
+                                                              const uint8_t* __restrict__ state,
+                                                              uint32_t* __restrict__ tri) {
+    __shared__ unsigned long long s_red[8];
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t nitems = sc->nitems;
+    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long destroyed = 0;
+    for (uint32_t it = gwarp; it < nitems; it += nwarps) {
+        const uint32_t x = item_x[it];
+        const unsigned long long b = inc_ptr[x] + (unsigned long long)item_c[it] * kListChunk;
+        const unsigned long long e = min(inc_ptr[x + 1], b + kListChunk);
+        for (unsigned long long i = b + lane; i < e; i += 32) {
+            const uint2 yw = inc[i];
+            const uint8_t sy = state[yw.x], sw = state[yw.y];
+            if (!sy || !sw) continue;                               // destroyed in an earlier round
+            if ((sy == 2 && yw.x < x) || (sw == 2 && yw.y < x)) continue;   // a smaller frontier corner owns it
+            destroyed++;
+            if (sy == 1) atomicSub(&tri[yw.x], 1u);
+            if (sw == 1) atomicSub(&tri[yw.y], 1u);
+        }
+    }
+    destroyed = warp_sum_u64(destroyed);
+    if (lane == 0) s_red[w] = destroyed;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int i = 0; i < 8; i++) t += s_red[i];
+        if (t) atomicAdd(&sc->destroyed, t);
+    }
+}
+
 // Retires the frontier (state 2 -> 0); the last block to finish closes the round: nalive -= |F|, T -= destroyed,
 // checks (densest.h:298, dsg.h:744), resets the per-round counters, flips the alive-list parity and sets the loop
 // condition (cudaGraphSetConditional when running as a graph body).
@@ -411,20 +464,104 @@ void destroy_loops(ga_graph* g) {
     g->loops = nullptr;
 }
 
+void reset_loops(ga_graph* g) {
+    ga_loops* L = g->loops;
+    if (!L) return;
+    cudaStreamSynchronize(g->stream);
+    void* bufs[] = {L->tri, L->state, L->out, L->alive[0], L->alive[1], L->frontier, L->item_x, L->item_c, L->sc,
+                    L->inc, L->inc_ptr};
+    for (void* b : bufs) dfree(g, b);
+    destroy_loops(g);
+}
+
+__global__ void k_widen_counts(const uint32_t* __restrict__ tri, unsigned long long* __restrict__ out, uint32_t n) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v <= n; v += gridDim.x * blockDim.x)
+        out[v] = v < n ? tri[v] : 0ull;
+}
+
+__global__ void k_list_lengths(const unsigned long long* __restrict__ inc_ptr, uint32_t* __restrict__ tri,
+                               uint32_t n, unsigned long long* total) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        tri[v] = (uint32_t)(inc_ptr[v + 1] - inc_ptr[v]);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *total = inc_ptr[n] / 3;
+}
+
+// Decides the update method once per graph. With GA_OPT_UPDATE_MODE 0 (auto) or 2, the incidence lists are built
+// when their 24 * T bytes (plus 8 (n + 1)) can be allocated; auto falls back to the enumeration update otherwise.
+// tri[] must hold the per-vertex triangle counts of the whole graph and T0 their total / 3.
+static ga_status build_lists(ga_graph* g, uint64_t T0) {
+    ga_loops* L = g->loops;
+    if (L->lists >= 0) return GA_OK;
+    if (g->opt_update_mode == 1 || g->n == 0) { L->lists = 0; return GA_OK; }
+    cudaStream_t st = g->stream;
+    const uint32_t n = g->n;
+    const uint64_t entries = 3 * T0;
+    const uint64_t need_items = (uint64_t)n + entries / kListChunk + 1;
+    ga_status s = dalloc(g, &L->inc_ptr, (size_t)n + 1);
+    if (s == GA_OK) s = dalloc(g, &L->inc, entries ? entries : 1);
+    uint32_t *ix = nullptr, *ic = nullptr;
+    if (s == GA_OK && need_items > L->item_cap) {
+        s = dalloc(g, &ix, need_items);
+        if (s == GA_OK) s = dalloc(g, &ic, need_items);
+    }
+    uint32_t* fill = nullptr;   // n cursors + the overflow counter
+    if (s == GA_OK && cudaMallocAsync((void**)&fill, ((size_t)n + 1) * 4, st) != cudaSuccess) {
+        (void)cudaGetLastError();
+        s = fail(GA_ERR_OUT_OF_MEMORY, "incidence list cursors do not fit");
+    }
+    if (s != GA_OK) {
+        dfree(g, L->inc_ptr); dfree(g, L->inc); dfree(g, ix); dfree(g, ic);
+        L->inc_ptr = nullptr; L->inc = nullptr;
+        if (g->opt_update_mode == 2) return s;
+        clear_error();
+        L->lists = 0;
+        return GA_OK;
+    }
+    if (ix) {
+        dfree(g, L->item_x); dfree(g, L->item_c);
+        L->item_x = ix; L->item_c = ic; L->item_cap = need_items;
+    }
+    k_widen_counts<<<grid_for((uint64_t)n + 1, 256), 256, 0, st>>>(L->tri, L->inc_ptr, n);
+    GA_CUDA(cudaGetLastError());
+    GA_TRY(scan_u64(g, L->inc_ptr, (uint64_t)n + 1));
+    GA_CUDA(cudaMemsetAsync(fill, 0, ((size_t)n + 1) * 4, st));
+    TcArgs<unsigned int> a{};
+    a.total = g->d_scalars + 1;
+    a.inc = L->inc;
+    a.inc_ptr = L->inc_ptr;
+    a.fill = fill;
+    a.overflow = fill + n;
+    s = run_tc<TC_LIST, false, unsigned int>(g, a, true);
+    uint32_t overflow = 0;
+    if (s == GA_OK && cudaMemcpyAsync(&overflow, fill + n, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        s = fail(GA_ERR_CUDA, "overflow read failed");
+    cudaFreeAsync(fill, st);
+    GA_TRY(s);
+    GA_CUDA(cudaStreamSynchronize(st));
+    if (overflow) return fail(GA_ERR_DEVICE_CHECK, "triangle listing disagreed with the count (%u entries)", overflow);
+    L->lists = 1;
+    return GA_OK;
+}
+
 // Enqueues one round on `st` (kernel parameters are fixed, everything per-round lives in *sc).
 template <int KIND>
 static ga_status enqueue_round(ga_graph* g, cudaStream_t st, cudaGraphConditionalHandle h, int use_h) {
     ga_loops* L = g->loops;
+    const unsigned long long* inc_ptr = L->lists == 1 ? L->inc_ptr : nullptr;
     if (KIND == LOOP_PEEL) {
         k_peel_mark<<<L->grid_scan, 256, 0, st>>>(L->sc, L->tri, L->state, L->out, L->alive[0], L->alive[1], L->frontier,
-                                             L->item_x, L->item_c, g->rowptr, g->in_ptr);
+                                             L->item_x, L->item_c, g->rowptr, g->in_ptr, inc_ptr);
     } else {
         k_core_min<<<L->grid_scan, 256, 0, st>>>(L->sc, L->tri, L->alive[0], L->alive[1]);
         k_core_mark<<<L->grid_scan, 256, 0, st>>>(L->sc, L->tri, L->state, L->out, L->alive[0], L->alive[1], L->frontier,
-                                             L->item_x, L->item_c, g->rowptr, g->in_ptr);
+                                             L->item_x, L->item_c, g->rowptr, g->in_ptr, inc_ptr);
     }
-    k_frontier_update<<<L->grid_update, kUpdWarps * 32, 0, st>>>(L->sc, g->rowptr, g->col, g->in_ptr, g->in_src,
-                                                            L->item_x, L->item_c, L->state, L->tri);
+    if (L->lists == 1)
+        k_frontier_update_list<<<L->grid_update, 256, 0, st>>>(L->sc, L->inc, L->inc_ptr, L->item_x, L->item_c,
+                                                               L->state, L->tri);
+    else
+        k_frontier_update<<<L->grid_update, kUpdWarps * 32, 0, st>>>(L->sc, g->rowptr, g->col, g->in_ptr, g->in_src,
+                                                                L->item_x, L->item_c, L->state, L->tri);
     k_retire_tail<KIND><<<L->grid_retire, 256, 0, st>>>(L->sc, L->state, L->frontier, h, use_h);
     GA_CUDA(cudaGetLastError());
     return GA_OK;
@@ -474,11 +611,17 @@ static ga_status run_loop(ga_graph* g, uint64_t num, uint64_t den, LoopScalars* 
     ga_loops* L = g->loops;
     cudaStream_t st = g->stream;
     const uint32_t n = g->n;
-    // tri[] = triangles per vertex on the whole graph (uint32 counters; T < 2^32 is checked below)
-    TcArgs<unsigned int> a{};
-    a.total = g->d_scalars;
-    a.vsup = L->tri;
-    GA_TRY((run_tc<TC_VSUP, false, unsigned int>(g, a, true)));
+    // tri[] = triangles per vertex on the whole graph (uint32 counters; T < 2^32 is checked below): the list lengths
+    // when the incidence lists exist, else one per-vertex triangle pass
+    if (L->lists == 1) {
+        if (n) k_list_lengths<<<grid_for(n, 256), 256, 0, st>>>(L->inc_ptr, L->tri, n, g->d_scalars);
+        GA_CUDA(cudaGetLastError());
+    } else {
+        TcArgs<unsigned int> a{};
+        a.total = g->d_scalars;
+        a.vsup = L->tri;
+        GA_TRY((run_tc<TC_VSUP, false, unsigned int>(g, a, true)));
+    }
     if (n) {
         k_loop_init<<<grid_for(n, 256), 256, 0, st>>>(L->state, L->out, L->alive[0], n);
         GA_CUDA(cudaGetLastError());
@@ -495,6 +638,7 @@ static ga_status run_loop(ga_graph* g, uint64_t num, uint64_t den, LoopScalars* 
             return fail(GA_ERR_ARITH, "tri*nalive*den could overflow uint64");
         if (T0 > UINT64_MAX / (3ull * (den + num))) return fail(GA_ERR_ARITH, "3*(den+num)*T could overflow uint64");
     }
+    GA_TRY(build_lists(g, T0));
     const uint64_t cap = g->opt_max_rounds ? (uint64_t)g->opt_max_rounds : (uint64_t)n + 1;
     const uint32_t max_rounds = (uint32_t)std::min<uint64_t>(cap, UINT32_MAX);
     k_loop_scalars<<<1, 1, 0, st>>>(L->sc, g->d_scalars, n, num, den, max_rounds);

@@ -46,26 +46,45 @@ constexpr int kThreads = kWarps * 32;
 constexpr int kLightSlots = 512;          // per-warp hash set: 128 buckets of 4 slots, anchors with out-degree <= 128
 constexpr uint32_t kLightBits = 7;        // log2 buckets of the light set
 
+// VSUP and ESUP book per-slot and per-in-edge counters; COUNT and LIST do not.
+__host__ __device__ constexpr bool counters(int mode) { return mode == TC_VSUP || mode == TC_ESUP; }
+
 template <int MODE>
 struct SlotLayout {   // 32-bit words per hash slot: key, +count (VSUP/ESUP), +position (ESUP)
-    static constexpr int words = 1 + (MODE >= TC_VSUP ? 1 : 0) + (MODE == TC_ESUP ? 1 : 0);
+    static constexpr int words = 1 + (counters(MODE) ? 1 : 0) + (MODE == TC_ESUP ? 1 : 0);
 };
 
-// Per-warp batch area: incl[32], rb[32], re[32], ecnt[32].
-constexpr int kBatchWords = 128;
+// Per-warp batch area: incl[32], rb[32], re[32], ecnt[32], u[32].
+constexpr int kBatchWords = 160;
 
 // Shared memory of the light phase per warp: slots * words + the batch area.
 template <int MODE>
 constexpr int light_warp_words() { return kLightSlots * SlotLayout<MODE>::words + kBatchWords; }
 
+// Writes the triangle (u lowest, v middle, x highest) into the incidence list of each corner. A list is sized by the
+// counting pass; an entry that would land past its list's end is dropped and counted in *overflow instead.
+template <class CT>
+__device__ __forceinline__ void list_one(const TcArgs<CT>& a, uint32_t c, uint32_t p, uint32_t q) {
+    const unsigned long long pos = a.inc_ptr[c] + atomicAdd(&a.fill[c], 1u);
+    if (pos < a.inc_ptr[c + 1]) a.inc[pos] = make_uint2(p, q);
+    else atomicAdd(a.overflow, 1u);
+}
+template <class CT>
+__device__ __forceinline__ void list_triangle(const TcArgs<CT>& a, uint32_t u, uint32_t v, uint32_t x) {
+    list_one(a, x, u, v);
+    list_one(a, u, v, x);
+    list_one(a, v, u, x);
+}
+
 template <int MODE, bool ALIVE, class CT>
 __device__ __forceinline__ void on_hit(const TcArgs<CT>& a, uint32_t* cnt, uint32_t h, uint32_t* ecnt,
-                                       uint32_t owner, uint32_t e) {
-    if (MODE >= TC_VSUP) {
+                                       uint32_t owner, uint32_t e, uint32_t anchor, uint32_t x, const uint32_t* s_u) {
+    if (counters(MODE)) {
         atomicAdd(&cnt[h], 1u);
         atomicAdd(&ecnt[owner], 1u);
     }
     if (MODE == TC_ESUP) atomicAdd(&a.esup[e], 1u);
+    if (MODE == TC_LIST) list_triangle(a, s_u[owner], anchor, x);
 }
 
 // Looks x (at col position e, probe list of in-edge `owner`) up in the hash set or, when `global`, by binary search in
@@ -74,7 +93,7 @@ template <int MODE, bool ALIVE, class CT>
 __device__ __forceinline__ uint32_t probe_one(const uint32_t* __restrict__ col, const TcArgs<CT>& a, uint32_t x,
                                               uint32_t e, uint32_t owner, const uint32_t* key, uint32_t* cnt,
                                               uint32_t bits, bool global, uint32_t vb, uint32_t dv,
-                                              uint32_t* s_ecnt) {
+                                              uint32_t* s_ecnt, uint32_t anchor, const uint32_t* s_u) {
     if (!global) {
         // bucketed set: 2^bits buckets of 4 slots; a bucket fills its slots in order, so an empty last slot ends
         // the search. One 128-bit shared load resolves almost every lookup.
@@ -86,7 +105,7 @@ __device__ __forceinline__ uint32_t probe_one(const uint32_t* __restrict__ col, 
             const uint32_t m = (t.x == x ? 1u : 0u) | (t.y == x ? 2u : 0u) | (t.z == x ? 4u : 0u) |
                                (t.w == x ? 8u : 0u);
             if (m) {
-                on_hit<MODE, ALIVE, CT>(a, cnt, 4 * b + (__ffs(m) - 1), s_ecnt, owner, e);
+                on_hit<MODE, ALIVE, CT>(a, cnt, 4 * b + (__ffs(m) - 1), s_ecnt, owner, e, anchor, x, s_u);
                 return 1;
             }
             if (t.w == GA_EMPTY) return 0;
@@ -95,12 +114,13 @@ __device__ __forceinline__ uint32_t probe_one(const uint32_t* __restrict__ col, 
     }
     const uint32_t j = lower_bound_u32(col, vb, vb + dv, x);
     if (j < vb + dv && col[j] == x && (!ALIVE || a.alive[x])) {
-        if (MODE >= TC_VSUP) atomicAdd(&s_ecnt[owner], 1u);
+        if (counters(MODE)) atomicAdd(&s_ecnt[owner], 1u);
         if (MODE == TC_VSUP) atomicAdd(&a.vsup[x], (CT)1);
         if (MODE == TC_ESUP) {
             atomicAdd(&a.esup[e], 1u);
             atomicAdd(&a.esup[j], 1u);
         }
+        if (MODE == TC_LIST) list_triangle(a, s_u[owner], anchor, x);
         return 1;
     }
     return 0;
@@ -116,9 +136,10 @@ __device__ __forceinline__ unsigned long long probe_batch(
     const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ col, const uint32_t* __restrict__ in_src,
     const uint32_t* __restrict__ in_eid, const TcArgs<CT>& a, uint32_t kb, uint32_t kend, const uint32_t* key,
     uint32_t* cnt, uint32_t bits, bool global, uint32_t vb, uint32_t dv, uint32_t* s_incl, uint32_t* s_rb,
-    uint32_t* s_ecnt, uint32_t lane) {
+    uint32_t* s_ecnt, uint32_t lane, uint32_t anchor) {
     unsigned long long hits = 0;
-    uint32_t* s_re = s_rb + 32;   // the caller's batch area: incl[32], rb[32], re[32], ecnt[32]
+    uint32_t* s_re = s_rb + 32;   // the caller's batch area: incl[32], rb[32], re[32], ecnt[32], u[32]
+    uint32_t* s_u = s_rb + 96;
     const uint32_t k = kb + lane;
     uint32_t nq = 0, rb = 0, re = 0, u = 0;
     if (k < kend) {
@@ -134,6 +155,7 @@ __device__ __forceinline__ unsigned long long probe_batch(
     s_incl[lane] = incl;
     s_rb[lane] = rb;
     s_re[lane] = re;
+    if (MODE == TC_LIST) s_u[lane] = u;
     __syncwarp();
     const uint4* __restrict__ col4 = reinterpret_cast<const uint4*>(col);
     uint32_t owner = 0;
@@ -144,16 +166,20 @@ __device__ __forceinline__ unsigned long long probe_batch(
         const uint4 v = __ldg(col4 + q);
         const uint32_t e0 = q << 2;
         if (e0 >= lo && e0 < hi)
-            hits += probe_one<MODE, ALIVE, CT>(col, a, v.x, e0, owner, key, cnt, bits, global, vb, dv, s_ecnt);
+            hits += probe_one<MODE, ALIVE, CT>(col, a, v.x, e0, owner, key, cnt, bits, global, vb, dv, s_ecnt,
+                                               anchor, s_u);
         if (e0 + 1 >= lo && e0 + 1 < hi)
-            hits += probe_one<MODE, ALIVE, CT>(col, a, v.y, e0 + 1, owner, key, cnt, bits, global, vb, dv, s_ecnt);
+            hits += probe_one<MODE, ALIVE, CT>(col, a, v.y, e0 + 1, owner, key, cnt, bits, global, vb, dv, s_ecnt,
+                                               anchor, s_u);
         if (e0 + 2 >= lo && e0 + 2 < hi)
-            hits += probe_one<MODE, ALIVE, CT>(col, a, v.z, e0 + 2, owner, key, cnt, bits, global, vb, dv, s_ecnt);
+            hits += probe_one<MODE, ALIVE, CT>(col, a, v.z, e0 + 2, owner, key, cnt, bits, global, vb, dv, s_ecnt,
+                                               anchor, s_u);
         if (e0 + 3 >= lo && e0 + 3 < hi)
-            hits += probe_one<MODE, ALIVE, CT>(col, a, v.w, e0 + 3, owner, key, cnt, bits, global, vb, dv, s_ecnt);
+            hits += probe_one<MODE, ALIVE, CT>(col, a, v.w, e0 + 3, owner, key, cnt, bits, global, vb, dv, s_ecnt,
+                                               anchor, s_u);
     }
     __syncwarp();
-    if (MODE >= TC_VSUP) {
+    if (counters(MODE)) {
         const uint32_t c = s_ecnt[lane];
         if (c) {
             if (MODE == TC_VSUP) atomicAdd(&a.vsup[u], (CT)c);
@@ -184,7 +210,7 @@ __device__ __forceinline__ void build_table(const uint32_t* __restrict__ col, co
     const uint32_t S = 4u << bits, mask = (1u << bits) - 1;
     for (uint32_t s = tid; s < S; s += nthr) {
         key[s] = GA_EMPTY;
-        if (MODE >= TC_VSUP) cnt[s] = 0;
+        if (counters(MODE)) cnt[s] = 0;
     }
     if (sync_block) __syncthreads(); else __syncwarp();
     for (uint32_t i = tid; i < dv; i += nthr) {
@@ -205,7 +231,7 @@ template <int MODE, class CT>
 __device__ __forceinline__ void flush_table(const TcArgs<CT>& a, uint32_t vb, const uint32_t* key,
                                             const uint32_t* cnt, const uint32_t* pos, uint32_t bits, uint32_t tid,
                                             uint32_t nthr) {
-    if (MODE < TC_VSUP) return;
+    if (!counters(MODE)) return;
     const uint32_t S = 4u << bits;
     for (uint32_t s = tid; s < S; s += nthr) {
         const uint32_t c = cnt[s];
@@ -236,7 +262,7 @@ __global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const ui
         const uint32_t Smax = 4u << heavy_bits_max;
         uint32_t* key = smem;
         uint32_t* cnt = key + Smax;
-        uint32_t* pos = cnt + (MODE >= TC_VSUP ? Smax : 0);
+        uint32_t* pos = cnt + (counters(MODE) ? Smax : 0);
         uint32_t* wbase = smem + (size_t)Smax * W + warp * kBatchWords;
         uint32_t *s_incl = wbase, *s_rb = wbase + 32, *s_ecnt = wbase + 96;
         s_ecnt[lane] = 0;
@@ -264,7 +290,7 @@ __global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const ui
                 kb = __shfl_sync(GA_FULL_MASK, kb, 0);
                 if (kb >= k1) break;
                 h += probe_batch<MODE, ALIVE, CT>(rowptr, col, in_src, in_eid, a, kb, min(kb + 32, k1), key, cnt,
-                                                  bits, global, vb, dv, s_incl, s_rb, s_ecnt, lane);
+                                                  bits, global, vb, dv, s_incl, s_rb, s_ecnt, lane, v);
             }
             hits += h;
             if (MODE == TC_VSUP) {
@@ -281,7 +307,7 @@ __global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const ui
         constexpr int PW = light_warp_words<MODE>();
         uint32_t* key = smem + warp * PW;
         uint32_t* cnt = key + kLightSlots;
-        uint32_t* pos = cnt + (MODE >= TC_VSUP ? kLightSlots : 0);
+        uint32_t* pos = cnt + (counters(MODE) ? kLightSlots : 0);
         uint32_t* s_incl = key + kLightSlots * W;
         uint32_t *s_rb = s_incl + 32, *s_ecnt = s_incl + 96;
         s_ecnt[lane] = 0;
@@ -300,7 +326,7 @@ __global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const ui
             const uint32_t k1 = light.k1[item];
             for (uint32_t kb = light.k0[item]; kb < k1; kb += 32)
                 h += probe_batch<MODE, ALIVE, CT>(rowptr, col, in_src, in_eid, a, kb, min(kb + 32, k1), key, cnt,
-                                                  bits, false, vb, dv, s_incl, s_rb, s_ecnt, lane);
+                                                  bits, false, vb, dv, s_incl, s_rb, s_ecnt, lane, v);
             hits += h;
             if (MODE == TC_VSUP) {
                 const unsigned long long t = warp_sum_u64(h);
@@ -351,6 +377,7 @@ __global__ void __launch_bounds__(256) k_tc_plain(const uint32_t* __restrict__ r
                         atomicAdd(&a.esup[i], 1u);
                         atomicAdd(&a.esup[j], 1u);
                     }
+                    if (MODE == TC_LIST) list_triangle(a, u, v, x);
                 }
                 i++;
                 j++;
@@ -430,6 +457,7 @@ template ga_status run_tc<TC_VSUP, false, unsigned long long>(ga_graph*, const T
 template ga_status run_tc<TC_VSUP, false, unsigned int>(ga_graph*, const TcArgs<unsigned int>&, bool);
 template ga_status run_tc<TC_VSUP, true, unsigned int>(ga_graph*, const TcArgs<unsigned int>&, bool);
 template ga_status run_tc<TC_ESUP, false, unsigned int>(ga_graph*, const TcArgs<unsigned int>&, bool);
+template ga_status run_tc<TC_LIST, false, unsigned int>(ga_graph*, const TcArgs<unsigned int>&, bool);
 
 }  // namespace ga
 

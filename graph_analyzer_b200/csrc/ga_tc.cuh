@@ -4,16 +4,23 @@
 
 namespace ga {
 
-enum TcMode { TC_COUNT = 0, TC_VSUP = 1, TC_ESUP = 2 };
+// COUNT: T only. VSUP: per-vertex counts. ESUP: per-edge counts. LIST: every triangle written once into the
+// incidence lists of its three corners (the other two corners of each triangle through v, in inc[inc_ptr[v] ..]).
+enum TcMode { TC_COUNT = 0, TC_VSUP = 1, TC_ESUP = 2, TC_LIST = 3 };
 
 // Outputs of one triangle pass. `total` (device) receives T; `vsup` (n counters of type CT) the per-vertex counts;
-// `esup` (m) the per-edge counts; `alive` (n bytes, optional) restricts the pass to the induced subgraph.
+// `esup` (m) the per-edge counts; `alive` (n bytes, optional) restricts the pass to the induced subgraph;
+// `inc`/`inc_ptr`/`fill` the incidence lists of TC_LIST (fill: n zeroed cursors).
 template <class CT>
 struct TcArgs {
     unsigned long long* total = nullptr;
     CT* vsup = nullptr;
     uint32_t* esup = nullptr;
     const uint8_t* alive = nullptr;
+    uint2* inc = nullptr;
+    const unsigned long long* inc_ptr = nullptr;
+    uint32_t* fill = nullptr;
+    uint32_t* overflow = nullptr;   // TC_LIST: entries that found their list full (must stay 0)
 };
 
 // One triangle pass on g's stream (asynchronous). zero_outputs: clear total/vsup/esup first.

@@ -137,7 +137,9 @@ typedef enum ga_option {
     GA_OPT_ITEM_WORK = 4,     /* probe work (list elements) per work item of the hash kernel (0 = 4096)            */
     GA_OPT_HEAVY_TABLE_BITS = 5, /* log2 buckets (4 slots each) of the block-wide hash set; anchors that need more
                                     binary-search the global row (0 = as large as shared memory allows, 3..13)      */
-    GA_OPT_LIGHT_MAX_DEG = 6  /* anchors with out-degree <= this use per-warp tables (0 = 128, at most 256)        */
+    GA_OPT_LIGHT_MAX_DEG = 6, /* anchors with out-degree <= this use per-warp tables (0 = 128, at most 256)        */
+    GA_OPT_UPDATE_MODE = 7    /* peeling/core rounds: 0 auto (triangle incidence lists when their 24*T bytes fit,
+                                 else re-enumeration), 1 re-enumerate the frontier's triangles, 2 incidence lists   */
 } ga_option;
 ga_status ga_graph_set_option(ga_graph* g, ga_option opt, int64_t value);
 

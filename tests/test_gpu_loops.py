@@ -12,7 +12,14 @@ from conftest import FIXTURES, fixture_path, golden_arrays, hub_pairs, random_pa
 pytestmark = pytest.mark.gpu
 
 EPS = [(1, 10), (1, 1), (0, 1), (3, 7), (1, 20), (1, 2)]
-MODES = {"graph": 2, "host": 1}
+# (GA_OPT_LOOP_MODE, GA_OPT_UPDATE_MODE): CUDA-graph or host-driven rounds x incidence-list or re-enumeration updates
+MODES = {"graph-lists": (2, 2), "graph-enum": (2, 1), "host-lists": (1, 2), "host-enum": (1, 1)}
+
+
+def _set_mode(ga, d, mode):
+    loop, update = MODES[mode]
+    d.set_option(ga.OPT_LOOP_MODE, loop)
+    d.set_option(ga.OPT_UPDATE_MODE, update)
 
 
 def _peel_eq(ga, oracle, g, d, num, den):
@@ -37,7 +44,7 @@ def test_fixtures_peel_and_cores(ga, oracle, golden, cuda_ok, name, mode):
     g = ga.load_graph(fixture_path(name))
     arr = golden_arrays(name)
     with ga.DeviceGraph(g) as d:
-        d.set_option(ga.OPT_LOOP_MODE, MODES[mode])
+        _set_mode(ga, d, mode)
         for num, den in EPS:
             r = d.batch_peel(num, den)
             want = golden[name]["peel"][f"{num}/{den}"]
@@ -56,13 +63,14 @@ def test_random_graphs(ga, oracle, cuda_ok, seed, mode):
     n = int(rng.integers(30, 600))
     g = ga.build_graph_from_edges(n, ga.canonical_edges(random_pairs(rng, n, float(rng.choice([0.03, 0.1, 0.3])))))
     with ga.DeviceGraph(g) as d:
-        d.set_option(ga.OPT_LOOP_MODE, MODES[mode])
+        _set_mode(ga, d, mode)
         for num, den in EPS:
             _peel_eq(ga, oracle, g, d, num, den)
         _core_eq(oracle, g, d)
 
 
-def test_hubs_and_wide_frontiers(ga, oracle, cuda_ok):
+@pytest.mark.parametrize("mode", ["graph-lists", "graph-enum"])
+def test_hubs_and_wide_frontiers(ga, oracle, cuda_ok, mode):
     """Hubs with up to 600 neighbours: frontier vertices of degree > 256 take the binary-search update path and
     split into several update items (the reference's --hub suite, emu_dsg.cpp:654-696, widened)."""
     rng = np.random.default_rng(20261010)
@@ -70,12 +78,14 @@ def test_hubs_and_wide_frontiers(ga, oracle, cuda_ok):
         n, raw = hub_pairs(rng, int(rng.integers(1, 4)), int(rng.integers(40, 600)), int(rng.integers(8, 40)))
         g = ga.build_graph_from_edges(n, ga.canonical_edges(raw))
         with ga.DeviceGraph(g) as d:
+            _set_mode(ga, d, mode)
             for num, den in EPS[:3]:
                 _peel_eq(ga, oracle, g, d, num, den)
             _core_eq(oracle, g, d)
 
 
-def test_clique_and_edge_cases(ga, oracle, cuda_ok):
+@pytest.mark.parametrize("mode", ["graph-lists", "graph-enum"])
+def test_clique_and_edge_cases(ga, oracle, cuda_ok, mode):
     n = 300
     iu, iv = np.triu_indices(n, 1)
     cases = [
@@ -88,6 +98,7 @@ def test_clique_and_edge_cases(ga, oracle, cuda_ok):
     for nn, p in cases:
         g = ga.build_graph_from_edges(nn, p)
         with ga.DeviceGraph(g) as d:
+            _set_mode(ga, d, mode)
             for num, den in EPS:
                 _peel_eq(ga, oracle, g, d, num, den)
             _core_eq(oracle, g, d)
@@ -96,8 +107,8 @@ def test_clique_and_edge_cases(ga, oracle, cuda_ok):
 def test_holme_kim_c1_peel_and_cores(ga, oracle, cuda_ok):
     g = ga.graph_from_pairs(8298, ga.gen_holme_kim(8298, 12, 12, 0.0, 0.5, seed=1))
     with ga.DeviceGraph(g) as d:
-        for mode in (2, 1):
-            d.set_option(ga.OPT_LOOP_MODE, mode)
+        for mode in MODES:
+            _set_mode(ga, d, mode)
             for num, den in [(1, 10), (1, 20), (1, 2)]:
                 _peel_eq(ga, oracle, g, d, num, den)
             _core_eq(oracle, g, d)
@@ -119,11 +130,29 @@ def test_round_cap_reports_error(ga, oracle, cuda_ok):
     rounds = oracle.core_levels(g)[2]
     assert rounds > 2
     with ga.DeviceGraph(g) as d:
-        for mode in (1, 2):
-            d.set_option(ga.OPT_LOOP_MODE, mode)
+        for mode in MODES:
+            _set_mode(ga, d, mode)
             d.set_option(ga.OPT_MAX_ROUNDS, 2)
             with pytest.raises(ga.GAError) as e:
                 d.core_decomposition()
             assert e.value.name == "GA_ERR_ROUND_LIMIT"
             d.set_option(ga.OPT_MAX_ROUNDS, 0)
             _core_eq(oracle, g, d)
+
+
+def test_lists_reused_across_calls(ga, oracle, cuda_ok):
+    """The incidence lists are built once per graph; later peel and core calls start from their lengths."""
+    g = ga.graph_from_pairs(3000, ga.gen_holme_kim(3000, 6, 7, 0.54, 0.5, seed=3))
+    with ga.DeviceGraph(g) as d:
+        d.set_option(ga.OPT_UPDATE_MODE, 2)
+        b0 = d.device_bytes()
+        _core_eq(oracle, g, d)
+        b1 = d.device_bytes()
+        assert b1 > b0                                           # lists allocated by the first loop call
+        for num, den in EPS:
+            _peel_eq(ga, oracle, g, d, num, den)
+        _core_eq(oracle, g, d)
+        assert d.device_bytes() == b1                            # and reused
+        d.set_option(ga.OPT_UPDATE_MODE, 1)                      # switching frees them
+        _core_eq(oracle, g, d)
+        assert d.device_bytes() < b1
