@@ -35,7 +35,8 @@ __all__ = [
     "canonical_edges", "gen_holme_kim", "gen_rmat", "permute_ids", "density_value", "peel_arith_ok",
     "peel_improves", "gpu_triangles", "gpu_batch_peel", "gpu_core_decomposition", "lib", "device_count",
     "OPT_TC_KERNEL", "OPT_LOOP_MODE", "OPT_MAX_ROUNDS", "OPT_ITEM_WORK", "OPT_HEAVY_TABLE_BITS",
-    "OPT_LIGHT_MAX_DEG", "OPT_UPDATE_MODE",
+    "OPT_LIGHT_MAX_DEG", "OPT_UPDATE_MODE", "HostBatch", "DeviceBatch", "BatchPeel", "pack_batch",
+    "gen_holme_kim_batch",
 ]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
@@ -80,6 +81,12 @@ class _CoreRes(C.Structure):
     _fields_ = [("kmax", C.c_uint32), ("rounds", C.c_uint32)]
 
 
+class _HostBatch(C.Structure):
+    _fields_ = [("num_graphs", C.c_uint32), ("total_vertices", C.c_uint64), ("total_edges", C.c_uint64),
+                ("vtx_off", C.POINTER(C.c_uint64)), ("edge_off", C.POINTER(C.c_uint64)),
+                ("rowptr", C.POINTER(C.c_uint32)), ("col", C.POINTER(C.c_uint32))]
+
+
 # (name, argtypes) of every exported entry point; the library must export all of them.
 SIGNATURES: dict[str, list] = {
     "ga_status_string": [C.c_int],
@@ -109,8 +116,18 @@ SIGNATURES: dict[str, list] = {
     "ga_tc_participation": [_vp, _vp, _vp, C.POINTER(C.c_uint64)],
     "ga_batch_peel": [_vp, C.c_uint64, C.c_uint64, C.POINTER(_PeelRes), _vp],
     "ga_core_decomposition": [_vp, _vp, C.POINTER(_CoreRes)],
+    "ga_gen_holme_kim_batch": [C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_double,
+                               C.c_uint64, C.POINTER(C.POINTER(_HostBatch))],
+    "ga_host_batch_free": [C.POINTER(_HostBatch)],
+    "ga_batch_create": [C.c_uint32, _vp, _vp, _vp, _vp, C.c_int, _vp, C.POINTER(_vp)],
+    "ga_batch_destroy": [_vp],
+    "ga_batch_set_option": [_vp, C.c_int, C.c_int64],
+    "ga_batch_device_bytes": [_vp, C.POINTER(C.c_uint64)],
+    "ga_batch_tc": [_vp, _vp],
+    "ga_batch_tc_peel": [_vp, C.c_uint64, C.c_uint64, _vp, _vp, _vp, _vp],
 }
-_RESTYPE = {"ga_status_string": C.c_char_p, "ga_last_error": C.c_char_p, "ga_host_graph_free": None}
+_RESTYPE = {"ga_status_string": C.c_char_p, "ga_last_error": C.c_char_p, "ga_host_graph_free": None,
+            "ga_host_batch_free": None}
 
 _lib: C.CDLL | None = None
 
@@ -439,3 +456,131 @@ def gpu_batch_peel(g: Graph, num: int = 1, den: int = 10, device: int = 0) -> Pe
 def gpu_core_decomposition(g: Graph, device: int = 0) -> CoreResult:
     with DeviceGraph(g, device) as d:
         return d.core_decomposition()
+
+
+# ------------------------------------------------------------------------------------------------------------------
+# batches: many graphs packed as one concatenated CSR (64-bit offsets, 32-bit local ids)
+# ------------------------------------------------------------------------------------------------------------------
+
+@dataclass
+class HostBatch:
+    """Packed batch: graph i owns vertices [vtx_off[i], vtx_off[i+1]) and edges [edge_off[i], edge_off[i+1]); its
+    local rowptr (n_i + 1 entries) starts at rowptr[vtx_off[i] + i]; col holds local ids."""
+
+    vtx_off: np.ndarray   # uint64[G+1]
+    edge_off: np.ndarray  # uint64[G+1]
+    rowptr: np.ndarray    # uint32[N+G]
+    col: np.ndarray       # uint32[M]
+
+    @property
+    def num_graphs(self) -> int:
+        return len(self.vtx_off) - 1
+
+    def graph(self, i: int) -> Graph:
+        v0, v1 = int(self.vtx_off[i]), int(self.vtx_off[i + 1])
+        e0, e1 = int(self.edge_off[i]), int(self.edge_off[i + 1])
+        rowptr = self.rowptr[v0 + i: v1 + i + 1].copy()
+        col = self.col[e0:e1].copy()
+        d = np.diff(rowptr.astype(np.int64))
+        src = np.repeat(np.arange(v1 - v0, dtype=np.uint32), d)
+        return Graph(v1 - v0, e1 - e0, rowptr, col, src, int(d.max()) if d.size else 0)
+
+
+def pack_batch(graphs: list[Graph]) -> HostBatch:
+    vtx_off = np.zeros(len(graphs) + 1, np.uint64)
+    edge_off = np.zeros(len(graphs) + 1, np.uint64)
+    vtx_off[1:] = np.cumsum([g.n for g in graphs])
+    edge_off[1:] = np.cumsum([g.m for g in graphs])
+    rowptr = np.concatenate([g.rowptr for g in graphs]).astype(np.uint32)
+    col = (np.concatenate([g.col for g in graphs]) if graphs else np.zeros(0)).astype(np.uint32)
+    return HostBatch(vtx_off, edge_off, rowptr, col)
+
+
+def gen_holme_kim_batch(num_graphs: int, n_lo: int = 64, n_hi: int = 262144, deg_lo: float = 4.0,
+                        deg_hi: float = 32.0, p_lo: float = 0.1, p_hi: float = 0.7, seed: int = 1) -> HostBatch:
+    """Seeded batch of Holme-Kim graphs (n log-uniform, mean degree and triad probability uniform), built in
+    parallel on the host."""
+    hb = C.POINTER(_HostBatch)()
+    _check(lib().ga_gen_holme_kim_batch(num_graphs, n_lo, n_hi, deg_lo, deg_hi, p_lo, p_hi, seed, C.byref(hb)))
+    h = hb.contents
+    G, N, M = h.num_graphs, h.total_vertices, h.total_edges
+    out = HostBatch(np.ctypeslib.as_array(h.vtx_off, shape=(G + 1,)).copy(),
+                    np.ctypeslib.as_array(h.edge_off, shape=(G + 1,)).copy(),
+                    np.ctypeslib.as_array(h.rowptr, shape=(N + G,)).copy(),
+                    np.ctypeslib.as_array(h.col, shape=(max(M, 1),))[:M].copy())
+    lib().ga_host_batch_free(hb)
+    return out
+
+
+@dataclass
+class BatchPeel:
+    triangles: np.ndarray       # uint64[G]
+    best_num: np.ndarray        # uint64[G]
+    best_den: np.ndarray        # uint64[G]
+    best_round: np.ndarray      # uint32[G]
+    rounds: np.ndarray          # uint32[G]
+    status: np.ndarray          # uint32[G] (ga_status per graph)
+    removed_round: np.ndarray   # uint32[N], batch order
+
+    def result(self, batch: HostBatch, i: int) -> PeelResult:
+        v0, v1 = int(batch.vtx_off[i]), int(batch.vtx_off[i + 1])
+        return PeelResult(int(self.best_num[i]), int(self.best_den[i]), int(self.best_round[i]),
+                          int(self.rounds[i]), self.removed_round[v0:v1])
+
+
+class DeviceBatch:
+    """A packed batch resident on one GPU (ga_batch)."""
+
+    def __init__(self, b: HostBatch, device: int = 0, stream: int | None = None):
+        self.G = b.num_graphs
+        self.N = int(b.vtx_off[-1])
+        vo = np.ascontiguousarray(b.vtx_off, np.uint64)
+        eo = np.ascontiguousarray(b.edge_off, np.uint64)
+        rp = np.ascontiguousarray(b.rowptr, np.uint32)
+        cl = np.ascontiguousarray(b.col if b.col.size else np.zeros(1, np.uint32), np.uint32)
+        h = _vp()
+        _check(lib().ga_batch_create(self.G, _ptr(vo), _ptr(eo), _ptr(rp), _ptr(cl), device, stream, C.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().ga_batch_destroy(self._h)
+            self._h = _vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_option(self, opt: int, value: int) -> None:
+        _check(lib().ga_batch_set_option(self._h, opt, value))
+
+    def device_bytes(self) -> int:
+        b = C.c_uint64(0)
+        _check(lib().ga_batch_device_bytes(self._h, C.byref(b)))
+        return b.value
+
+    def tc(self) -> np.ndarray:
+        t = np.zeros(self.G, np.uint64)
+        _check(lib().ga_batch_tc(self._h, _ptr(t)))
+        return t
+
+    def tc_peel(self, num: int = 1, den: int = 10, want_removed: bool = True) -> BatchPeel:
+        G = self.G
+        t = np.zeros(G, np.uint64)
+        res = (_PeelRes * G)()
+        st = np.zeros(G, np.uint32)
+        rr = np.zeros(max(self.N, 1), np.uint32) if want_removed else None
+        _check(lib().ga_batch_tc_peel(self._h, num, den, _ptr(t), C.addressof(res), _ptr(st), _ptr(rr)))
+        return BatchPeel(t, np.array([r.best_num for r in res], np.uint64),
+                         np.array([r.best_den for r in res], np.uint64),
+                         np.array([r.best_round for r in res], np.uint32),
+                         np.array([r.rounds for r in res], np.uint32), st,
+                         rr[: self.N] if rr is not None else np.zeros(0, np.uint32))

@@ -158,4 +158,13 @@ ga_status scan_u64(ga_graph* g, unsigned long long* data, uint64_t n);
 // Frees the loop state and its device buffers (the next loop call rebuilds them).
 void reset_loops(ga_graph* g);
 
+// Batches: g is the disjoint union of `count` graphs, graph s owning vertices [d_off[s], d_off[s+1]) (device array
+// of count + 1 offsets that outlives g's use of it). set_segments installs the per-graph loop state once;
+// count_segments gives every graph's triangle count; peel_segments peels all graphs in one loop, each exactly as if
+// alone (any output may be null; removed_round has n entries in union order).
+ga_status set_segments(ga_graph* g, const unsigned long long* d_off, uint32_t count);
+ga_status count_segments(ga_graph* g, uint64_t* triangles);
+ga_status peel_segments(ga_graph* g, uint64_t num, uint64_t den, uint64_t* triangles, ga_peel_result* res,
+                        uint32_t* status, uint32_t* removed_round);
+
 }  // namespace ga

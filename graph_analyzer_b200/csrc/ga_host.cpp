@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cerrno>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -403,6 +404,84 @@ ga_status ga_gen_rmat(uint32_t scale, uint64_t nsamples, double a, double b, dou
             pairs[2 * s + 1] = v;
         }
     }
+    return GA_OK;
+}
+
+void ga_host_batch_free(ga_host_batch* b) {
+    if (!b) return;
+    std::free(b->vtx_off);
+    std::free(b->edge_off);
+    std::free(b->rowptr);
+    std::free(b->col);
+    std::free(b);
+}
+
+ga_status ga_gen_holme_kim_batch(uint32_t num_graphs, uint32_t n_lo, uint32_t n_hi, double deg_lo, double deg_hi,
+                                 double p_lo, double p_hi, uint64_t seed, ga_host_batch** out) {
+    if (!out || num_graphs == 0 || n_lo < 8 || n_hi < n_lo || deg_lo < 2.0 || deg_hi < deg_lo || p_lo < 0 ||
+        p_hi < p_lo || p_hi > 1)
+        return fail(GA_ERR_INVALID_ARGUMENT, "holme_kim_batch: need graphs > 0, 8 <= n_lo <= n_hi, "
+                                             "2 <= deg_lo <= deg_hi, 0 <= p_lo <= p_hi <= 1");
+    *out = nullptr;
+    struct One { std::vector<uint32_t> rowptr, col; uint32_t n = 0; ga_status s = GA_OK; };
+    std::vector<One> gs(num_graphs);
+    std::atomic<int> failed{0};
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t gi = 0; gi < (int64_t)num_graphs; gi++) {
+        if (failed.load()) continue;
+        One& o = gs[gi];
+        Rng r(mix64(seed ^ mix64((uint64_t)gi + 0x6261746368ull)));
+        const double ln_lo = std::log((double)n_lo), ln_hi = std::log((double)n_hi);
+        uint32_t n = (uint32_t)std::llround(std::exp(ln_lo + (ln_hi - ln_lo) * r.uniform()));
+        n = std::min(std::max(n, n_lo), n_hi);
+        const double k = (deg_lo + (deg_hi - deg_lo) * r.uniform()) / 2.0;   // edges per new vertex
+        const uint32_t m_lo = std::max<uint32_t>(1, (uint32_t)k);
+        const double frac = k - (double)m_lo;
+        const uint32_t m_hi = frac > 0 ? m_lo + 1 : m_lo;
+        const double triad = p_lo + (p_hi - p_lo) * r.uniform();
+        const uint64_t gseed = r.next();
+        o.n = n;
+        if (n <= m_hi) { o.s = fail(GA_ERR_INVALID_ARGUMENT, "graph %lld too small", (long long)gi); failed = 1; continue; }
+        std::vector<uint32_t> pairs(2ull * n * m_hi);
+        uint64_t np = 0;
+        ga_status s = ga_gen_holme_kim(n, m_lo, m_hi, frac, triad, gseed, pairs.data(), (uint64_t)n * m_hi, &np);
+        if (s == GA_OK) s = ga_permute_ids(pairs.data(), np, n, gseed);
+        if (s == GA_OK) {
+            o.rowptr.resize((size_t)n + 1);
+            o.col.resize(np ? np : 1);
+            std::vector<uint32_t> src(np ? np : 1);
+            uint32_t mx = 0;
+            s = build_csr(n, pairs.data(), (uint32_t)np, o.rowptr.data(), o.col.data(), src.data(), &mx);
+            o.col.resize(np);
+        }
+        if (s != GA_OK) { o.s = s; failed = 1; }
+    }
+    for (size_t g = 0; g < gs.size(); g++)   // worker threads' messages are thread-local: report on this thread
+        if (gs[g].s != GA_OK) return fail(gs[g].s, "holme_kim_batch: generating graph %zu failed", g);
+    ga_host_batch* b = (ga_host_batch*)std::calloc(1, sizeof(ga_host_batch));
+    if (!b) return fail(GA_ERR_OUT_OF_MEMORY, "host allocation failed");
+    b->num_graphs = num_graphs;
+    b->vtx_off = (uint64_t*)std::malloc((num_graphs + 1ull) * 8);
+    b->edge_off = (uint64_t*)std::malloc((num_graphs + 1ull) * 8);
+    if (!b->vtx_off || !b->edge_off) { ga_host_batch_free(b); return fail(GA_ERR_OUT_OF_MEMORY, "host allocation"); }
+    b->vtx_off[0] = b->edge_off[0] = 0;
+    for (uint32_t g = 0; g < num_graphs; g++) {
+        b->vtx_off[g + 1] = b->vtx_off[g] + gs[g].n;
+        b->edge_off[g + 1] = b->edge_off[g] + gs[g].col.size();
+    }
+    b->total_vertices = b->vtx_off[num_graphs];
+    b->total_edges = b->edge_off[num_graphs];
+    b->rowptr = (uint32_t*)std::malloc((b->total_vertices + num_graphs) * 4);
+    b->col = (uint32_t*)std::malloc((b->total_edges + 1) * 4);
+    if (!b->rowptr || !b->col) { ga_host_batch_free(b); return fail(GA_ERR_OUT_OF_MEMORY, "host allocation"); }
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t g = 0; g < (int64_t)num_graphs; g++) {
+        std::memcpy(b->rowptr + b->vtx_off[g] + g, gs[g].rowptr.data(), gs[g].rowptr.size() * 4);
+        if (!gs[g].col.empty()) std::memcpy(b->col + b->edge_off[g], gs[g].col.data(), gs[g].col.size() * 4);
+        std::vector<uint32_t>().swap(gs[g].col);
+        std::vector<uint32_t>().swap(gs[g].rowptr);
+    }
+    *out = b;
     return GA_OK;
 }
 

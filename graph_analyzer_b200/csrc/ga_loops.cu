@@ -48,7 +48,38 @@ struct LoopScalars {
 };
 
 // status codes written by the device
-enum : uint32_t { LS_OK = 0, LS_NO_PROGRESS = 1, LS_ROUND_LIMIT = 2, LS_LEVEL_DOWN = 3, LS_OVER_REMOVED = 4 };
+enum : uint32_t { LS_OK = 0, LS_NO_PROGRESS = 1, LS_ROUND_LIMIT = 2, LS_LEVEL_DOWN = 3, LS_OVER_REMOVED = 4,
+                  LS_ARITH = 5 };
+
+// Per-graph state when one loop peels many disjoint graphs at once (a batch): graph s owns vertices
+// [off[s], off[s+1]) and has its own T, alive count, threshold, best density, round count and status, exactly as if
+// it were peeled alone. count == 0: a single graph (the LoopScalars fields are used instead).
+struct Segs {
+    uint32_t count = 0;
+    const unsigned long long* off = nullptr;          // count + 1
+    unsigned long long *T = nullptr, *nalive = nullptr, *removed = nullptr, *destroyed = nullptr;
+    unsigned long long *best_num = nullptr, *best_den = nullptr, *T0 = nullptr;
+    uint32_t *best_round = nullptr, *rounds = nullptr, *status = nullptr;
+};
+
+// Segment of vertex v: the last s with off[s] <= v.
+__device__ __forceinline__ uint32_t seg_of(const Segs& sg, uint32_t v) {
+    uint32_t lo = 0, hi = sg.count;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (sg.off[mid] <= v) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// peel_arith_ok (densest.h:65-72) for one graph with n vertices and T0 triangles (eps already range-checked).
+__host__ __device__ inline bool peel_arith_fits(unsigned long long n, unsigned long long T0, unsigned long long num,
+                                                unsigned long long den) {
+    if (T0 >= (1ull << 32)) return false;
+    if (n > 0 && T0 > ~0ull / (n * den)) return false;
+    if (T0 > ~0ull / (3ull * (den + num))) return false;
+    return true;
+}
 
 }  // namespace ga
 
@@ -71,6 +102,9 @@ struct ga_loops {
     int lists = -1;                    // -1 undecided, 0 enumeration update, 1 incidence-list update
     uint2* inc = nullptr;
     unsigned long long* inc_ptr = nullptr;   // n+1
+    ga::Segs segs;                     // per-graph state of a batch (count 0 for a single graph)
+    cudaGraphExec_t exec_seg = nullptr;
+    cudaGraph_t graph_seg = nullptr;
 };
 
 namespace ga {
@@ -144,14 +178,16 @@ __device__ __forceinline__ void append_survivor(bool keep, uint32_t v, uint32_t*
 }
 
 // Peel round, step 1: best-density bookkeeping (peel_improves, densest.h:297) and the mark_peel rule
-// (kernels.cuh:448-451) over the alive list.
+// (kernels.cuh:448-451) over the alive list. With segments each vertex uses its own graph's T and alive count (the
+// per-graph best density is kept by the tail), removals are counted per graph (one atomic per graph per warp), and
+// the vertices of a graph that was refused or failed leave the loop silently.
 __global__ void __launch_bounds__(256) k_peel_mark(LoopScalars* sc, const uint32_t* __restrict__ tri,
                                                    uint8_t* __restrict__ state, uint32_t* __restrict__ removed_round,
                                                    uint32_t* alive0, uint32_t* alive1,
                                                    uint32_t* __restrict__ frontier, uint32_t* __restrict__ item_x,
                                                    uint32_t* __restrict__ item_c, const uint32_t* __restrict__ rowptr,
                                                    const uint32_t* __restrict__ in_ptr,
-                                                   const unsigned long long* __restrict__ inc_ptr) {
+                                                   const unsigned long long* __restrict__ inc_ptr, Segs sg) {
     const uint32_t p = sc->parity;
     const uint32_t* in = p ? alive1 : alive0;
     uint32_t* outl = p ? alive0 : alive1;
@@ -159,7 +195,7 @@ __global__ void __launch_bounds__(256) k_peel_mark(LoopScalars* sc, const uint32
     const unsigned long long T = sc->T, nalive = sc->nalive, num = sc->num, den = sc->den;
     const unsigned long long rhs = 3ull * (den + num) * T;
     const uint32_t round = sc->round;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (!sg.count && blockIdx.x == 0 && threadIdx.x == 0) {
         if (sc->best_den == 0 || T * sc->best_den > sc->best_num * nalive) {
             sc->best_num = T;
             sc->best_den = nalive;
@@ -172,16 +208,36 @@ __global__ void __launch_bounds__(256) k_peel_mark(LoopScalars* sc, const uint32
         const uint32_t i = i0 + lane;
         const bool valid = i < na;
         const uint32_t v = valid ? in[i] : 0;
-        bool rem = false;
+        bool rem = false, drop = false;
+        uint32_t s = 0;
         if (valid) {
-            rem = (unsigned long long)tri[v] * nalive * den <= rhs;
+            if (sg.count) {
+                s = seg_of(sg, v);
+                if (sg.status[s] != LS_OK) {
+                    drop = true;
+                    state[v] = 0;
+                } else {
+                    const unsigned long long Ts = sg.T[s], ns = sg.nalive[s];
+                    rem = (unsigned long long)tri[v] * ns * den <= 3ull * (den + num) * Ts;
+                }
+            } else {
+                rem = (unsigned long long)tri[v] * nalive * den <= rhs;
+            }
             if (rem) {
                 state[v] = 2;
                 removed_round[v] = round;
             }
         }
+        if (sg.count) {   // removals per graph: lanes of the same graph combine into one atomic
+            const uint32_t bal = __ballot_sync(GA_FULL_MASK, rem);
+            if (bal) {
+                const uint32_t peers = __match_any_sync(GA_FULL_MASK, rem ? s : 0xFFFFFFFFu);
+                if (rem && lane == (uint32_t)(__ffs(peers) - 1))
+                    atomicAdd(&sg.removed[s], (unsigned long long)__popc(peers));
+            }
+        }
         append_frontier(rem, v, rowptr, in_ptr, inc_ptr, sc, frontier, item_x, item_c, lane);
-        append_survivor(valid && !rem, v, outl, &sc->alive_count[p ^ 1], lane);
+        append_survivor(valid && !rem && !drop, v, outl, &sc->alive_count[p ^ 1], lane);
     }
 }
 
@@ -239,7 +295,7 @@ __global__ void __launch_bounds__(256) k_core_mark(LoopScalars* sc, const uint32
 __global__ void __launch_bounds__(kUpdWarps * 32) k_frontier_update(
     LoopScalars* sc, const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ col,
     const uint32_t* __restrict__ in_ptr, const uint32_t* __restrict__ in_src, const uint32_t* __restrict__ item_x,
-    const uint32_t* __restrict__ item_c, const uint8_t* __restrict__ state, uint32_t* __restrict__ tri) {
+    const uint32_t* __restrict__ item_c, const uint8_t* __restrict__ state, uint32_t* __restrict__ tri, Segs sg) {
     constexpr uint32_t kSlots = 2 * kChunk;   // 512 slots, load <= 1/2
     constexpr uint32_t kBits = 9;
     __shared__ uint32_t s_key[kUpdWarps][kSlots];
@@ -253,6 +309,7 @@ __global__ void __launch_bounds__(kUpdWarps * 32) k_frontier_update(
     unsigned long long destroyed = 0;
     for (uint32_t it = gwarp; it < nitems; it += nwarps) {
         const uint32_t x = item_x[it], c = item_c[it];
+        const unsigned long long d0 = destroyed;
         const uint32_t xb = rowptr[x], dout = rowptr[x + 1] - xb;
         const uint32_t ib = in_ptr[x], din = in_ptr[x + 1] - ib;
         const uint32_t deg = dout + din;
@@ -323,6 +380,10 @@ __global__ void __launch_bounds__(kUpdWarps * 32) k_frontier_update(
             }
             __syncwarp();
         }
+        if (sg.count) {   // per-graph count of destroyed triangles
+            const unsigned long long t = warp_sum_u64(destroyed - d0);
+            if (lane == 0 && t) atomicAdd(&sg.destroyed[seg_of(sg, x)], t);
+        }
     }
     destroyed = warp_sum_u64(destroyed);
     if (lane == 0) s_red[w] = destroyed;
@@ -343,7 +404,7 @@ __global__ void __launch_bounds__(256) k_frontier_update_list(LoopScalars* sc, c
                                                               const uint32_t* __restrict__ item_x,
                                                               const uint32_t* __restrict__ item_c,
                                                               const uint8_t* __restrict__ state,
-                                                              uint32_t* __restrict__ tri) {
+                                                              uint32_t* __restrict__ tri, Segs sg) {
     __shared__ unsigned long long s_red[8];
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t nitems = sc->nitems;
@@ -353,6 +414,7 @@ __global__ void __launch_bounds__(256) k_frontier_update_list(LoopScalars* sc, c
         const uint32_t x = item_x[it];
         const unsigned long long b = inc_ptr[x] + (unsigned long long)item_c[it] * kListChunk;
         const unsigned long long e = min(inc_ptr[x + 1], b + kListChunk);
+        const unsigned long long d0 = destroyed;
         for (unsigned long long i = b + lane; i < e; i += 32) {
             const uint2 yw = inc[i];
             const uint8_t sy = state[yw.x], sw = state[yw.y];
@@ -361,6 +423,10 @@ __global__ void __launch_bounds__(256) k_frontier_update_list(LoopScalars* sc, c
             destroyed++;
             if (sy == 1) atomicSub(&tri[yw.x], 1u);
             if (sw == 1) atomicSub(&tri[yw.y], 1u);
+        }
+        if (sg.count) {   // per-graph count of destroyed triangles
+            const unsigned long long t = warp_sum_u64(destroyed - d0);
+            if (lane == 0 && t) atomicAdd(&sg.destroyed[seg_of(sg, x)], t);
         }
     }
     destroyed = warp_sum_u64(destroyed);
@@ -379,8 +445,9 @@ __global__ void __launch_bounds__(256) k_frontier_update_list(LoopScalars* sc, c
 template <int KIND>
 __global__ void __launch_bounds__(256) k_retire_tail(LoopScalars* sc, uint8_t* __restrict__ state,
                                                      const uint32_t* __restrict__ frontier,
-                                                     cudaGraphConditionalHandle handle, int use_handle) {
+                                                     cudaGraphConditionalHandle handle, int use_handle, Segs sg) {
     __shared__ bool s_last;
+    __shared__ unsigned long long s_alive[8];
     const uint32_t F = sc->fcount;
     // independent bound: block 0 counts every execution of this kernel; past max_rounds + 1 the loop is forced to
     // stop even if the round bookkeeping below were broken (a WHILE node keeps its last condition value otherwise)
@@ -398,19 +465,58 @@ __global__ void __launch_bounds__(256) k_retire_tail(LoopScalars* sc, uint8_t* _
     __syncthreads();
     if (threadIdx.x == 0) s_last = atomicAdd(&sc->done_blocks, 1u) == gridDim.x - 1;
     __syncthreads();
-    if (!s_last || threadIdx.x != 0) return;
+    if (!s_last) return;
     __threadfence();
+    // every graph of a batch closes its own round (all threads of the last block): removed and destroyed counts,
+    // the checks of densest.h:298, then peel_improves for the alive set the next round starts from
+    unsigned long long alive = 0;
+    if (sg.count) {
+        const uint32_t ran = sc->round;
+        for (uint32_t s = threadIdx.x; s < sg.count; s += blockDim.x) {
+            if (sg.status[s] == LS_OK && sg.nalive[s] > 0) {
+                const unsigned long long rem = sg.removed[s], des = sg.destroyed[s];
+                uint32_t st = LS_OK;
+                if (rem == 0) st = LS_NO_PROGRESS;
+                if (rem > sg.nalive[s] || des > sg.T[s]) st = LS_OVER_REMOVED;
+                const unsigned long long na = sg.nalive[s] - min(rem, sg.nalive[s]);
+                const unsigned long long T = sg.T[s] - min(des, sg.T[s]);
+                sg.nalive[s] = na;
+                sg.T[s] = T;
+                sg.rounds[s] = ran + 1;
+                if (st == LS_OK && na > 0 && ran + 1 >= sc->max_rounds) st = LS_ROUND_LIMIT;
+                if (st == LS_OK && na > 0 && (sg.best_den[s] == 0 || T * sg.best_den[s] > sg.best_num[s] * na)) {
+                    sg.best_num[s] = T;
+                    sg.best_den[s] = na;
+                    sg.best_round[s] = ran + 1;
+                }
+                sg.status[s] = st;
+                if (st == LS_OK) alive += na;
+            }
+            sg.removed[s] = 0;
+            sg.destroyed[s] = 0;
+        }
+        alive = warp_sum_u64(alive);
+        if ((threadIdx.x & 31) == 0) s_alive[threadIdx.x >> 5] = alive;
+        __syncthreads();
+        alive = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) alive += s_alive[w];
+    }
+    if (threadIdx.x != 0) return;
     LoopScalars s = *sc;   // written by earlier kernels of this round (visible at the kernel boundary)
     uint32_t status = s.status;
-    if (F == 0 && s.nalive > 0) status = LS_NO_PROGRESS;
-    if (F > s.nalive) status = LS_OVER_REMOVED;
+    if (sg.count) {
+        s.nalive = alive;
+    } else {
+        if (F == 0 && s.nalive > 0) status = LS_NO_PROGRESS;
+        if (F > s.nalive) status = LS_OVER_REMOVED;
+        if (s.destroyed > s.T) status = LS_OVER_REMOVED;
+        s.nalive -= min((unsigned long long)F, s.nalive);
+        s.T -= min(s.destroyed, s.T);
+    }
     if (KIND == LOOP_CORE) {
         if (s.kround < s.kcur) status = LS_LEVEL_DOWN;
         s.kcur = s.kround;
     }
-    if (s.destroyed > s.T) status = LS_OVER_REMOVED;
-    s.nalive -= min((unsigned long long)F, s.nalive);
-    s.T -= min(s.destroyed, s.T);
     s.round += 1;
     s.parity ^= 1;
     s.alive_count[s.parity ^ 1] = 0;   // the next round's output list
@@ -424,6 +530,42 @@ __global__ void __launch_bounds__(256) k_retire_tail(LoopScalars* sc, uint8_t* _
     s.cont = (status == LS_OK && s.nalive > 0 && s.iters <= s.max_rounds) ? 1u : 0u;
     *sc = s;
     if (use_handle) cudaGraphSetConditional(handle, s.cont);
+}
+
+// Per graph: T0 = (sum of its vertices' triangle counts) / 3. One block per graph.
+__global__ void k_seg_T(const uint32_t* __restrict__ tri, Segs sg) {
+    __shared__ unsigned long long s_w[8];
+    for (uint32_t s = blockIdx.x; s < sg.count; s += gridDim.x) {
+        unsigned long long acc = 0;
+        for (unsigned long long v = sg.off[s] + threadIdx.x; v < sg.off[s + 1]; v += blockDim.x) acc += tri[v];
+        acc = warp_sum_u64(acc);
+        if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long t = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += s_w[w];
+            sg.T0[s] = t / 3;
+        }
+        __syncthreads();
+    }
+}
+
+// Per graph: the state a lone batch_peel_loop starts from (densest.h:284-297): peel_arith_ok refusal, alive = n,
+// T = T0, and round 0 recorded as the best so far (peel_improves with nothing recorded).
+__global__ void k_seg_init(Segs sg, unsigned long long num, unsigned long long den) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < sg.count; s += gridDim.x * blockDim.x) {
+        const unsigned long long n = sg.off[s + 1] - sg.off[s], T0 = sg.T0[s];
+        const bool ok = peel_arith_fits(n, T0, num, den);
+        sg.status[s] = ok ? LS_OK : LS_ARITH;
+        sg.T[s] = T0;
+        sg.nalive[s] = ok ? n : 0;
+        sg.removed[s] = 0;
+        sg.destroyed[s] = 0;
+        sg.rounds[s] = 0;
+        sg.best_num[s] = ok && n ? T0 : 0;
+        sg.best_den[s] = ok && n ? n : 0;
+        sg.best_round[s] = 0;
+    }
 }
 
 // ---- host side --------------------------------------------------------------------------------------------------
@@ -460,6 +602,8 @@ void destroy_loops(ga_graph* g) {
         if (L->exec[k]) cudaGraphExecDestroy(L->exec[k]);
         if (L->graph[k]) cudaGraphDestroy(L->graph[k]);
     }
+    if (L->exec_seg) cudaGraphExecDestroy(L->exec_seg);
+    if (L->graph_seg) cudaGraphDestroy(L->graph_seg);
     delete L;   // device buffers belong to g->allocations
     g->loops = nullptr;
 }
@@ -548,9 +692,10 @@ template <int KIND>
 static ga_status enqueue_round(ga_graph* g, cudaStream_t st, cudaGraphConditionalHandle h, int use_h) {
     ga_loops* L = g->loops;
     const unsigned long long* inc_ptr = L->lists == 1 ? L->inc_ptr : nullptr;
+    const Segs sg = KIND == LOOP_PEEL ? L->segs : Segs{};
     if (KIND == LOOP_PEEL) {
         k_peel_mark<<<L->grid_scan, 256, 0, st>>>(L->sc, L->tri, L->state, L->out, L->alive[0], L->alive[1], L->frontier,
-                                             L->item_x, L->item_c, g->rowptr, g->in_ptr, inc_ptr);
+                                             L->item_x, L->item_c, g->rowptr, g->in_ptr, inc_ptr, sg);
     } else {
         k_core_min<<<L->grid_scan, 256, 0, st>>>(L->sc, L->tri, L->alive[0], L->alive[1]);
         k_core_mark<<<L->grid_scan, 256, 0, st>>>(L->sc, L->tri, L->state, L->out, L->alive[0], L->alive[1], L->frontier,
@@ -558,11 +703,11 @@ static ga_status enqueue_round(ga_graph* g, cudaStream_t st, cudaGraphConditiona
     }
     if (L->lists == 1)
         k_frontier_update_list<<<L->grid_update, 256, 0, st>>>(L->sc, L->inc, L->inc_ptr, L->item_x, L->item_c,
-                                                               L->state, L->tri);
+                                                               L->state, L->tri, sg);
     else
         k_frontier_update<<<L->grid_update, kUpdWarps * 32, 0, st>>>(L->sc, g->rowptr, g->col, g->in_ptr, g->in_src,
-                                                                L->item_x, L->item_c, L->state, L->tri);
-    k_retire_tail<KIND><<<L->grid_retire, 256, 0, st>>>(L->sc, L->state, L->frontier, h, use_h);
+                                                                L->item_x, L->item_c, L->state, L->tri, sg);
+    k_retire_tail<KIND><<<L->grid_retire, 256, 0, st>>>(L->sc, L->state, L->frontier, h, use_h, sg);
     GA_CUDA(cudaGetLastError());
     return GA_OK;
 }
@@ -571,10 +716,12 @@ static ga_status enqueue_round(ga_graph* g, cudaStream_t st, cudaGraphConditiona
 template <int KIND>
 static ga_status ensure_graph(ga_graph* g) {
     ga_loops* L = g->loops;
-    if (L->exec[KIND]) return GA_OK;
+    const bool seg = KIND == LOOP_PEEL && L->segs.count > 0;   // a batch peel has its own graph
+    cudaGraphExec_t& exec = seg ? L->exec_seg : L->exec[KIND];
+    if (exec) return GA_OK;
     cudaGraph_t graph;
     GA_CUDA(cudaGraphCreate(&graph, 0));
-    L->graph[KIND] = graph;
+    (seg ? L->graph_seg : L->graph[KIND]) = graph;
     cudaGraphConditionalHandle handle;
     GA_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
     cudaGraphNodeParams params = {};
@@ -599,7 +746,7 @@ static ga_status ensure_graph(ga_graph* g) {
     }
     cudaStreamDestroy(cap);
     GA_TRY(s);
-    GA_CUDA(cudaGraphInstantiate(&L->exec[KIND], graph, 0));
+    GA_CUDA(cudaGraphInstantiate(&exec, graph, 0));
     return GA_OK;
 }
 
@@ -629,10 +776,17 @@ static ga_status run_loop(ga_graph* g, uint64_t num, uint64_t den, LoopScalars* 
     GA_CUDA(cudaMemcpyAsync(g->h_scalars, g->d_scalars, 8, cudaMemcpyDeviceToHost, st));
     GA_CUDA(cudaStreamSynchronize(st));
     const uint64_t T0 = g->h_scalars[0];
-    if (T0 >= (1ull << 32))
+    const bool seg = KIND == LOOP_PEEL && L->segs.count > 0;
+    if (seg) {
+        // a batch: every graph is checked on its own (peel_arith_ok with its own n and T0)
+        k_seg_T<<<std::min<uint32_t>(L->segs.count, 148u * 16u), 256, 0, st>>>(L->tri, L->segs);
+        k_seg_init<<<grid_for(L->segs.count, 256), 256, 0, st>>>(L->segs, num, den);
+        GA_CUDA(cudaGetLastError());
+    } else if (T0 >= (1ull << 32)) {
         return fail(GA_ERR_ARITH, "triangle count %llu >= 2^32: uint32 tri[] counters could overflow",
                     (unsigned long long)T0);
-    if (KIND == LOOP_PEEL) {
+    }
+    if (KIND == LOOP_PEEL && !seg) {
         // peel_arith_ok (densest.h:65-72) with the device count as T0
         if (n > 0 && T0 > UINT64_MAX / ((uint64_t)n * den))
             return fail(GA_ERR_ARITH, "tri*nalive*den could overflow uint64");
@@ -647,7 +801,7 @@ static ga_status run_loop(ga_graph* g, uint64_t num, uint64_t den, LoopScalars* 
         const bool graph_mode = g->opt_loop_mode != 1;
         if (graph_mode) {
             GA_TRY(ensure_graph<KIND>(g));
-            GA_CUDA(cudaGraphLaunch(L->exec[KIND], st));
+            GA_CUDA(cudaGraphLaunch(seg ? L->exec_seg : L->exec[KIND], st));
         } else {
             for (uint64_t r = 0;; r++) {
                 GA_TRY(enqueue_round<KIND>(g, st, 0, 0));
@@ -667,6 +821,71 @@ static ga_status run_loop(ga_graph* g, uint64_t num, uint64_t den, LoopScalars* 
         case LS_NO_PROGRESS: return fail(GA_ERR_DEVICE_CHECK, "no vertex removed in round %u", result->round - 1);
         case LS_LEVEL_DOWN: return fail(GA_ERR_DEVICE_CHECK, "core level decreased in round %u", result->round - 1);
         default: return fail(GA_ERR_DEVICE_CHECK, "removed more vertices than alive (round %u)", result->round - 1);
+    }
+    return GA_OK;
+}
+
+ga_status set_segments(ga_graph* g, const unsigned long long* d_off, uint32_t count) {
+    GA_TRY(ensure_loops(g));
+    Segs& sg = g->loops->segs;
+    sg.count = count;
+    sg.off = d_off;
+    GA_TRY(dalloc(g, &sg.T, count));
+    GA_TRY(dalloc(g, &sg.nalive, count));
+    GA_TRY(dalloc(g, &sg.removed, count));
+    GA_TRY(dalloc(g, &sg.destroyed, count));
+    GA_TRY(dalloc(g, &sg.best_num, count));
+    GA_TRY(dalloc(g, &sg.best_den, count));
+    GA_TRY(dalloc(g, &sg.T0, count));
+    GA_TRY(dalloc(g, &sg.best_round, count));
+    GA_TRY(dalloc(g, &sg.rounds, count));
+    GA_TRY(dalloc(g, &sg.status, count));
+    return GA_OK;
+}
+
+ga_status count_segments(ga_graph* g, uint64_t* triangles) {
+    if (!g->loops || !g->loops->segs.count) return fail(GA_ERR_INVALID_ARGUMENT, "graph has no segments");
+    GA_TRY(prepare(g));
+    ga_loops* L = g->loops;
+    cudaStream_t st = g->stream;
+    TcArgs<unsigned int> a{};
+    a.total = g->d_scalars;
+    a.vsup = L->tri;
+    GA_TRY((run_tc<TC_VSUP, false, unsigned int>(g, a, true)));
+    k_seg_T<<<std::min<uint32_t>(L->segs.count, 148u * 16u), 256, 0, st>>>(L->tri, L->segs);
+    GA_CUDA(cudaGetLastError());
+    GA_CUDA(cudaMemcpyAsync(triangles, L->segs.T0, (size_t)L->segs.count * 8, cudaMemcpyDeviceToHost, st));
+    GA_CUDA(cudaStreamSynchronize(st));
+    return GA_OK;
+}
+
+ga_status peel_segments(ga_graph* g, uint64_t num, uint64_t den, uint64_t* triangles, ga_peel_result* res,
+                        uint32_t* status, uint32_t* removed_round) {
+    if (!g->loops || !g->loops->segs.count) return fail(GA_ERR_INVALID_ARGUMENT, "graph has no segments");
+    LoopScalars s;
+    GA_TRY(run_loop<LOOP_PEEL>(g, num, den, &s));
+    const Segs& sg = g->loops->segs;
+    const uint32_t G = sg.count;
+    std::vector<unsigned long long> T0(G), bn(G), bd(G);
+    std::vector<uint32_t> br(G), rounds(G), st(G);
+    cudaStream_t stream = g->stream;
+    GA_CUDA(cudaMemcpyAsync(T0.data(), sg.T0, (size_t)G * 8, cudaMemcpyDeviceToHost, stream));
+    GA_CUDA(cudaMemcpyAsync(bn.data(), sg.best_num, (size_t)G * 8, cudaMemcpyDeviceToHost, stream));
+    GA_CUDA(cudaMemcpyAsync(bd.data(), sg.best_den, (size_t)G * 8, cudaMemcpyDeviceToHost, stream));
+    GA_CUDA(cudaMemcpyAsync(br.data(), sg.best_round, (size_t)G * 4, cudaMemcpyDeviceToHost, stream));
+    GA_CUDA(cudaMemcpyAsync(rounds.data(), sg.rounds, (size_t)G * 4, cudaMemcpyDeviceToHost, stream));
+    GA_CUDA(cudaMemcpyAsync(st.data(), sg.status, (size_t)G * 4, cudaMemcpyDeviceToHost, stream));
+    if (removed_round && g->n)
+        GA_CUDA(cudaMemcpyAsync(removed_round, g->loops->out, (size_t)g->n * 4, cudaMemcpyDeviceToHost, stream));
+    GA_CUDA(cudaStreamSynchronize(stream));
+    for (uint32_t i = 0; i < G; i++) {
+        if (triangles) triangles[i] = T0[i];
+        if (res) res[i] = ga_peel_result{bn[i], bd[i], br[i], rounds[i]};
+        if (status)
+            status[i] = st[i] == LS_OK ? GA_OK
+                        : st[i] == LS_ARITH ? GA_ERR_ARITH
+                        : st[i] == LS_ROUND_LIMIT ? GA_ERR_ROUND_LIMIT
+                                                  : GA_ERR_DEVICE_CHECK;
     }
     return GA_OK;
 }

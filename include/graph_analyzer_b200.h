@@ -105,6 +105,27 @@ ga_status ga_gen_rmat(uint32_t scale, uint64_t nsamples, double a, double b, dou
 /* Relabels every endpoint through a seeded uniform permutation of 0..n-1. */
 ga_status ga_permute_ids(uint32_t* pairs, uint64_t npairs, uint32_t n, uint64_t seed);
 
+/* Many graphs packed as one concatenated CSR with 64-bit offsets and 32-bit local ids (no counterpart in the
+ * reference, which handles one graph per process). Graph g owns vertices [vtx_off[g], vtx_off[g+1]) and edges
+ * [edge_off[g], edge_off[g+1]); its local rowptr (n_g + 1 entries, values 0..m_g) starts at rowptr[vtx_off[g] + g];
+ * col holds local vertex ids. Each graph is oriented and sorted exactly like build_graph_from_edges. */
+typedef struct ga_host_batch {
+    uint32_t num_graphs;
+    uint64_t total_vertices;   /* N = vtx_off[G]  */
+    uint64_t total_edges;      /* M = edge_off[G] */
+    uint64_t* vtx_off;         /* G + 1           */
+    uint64_t* edge_off;        /* G + 1           */
+    uint32_t* rowptr;          /* N + G           */
+    uint32_t* col;             /* M               */
+} ga_host_batch;
+
+/* Seeded batch of Holme-Kim graphs, generated in parallel: for graph g, n is log-uniform in [n_lo, n_hi], the mean
+ * undirected degree is uniform in [deg_lo, deg_hi] (2 * edges per new vertex, fractional) and the triad probability
+ * uniform in [p_lo, p_hi]; ids permuted per graph. Library-owned result, free with ga_host_batch_free. */
+ga_status ga_gen_holme_kim_batch(uint32_t num_graphs, uint32_t n_lo, uint32_t n_hi, double deg_lo, double deg_hi,
+                                 double p_lo, double p_hi, uint64_t seed, ga_host_batch** out);
+void ga_host_batch_free(ga_host_batch* b);
+
 /* ---------------------------------------------------------------------------------------------------------------
  * Device-resident graph (replaces the upload() + cudaMalloc pattern of gpu_tc.cu:43-62, gpu_densest.cu:48-96 and
  * gpu_dsg.cu:61-80). The CSR stays resident for repeated queries; derived device structures (src, in-lists,
@@ -197,6 +218,28 @@ typedef struct ga_peel_result {
  * Refusals follow peel_arith_ok (densest.h:65-72): GA_ERR_INVALID_ARGUMENT for eps out of range, GA_ERR_ARITH for
  * the overflow bounds. */
 ga_status ga_batch_peel(ga_graph* g, uint64_t num, uint64_t den, ga_peel_result* res, uint32_t* removed_round);
+
+/* ---- batches: many graphs resident together, counted and peeled by single launches (no counterpart in the
+ *      reference, whose drivers handle one graph per process) ---- */
+typedef struct ga_batch ga_batch;
+
+/* Uploads a packed batch (the ga_host_batch layout: vtx_off/edge_off G+1 offsets, rowptr N+G local offsets, col M
+ * local ids; host memory) to `device`. Each graph must be a valid oriented CSR (build_graph_from_edges layout); a
+ * batch holds fewer than 2^32 edges and vertices in total (GA_ERR_CAPACITY otherwise: split it). */
+ga_status ga_batch_create(uint32_t num_graphs, const uint64_t* vtx_off, const uint64_t* edge_off,
+                          const uint32_t* rowptr, const uint32_t* col, int device, void* stream, ga_batch** out);
+ga_status ga_batch_destroy(ga_batch* b);
+/* Same options as ga_graph_set_option, applied to the batch's kernels and loop. */
+ga_status ga_batch_set_option(ga_batch* b, ga_option opt, int64_t value);
+ga_status ga_batch_device_bytes(const ga_batch* b, uint64_t* bytes);
+/* Triangle count of every graph (triangles: host, G entries), one persistent launch over all graphs. */
+ga_status ga_batch_tc(ga_batch* b, uint64_t* triangles);
+/* Triangle count and triangle-density batch peeling (eps = num/den) of every graph: one count launch and one
+ * device-resident peeling loop for all graphs. Per graph (host arrays, G entries, any may be NULL): triangles,
+ * res (the PeelResult integers of that graph peeled alone), status (GA_OK, GA_ERR_ARITH when peel_arith_ok
+ * refuses that graph, GA_ERR_DEVICE_CHECK / GA_ERR_ROUND_LIMIT); removed_round: N entries in batch order. */
+ga_status ga_batch_tc_peel(ga_batch* b, uint64_t num, uint64_t den, uint64_t* triangles, ga_peel_result* res,
+                           uint32_t* status, uint32_t* removed_round);
 
 /* ---- (k, triangle)-core decomposition: replaces core_decomp_loop_inc<GpuCoreBackendInc> (dsg.h:724-751,
  *      gpu_dsg.cu:138-199) ---- */

@@ -139,3 +139,21 @@ def test_device_calls_fail_cleanly_without_gpu(ga):
     with pytest.raises(ga.GAError) as e:
         ga.DeviceGraph(g)
     assert e.value.name == "GA_ERR_NO_DEVICE"
+
+
+def test_holme_kim_batch_generator(ga, oracle):
+    b = ga.gen_holme_kim_batch(24, 64, 3000, 4.0, 16.0, 0.1, 0.7, seed=7)
+    b2 = ga.gen_holme_kim_batch(24, 64, 3000, 4.0, 16.0, 0.1, 0.7, seed=7)
+    assert np.array_equal(b.col, b2.col) and np.array_equal(b.rowptr, b2.rowptr)   # deterministic
+    assert b.num_graphs == 24 and b.vtx_off[0] == 0 and b.edge_off[-1] == len(b.col)
+    ns = np.diff(b.vtx_off)
+    assert ns.min() >= 64 and ns.max() <= 3000
+    for i in range(b.num_graphs):
+        g = b.graph(i)
+        # every packed graph is exactly the reference's orientation of its own edge set
+        pairs = np.stack([g.src, g.col], 1)
+        o = oracle.build_graph_from_edges(g.n, oracle.canonical_edges(pairs))
+        assert np.array_equal(o.rowptr, g.rowptr) and np.array_equal(o.col, g.col)
+        assert 1.5 <= 2 * g.m / g.n <= 17
+    packed = ga.pack_batch([b.graph(i) for i in range(b.num_graphs)])
+    assert np.array_equal(packed.rowptr, b.rowptr) and np.array_equal(packed.col, b.col)
