@@ -101,6 +101,9 @@ struct ga_graph {
     ga_items light, heavy;        // degree-binned work lists of the hash-probe kernel
     bool prepared = false;
     ga_loops* loops = nullptr;    // peeling / core loop state, allocated on first use
+    // a batch: the graph is the disjoint union of seg_count graphs, graph s owning vertices [seg_off[s], seg_off[s+1])
+    const unsigned long long* seg_off = nullptr;
+    uint32_t seg_count = 0;
 
     // small device / pinned host scalars
     unsigned long long* d_scalars = nullptr;   // 64 slots
@@ -109,6 +112,8 @@ struct ga_graph {
 
     // options (ga_option)
     int64_t opt_tc_kernel = 0, opt_loop_mode = 0, opt_max_rounds = 0, opt_update_mode = 0;
+    int tuned_kernel = 0;          // count kernel chosen by the autotuner (1 plain, 2 hash; 0 not tuned yet)
+    uint64_t tune_key = 0;         // degree-distribution signature it was chosen for
     uint32_t item_work = 4096, heavy_bits_cap = 0, light_max_deg = 128;
 
     // every device allocation, freed by ga_graph_destroy
@@ -149,6 +154,12 @@ void destroy_loops(ga_graph* g);
 
 // Builds src, in-lists and work lists (idempotent).
 ga_status prepare(ga_graph* g);
+
+// Picks the count kernel for GA_OPT_TC_KERNEL = 0 from the graph's degree-distribution signature (cached per
+// signature; times both kernels once for a new one). Called by ga_graph_prepare.
+ga_status autotune(ga_graph* g);
+// prepare + autotune (GA_OPT_TC_KERNEL = 0): what every synchronous entry point does first.
+ga_status ready(ga_graph* g);
 
 // Device-wide exclusive scan of n uint32 values (in place allowed) on g's stream.
 ga_status exclusive_scan_u32(ga_graph* g, const uint32_t* in, uint32_t* out, uint32_t n, bool write_total);

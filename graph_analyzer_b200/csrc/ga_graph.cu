@@ -368,6 +368,7 @@ ga_status prepare(ga_graph* g) {
         return fail(GA_ERR_INVALID_GRAPH, "CSR is not oriented by (degree, id) (graph.h:43-45): an edge points from "
                                           "the larger to the smaller endpoint, or an undirected edge is stored twice");
     g->prepared = true;
+    g->tuned_kernel = 0;   // work lists changed: decide the kernel again (cached per signature)
     return GA_OK;
 }
 
@@ -496,7 +497,8 @@ ga_status ga_graph_device_bytes(const ga_graph* g, uint64_t* bytes) {
 
 ga_status ga_graph_prepare(ga_graph* g) {
     if (!g) return fail(GA_ERR_INVALID_ARGUMENT, "null graph");
-    return prepare(g);
+    GA_TRY(use_device(g));
+    return ready(g);
 }
 
 ga_status ga_graph_set_option(ga_graph* g, ga_option opt, int64_t value) {

@@ -586,6 +586,22 @@ static ga_status ensure_loops(ga_graph* g) {
     GA_TRY(dalloc(g, &L->item_x, L->item_cap));
     GA_TRY(dalloc(g, &L->item_c, L->item_cap));
     GA_TRY(dalloc(g, &L->sc, 1));
+    if (g->seg_count) {   // per-graph state of a batch
+        Segs& sg = L->segs;
+        const uint32_t c = g->seg_count;
+        sg.count = c;
+        sg.off = g->seg_off;
+        GA_TRY(dalloc(g, &sg.T, c));
+        GA_TRY(dalloc(g, &sg.nalive, c));
+        GA_TRY(dalloc(g, &sg.removed, c));
+        GA_TRY(dalloc(g, &sg.destroyed, c));
+        GA_TRY(dalloc(g, &sg.best_num, c));
+        GA_TRY(dalloc(g, &sg.best_den, c));
+        GA_TRY(dalloc(g, &sg.T0, c));
+        GA_TRY(dalloc(g, &sg.best_round, c));
+        GA_TRY(dalloc(g, &sg.rounds, c));
+        GA_TRY(dalloc(g, &sg.status, c));
+    }
     // fixed launch shapes (the graph body is captured once): grid-stride scans, persistent update grid
     int occ = 0;
     GA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_frontier_update, kUpdWarps * 32, 0));
@@ -613,7 +629,9 @@ void reset_loops(ga_graph* g) {
     if (!L) return;
     cudaStreamSynchronize(g->stream);
     void* bufs[] = {L->tri, L->state, L->out, L->alive[0], L->alive[1], L->frontier, L->item_x, L->item_c, L->sc,
-                    L->inc, L->inc_ptr};
+                    L->inc, L->inc_ptr, L->segs.T, L->segs.nalive, L->segs.removed, L->segs.destroyed,
+                    L->segs.best_num, L->segs.best_den, L->segs.T0, L->segs.best_round, L->segs.rounds,
+                    L->segs.status};
     for (void* b : bufs) dfree(g, b);
     destroy_loops(g);
 }
@@ -753,7 +771,7 @@ static ga_status ensure_graph(ga_graph* g) {
 // Common driver: init (full per-vertex count, state), then the round loop in the selected mode.
 template <int KIND>
 static ga_status run_loop(ga_graph* g, uint64_t num, uint64_t den, LoopScalars* result) {
-    GA_TRY(prepare(g));
+    GA_TRY(ready(g));
     GA_TRY(ensure_loops(g));
     ga_loops* L = g->loops;
     cudaStream_t st = g->stream;
@@ -826,26 +844,16 @@ static ga_status run_loop(ga_graph* g, uint64_t num, uint64_t den, LoopScalars* 
 }
 
 ga_status set_segments(ga_graph* g, const unsigned long long* d_off, uint32_t count) {
-    GA_TRY(ensure_loops(g));
-    Segs& sg = g->loops->segs;
-    sg.count = count;
-    sg.off = d_off;
-    GA_TRY(dalloc(g, &sg.T, count));
-    GA_TRY(dalloc(g, &sg.nalive, count));
-    GA_TRY(dalloc(g, &sg.removed, count));
-    GA_TRY(dalloc(g, &sg.destroyed, count));
-    GA_TRY(dalloc(g, &sg.best_num, count));
-    GA_TRY(dalloc(g, &sg.best_den, count));
-    GA_TRY(dalloc(g, &sg.T0, count));
-    GA_TRY(dalloc(g, &sg.best_round, count));
-    GA_TRY(dalloc(g, &sg.rounds, count));
-    GA_TRY(dalloc(g, &sg.status, count));
-    return GA_OK;
+    reset_loops(g);
+    g->seg_off = d_off;
+    g->seg_count = count;
+    return ensure_loops(g);
 }
 
 ga_status count_segments(ga_graph* g, uint64_t* triangles) {
-    if (!g->loops || !g->loops->segs.count) return fail(GA_ERR_INVALID_ARGUMENT, "graph has no segments");
-    GA_TRY(prepare(g));
+    if (!g->seg_count) return fail(GA_ERR_INVALID_ARGUMENT, "graph has no segments");
+    GA_TRY(ready(g));
+    GA_TRY(ensure_loops(g));
     ga_loops* L = g->loops;
     cudaStream_t st = g->stream;
     TcArgs<unsigned int> a{};
@@ -861,7 +869,7 @@ ga_status count_segments(ga_graph* g, uint64_t* triangles) {
 
 ga_status peel_segments(ga_graph* g, uint64_t num, uint64_t den, uint64_t* triangles, ga_peel_result* res,
                         uint32_t* status, uint32_t* removed_round) {
-    if (!g->loops || !g->loops->segs.count) return fail(GA_ERR_INVALID_ARGUMENT, "graph has no segments");
+    if (!g->seg_count) return fail(GA_ERR_INVALID_ARGUMENT, "graph has no segments");
     LoopScalars s;
     GA_TRY(run_loop<LOOP_PEEL>(g, num, den, &s));
     const Segs& sg = g->loops->segs;

@@ -31,6 +31,10 @@
 //          through shared counters as above, e_ux with one global atomic per triangle.
 //   ALIVE: restricts everything to the subgraph induced by alive[] (tc_per_vertex_alive, kernels.cuh:399-425).
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <mutex>
 
 #include "ga_device.cuh"
 #include "ga_tc.cuh"
@@ -447,9 +451,123 @@ ga_status run_tc(ga_graph* g, const TcArgs<CT>& a, bool zero_outputs) {
         if (MODE == TC_VSUP && g->n) GA_CUDA(cudaMemsetAsync(a.vsup, 0, (size_t)g->n * sizeof(CT), st));
         if (MODE == TC_ESUP && g->m) GA_CUDA(cudaMemsetAsync(a.esup, 0, (size_t)g->m * sizeof(uint32_t), st));
     }
-    if (g->opt_tc_kernel == 1) return launch_plain<MODE, ALIVE, CT>(g, a);
+    const int64_t kernel = g->opt_tc_kernel ? g->opt_tc_kernel : g->tuned_kernel;
+    if (kernel == 1) return launch_plain<MODE, ALIVE, CT>(g, a);
     if (g->heavy.count == 0 && g->light.count == 0) return GA_OK;
     return launch_hash<MODE, ALIVE, CT>(g, a);
+}
+
+// ---- autotuner ----------------------------------------------------------------------------------------------------
+// The best count kernel depends on the degree distribution: on graphs whose out-lists are all short (Holme-Kim with a
+// handful of edges per vertex) the plain merge wins, on skewed graphs with long lists (R-MAT) the degree-binned hash
+// kernel wins by several times. The choice is cached per degree-distribution signature: log2 of n and m and the
+// fraction of edges whose source has out-degree in each log2 bucket, in sixteenths. A signature seen before is
+// answered from the cache (process-wide; also kept in the file named by GA_TUNE_CACHE when that is set); a new one
+// is decided by timing both kernels once on the graph.
+
+__global__ void k_degree_hist(const uint32_t* __restrict__ rowptr, uint32_t n, unsigned long long* hist) {
+    __shared__ unsigned long long s_h[33];
+    if (threadIdx.x < 33) s_h[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const uint32_t d = rowptr[v + 1] - rowptr[v];
+        if (d) atomicAdd(&s_h[32 - __clz(d)], (unsigned long long)d);
+    }
+    __syncthreads();
+    if (threadIdx.x < 33 && s_h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], s_h[threadIdx.x]);
+}
+
+static std::mutex g_tune_mu;
+static std::map<uint64_t, int> g_tune_cache;
+static bool g_tune_loaded = false;
+
+static void tune_cache_load_locked() {
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char* path = std::getenv("GA_TUNE_CACHE");
+    if (!path) return;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return;
+    unsigned long long key;
+    int kernel;
+    while (std::fscanf(f, "%llx %d", &key, &kernel) == 2)
+        if (kernel == 1 || kernel == 2) g_tune_cache[key] = kernel;
+    std::fclose(f);
+}
+
+static void tune_cache_store_locked(uint64_t key, int kernel) {
+    g_tune_cache[key] = kernel;
+    const char* path = std::getenv("GA_TUNE_CACHE");
+    if (!path) return;
+    FILE* f = std::fopen(path, "a");
+    if (!f) return;
+    std::fprintf(f, "%llx %d\n", (unsigned long long)key, kernel);
+    std::fclose(f);
+}
+
+ga_status ready(ga_graph* g) {
+    GA_TRY(prepare(g));
+    if (g->opt_tc_kernel == 0) GA_TRY(autotune(g));
+    return GA_OK;
+}
+
+ga_status autotune(ga_graph* g) {
+    if (g->tuned_kernel) return GA_OK;
+    cudaStream_t st = g->stream;
+    const uint32_t n = g->n;
+    if (g->m == 0) { g->tuned_kernel = 2; return GA_OK; }
+    // signature
+    unsigned long long* d_hist = nullptr;
+    GA_CUDA(cudaMallocAsync((void**)&d_hist, 33 * 8, st));
+    unsigned long long hist[33] = {};
+    cudaMemsetAsync(d_hist, 0, 33 * 8, st);
+    k_degree_hist<<<grid_for(n, 256, (unsigned)g->sm_count * 8), 256, 0, st>>>(g->rowptr, n, d_hist);
+    cudaMemcpyAsync(hist, d_hist, 33 * 8, cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(d_hist, st);
+    GA_CUDA(cudaStreamSynchronize(st));
+    uint64_t key = mix64(32 - __builtin_clz(n | 1)) ^ mix64(0x100 + 32 - __builtin_clz(g->m));
+    for (int b = 0; b < 33; b++) {
+        const uint64_t q = (hist[b] * 16 + g->m / 2) / g->m;   // sixteenths of the edges
+        key = mix64(key ^ (q << 8) ^ (uint64_t)b);
+    }
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        tune_cache_load_locked();
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            g->tuned_kernel = it->second;
+            g->tune_key = key;
+            return GA_OK;
+        }
+    }
+    // time both kernels once (count only) on this graph
+    cudaEvent_t e0, e1;
+    GA_CUDA(cudaEventCreate(&e0));
+    GA_CUDA(cudaEventCreate(&e1));
+    float ms[3] = {0, 0, 0};
+    TcArgs<unsigned int> a{};
+    a.total = g->d_scalars + 2;
+    ga_status s = GA_OK;
+    for (int k = 1; k <= 2 && s == GA_OK; k++) {
+        g->tuned_kernel = k;
+        cudaEventRecord(e0, st);
+        s = run_tc<TC_COUNT, false, unsigned int>(g, a, true);
+        cudaEventRecord(e1, st);
+        if (s == GA_OK && cudaEventSynchronize(e1) != cudaSuccess) s = fail(GA_ERR_CUDA, "autotune timing failed");
+        if (s == GA_OK) cudaEventElapsedTime(&ms[k], e0, e1);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    g->tuned_kernel = 0;
+    GA_TRY(s);
+    const int best = ms[1] < ms[2] ? 1 : 2;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        tune_cache_store_locked(key, best);
+    }
+    g->tuned_kernel = best;
+    g->tune_key = key;
+    return GA_OK;
 }
 
 template ga_status run_tc<TC_COUNT, false, unsigned int>(ga_graph*, const TcArgs<unsigned int>&, bool);
@@ -486,6 +604,7 @@ extern "C" {
 ga_status ga_tc_count(ga_graph* g, uint64_t* triangles) {
     if (!g || !triangles) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
     GA_TRY(use_device(g));
+    GA_TRY(ready(g));
     TcArgs<unsigned int> a{};
     a.total = g->d_scalars;
     GA_TRY((run_tc<TC_COUNT, false, unsigned int>(g, a, true)));
@@ -503,6 +622,7 @@ ga_status ga_tc_count_async(ga_graph* g, uint64_t* d_triangles) {
 ga_status ga_tc_support_edges_device(ga_graph* g, uint32_t* d_sup, uint64_t* triangles) {
     if (!g || (!d_sup && g->m)) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
     GA_TRY(use_device(g));
+    GA_TRY(ready(g));
     TcArgs<unsigned int> a{};
     a.total = g->d_scalars;
     a.esup = d_sup;
@@ -525,6 +645,7 @@ ga_status ga_tc_support_edges(ga_graph* g, uint32_t* sup, uint64_t* triangles) {
 ga_status ga_tc_support_vertices(ga_graph* g, uint64_t* deg, uint64_t* triangles) {
     if (!g || (!deg && g->n)) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
     GA_TRY(use_device(g));
+    GA_TRY(ready(g));
     Scratch s;
     s.st = g->stream;
     GA_CUDA(cudaMallocAsync(&s.p, ((size_t)g->n + 1) * 8, g->stream));
