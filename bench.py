@@ -301,6 +301,162 @@ def run_ours(args):
     return 0
 
 
+# ---- secondary workloads (one JSON line each; the default line above is the headline) ---------------------------
+
+def _timed(torch, fn, reps=1):
+    """Device-synchronised wall time of fn() in ms (mean over reps) and its last result."""
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = None
+    for _ in range(reps):
+        r = fn()
+    torch.cuda.synchronize()
+    return (time.perf_counter() - t0) * 1e3 / reps, r
+
+
+def _peel_key(p):
+    return (p.best_num, p.best_den, p.best_round, p.rounds)
+
+
+def run_hk2(args):
+    """Holme-Kim n = 1.70M, 6-7 edges per new vertex (mean 6.54), p = 0.3: (a) plain one-kernel-per-launch count and
+    host-driven peeling (one sync per round) vs (b) autotuned kernels with the peeling loop captured as a CUDA graph,
+    eps in {1/20, 1/10, 1/2}; results must be bit-identical between the two."""
+    import torch
+    import graph_analyzer_b200 as ga
+    t0 = time.time()
+    g = ga.graph_from_pairs(1_700_000, ga.gen_holme_kim(1_700_000, 6, 7, 0.54, 0.3, seed=SEED))
+    log(f"graph: Holme-Kim n={g.n} m={g.m} ({time.time() - t0:.1f} s on the host)")
+    plain = ga.DeviceGraph(g)
+    for opt, v in ((ga.OPT_TC_KERNEL, 1), (ga.OPT_LOOP_MODE, 1), (ga.OPT_UPDATE_MODE, 1)):
+        plain.set_option(opt, v)
+    tuned = ga.DeviceGraph(g)
+    tuned.set_option(ga.OPT_LOOP_MODE, 2)
+    plain.prepare()
+    tuned.prepare()
+    out = {"tc_ms": {}, "peel_ms": {}, "first_peel_ms_tuned": None}
+    T = {}
+    for name, d in (("plain", plain), ("tuned", tuned)):
+        for _ in range(args.warmup):
+            d.tc_count()
+        out["tc_ms"][name], T[name] = _timed(torch, d.tc_count, args.steps)
+    assert T["plain"] == T["tuned"]
+    first, _ = _timed(torch, lambda: tuned.batch_peel(1, 10))   # builds the incidence lists once
+    out["first_peel_ms_tuned"] = first
+    identical = True
+    for num, den in ((1, 20), (1, 10), (1, 2)):
+        res = {}
+        for name, d in (("plain", plain), ("tuned", tuned)):
+            d.batch_peel(num, den)
+            ms, res[name] = _timed(torch, lambda: d.batch_peel(num, den), max(1, args.steps // 2))
+            out["peel_ms"].setdefault(f"{num}/{den}", {})[name] = ms
+        identical &= res["plain"] == res["tuned"]
+        out["peel_ms"][f"{num}/{den}"]["result"] = list(_peel_key(res["tuned"]))
+    plain.close()
+    tuned.close()
+    tot = {k: out["tc_ms"][k] + sum(v[k] for v in out["peel_ms"].values()) for k in ("plain", "tuned")}
+    line = {"workload": "hk1.7M_tc_peel", "metric": "TC + batch peel (3 eps) ms, plain vs autotuned graph-captured",
+            "value": tot["tuned"], "unit": "ms", "higher_is_better": False, "plain_ms": tot["plain"],
+            "speedup": tot["plain"] / tot["tuned"], "bit_identical": bool(identical), "triangles": T["tuned"],
+            "n": g.n, "m": g.m, **out}
+    print(json.dumps(line), flush=True)
+    return 0 if identical else 1
+
+
+def run_rmat22_full(args):
+    """R-MAT scale 22 (34.7M edges): TC, per-edge uint32 supports and the full (k, triangle)-core decomposition;
+    plain launches (one-thread-per-edge kernel, host-driven rounds) vs autotuned + graph-captured."""
+    import torch
+    import graph_analyzer_b200 as ga
+    g = make_graph(ga)
+    plain = ga.DeviceGraph(g)
+    for opt, v in ((ga.OPT_TC_KERNEL, 1), (ga.OPT_LOOP_MODE, 1)):
+        plain.set_option(opt, v)
+    tuned = ga.DeviceGraph(g)
+    tuned.set_option(ga.OPT_LOOP_MODE, 2)
+    plain.prepare()
+    tuned.prepare()
+    d_sup = torch.zeros(g.m, dtype=torch.int32, device="cuda")
+    out = {}
+    for name, d in (("plain", plain), ("tuned", tuned)):
+        d.tc_count()
+        out[f"tc_ms_{name}"], T = _timed(torch, d.tc_count, args.steps)
+        d.support_edges_device(d_sup.data_ptr())
+        out[f"esup_ms_{name}"], _ = _timed(torch, lambda: d.support_edges_device(d_sup.data_ptr()), 2)
+    first, _ = _timed(torch, lambda: tuned.core_decomposition(want_core=False))   # lists built here
+    out["first_cores_ms_tuned"] = first
+    res = {}
+    for name, d in (("plain", plain), ("tuned", tuned)):
+        out[f"cores_ms_{name}"], res[name] = _timed(torch, lambda: d.core_decomposition(), 1)
+    identical = (res["plain"].kmax == res["tuned"].kmax and res["plain"].rounds == res["tuned"].rounds
+                 and np.array_equal(res["plain"].core, res["tuned"].core))
+    plain.close()
+    tuned.close()
+    line = {"workload": "rmat22_tc_esup_cores", "metric": "TC, per-edge supports, (k,triangle)-cores ms",
+            "value": out["tc_ms_tuned"] + out["esup_ms_tuned"] + out["cores_ms_tuned"], "unit": "ms",
+            "higher_is_better": False, "triangles": T, "kmax": res["tuned"].kmax, "rounds": res["tuned"].rounds,
+            "bit_identical": bool(identical), "n": g.n, "m": g.m, **out}
+    print(json.dumps(line), flush=True)
+    return 0 if identical else 1
+
+
+def run_batch(args):
+    """4,096 Holme-Kim graphs (n log-uniform in [64, 262144], mean degree U[4, 32], p U[0.1, 0.7]) packed as one
+    concatenated CSR: TC + eps = 1/10 batch peeling of every graph by one count launch and one graph-captured
+    peeling loop, vs 4,096 plain per-graph launches (one-thread-per-edge count, host-driven rounds)."""
+    import torch
+    import graph_analyzer_b200 as ga
+    G = args.graphs
+    t0 = time.time()
+    b = ga.gen_holme_kim_batch(G, 64, 262144, 4.0, 32.0, 0.1, 0.7, seed=SEED)
+    N, M = int(b.vtx_off[-1]), int(b.edge_off[-1])
+    log(f"batch: {G} graphs, N={N} M={M} ({time.time() - t0:.1f} s on the host)")
+    t0 = time.perf_counter()
+    db = ga.DeviceBatch(b)
+    create_ms = (time.perf_counter() - t0) * 1e3
+    first_ms, r0 = _timed(torch, lambda: db.tc_peel(1, 10))        # autotune + incidence lists + run
+    steps = max(1, args.steps // 2)
+    batch_ms, r = _timed(torch, lambda: db.tc_peel(1, 10), steps)
+    assert np.array_equal(r.triangles, r0.triangles)
+    db_bytes = db.device_bytes()
+    db.close()
+    # plain: every graph resident on its own, one count launch and a host-driven peeling loop per graph
+    rp = torch.from_numpy(b.rowptr.view(np.int32)).cuda()
+    cl = torch.from_numpy(b.col.view(np.int32)).cuda()
+    handles = []
+    for i in range(G):
+        v0, e0 = int(b.vtx_off[i]), int(b.edge_off[i])
+        n, m = int(b.vtx_off[i + 1]) - v0, int(b.edge_off[i + 1]) - e0
+        d = ga.DeviceGraph.from_device(rp.data_ptr() + 4 * (v0 + i), cl.data_ptr() + 4 * e0, n, m)
+        for opt, v in ((ga.OPT_TC_KERNEL, 1), (ga.OPT_LOOP_MODE, 1), (ga.OPT_UPDATE_MODE, 1)):
+            d.set_option(opt, v)
+        d.prepare()
+        handles.append(d)
+    del rp, cl
+    mismatches = 0
+
+    def plain_all():
+        nonlocal mismatches
+        mismatches = 0
+        for i, d in enumerate(handles):
+            t = d.tc_count()
+            p = d.batch_peel(1, 10, want_removed=False)
+            if t != r.triangles[i] or _peel_key(p) != (r.best_num[i], r.best_den[i], r.best_round[i], r.rounds[i]):
+                mismatches += 1
+    plain_all()                                                       # warm-up (loop state per graph)
+    plain_ms, _ = _timed(torch, plain_all, 1)
+    for d in handles:
+        d.close()
+    line = {"workload": "batch4096_hk_tc_peel", "metric": "batched vs plain graphs/s (TC + eps=1/10 batch peel)",
+            "value": G / (batch_ms / 1e3), "unit": "graphs/s", "higher_is_better": True,
+            "plain_graphs_per_s": G / (plain_ms / 1e3), "speedup_vs_plain": plain_ms / batch_ms,
+            "batch_ms": batch_ms, "first_batch_ms": first_ms, "create_ms": create_ms, "plain_ms": plain_ms,
+            "graphs": G, "N": N, "M": M, "triangles": int(r.triangles.sum()), "device_bytes": db_bytes,
+            "bit_identical": mismatches == 0, "status_ok": bool(np.all(r.status == 0))}
+    print(json.dumps(line), flush=True)
+    return 0 if mismatches == 0 else 1
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -308,12 +464,21 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--workload", choices=["rmat22", "hk2", "rmat22-full", "batch"], default="rmat22",
+                    help="rmat22 (default, the headline line) or a secondary workload")
+    ap.add_argument("--graphs", type=int, default=4096, help="graphs in the batch workload")
     args = ap.parse_args()
     if args.warmup < 3:
         log("warm-up raised to 3 steps")
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "hk2":
+        return run_hk2(args)
+    if args.workload == "rmat22-full":
+        return run_rmat22_full(args)
+    if args.workload == "batch":
+        return run_batch(args)
     return run_ours(args)
 
 
