@@ -457,6 +457,134 @@ def run_batch(args):
     return 0 if mismatches == 0 else 1
 
 
+def _serve_trace(ga, R, rng):
+    """Request trace: 60% TC, 30% batch peel (eps = 1/10), 10% (k, triangle)-cores; 30% of requests re-query one of the
+    32 most recently used graphs, the others go to a new graph - 95% Holme-Kim from the batch generator above, 5% R-MAT
+    at scales 20-23 (a new registration of one pre-built graph per scale, so it is uploaded like a new graph)."""
+    t0 = time.time()
+    hk = ga.gen_holme_kim_batch(R, 64, 262144, 4.0, 32.0, 0.1, 0.7, seed=SEED + 7)
+    rmat = {sc: make_graph(ga, sc, EDGE_FACTOR, SEED + sc) for sc in (20, 21, 22, 23)}
+    graphs, used, trace, hk_next = [], [], [], 0
+    for _ in range(R):
+        if used and rng.random() < 0.3:
+            gi = used[-1 - int(rng.integers(0, min(len(used), 32)))]
+        else:
+            if rng.random() < 0.05:
+                graphs.append(rmat[int(rng.integers(20, 24))])
+            else:
+                graphs.append(hk.graph(hk_next))
+                hk_next += 1
+            gi = len(graphs) - 1
+            used.append(gi)
+        u = rng.random()
+        trace.append((gi, 0 if u < 0.6 else 1 if u < 0.9 else 2))
+    log(f"serve trace: {R} requests on {len(graphs)} graphs ({time.time() - t0:.1f} s on the host)")
+    return graphs, trace
+
+
+def _serve_value(ga, kind, r):
+    if kind == ga.REQ_TC:
+        return (r.triangles,)
+    if kind == ga.REQ_PEEL:
+        return (r.peel.best_num, r.peel.best_den, r.peel.best_round, r.peel.rounds)
+    return r.core
+
+
+def _serve_run(ga, graphs, trace, arrivals_s):
+    """Submits the trace at the given arrival times (open loop) to a fresh server; returns per-request latency (ms,
+    submit to completion), results, wall time of the run and the server statistics."""
+    with ga.Server() as s:
+        ids = [s.add_graph(g) for g in graphs]
+        tickets = []
+        t0 = time.perf_counter()
+        for (gi, kind), at in zip(trace, arrivals_s):
+            dt = t0 + at - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            tickets.append(s.submit(ids[gi], kind, 1, 10))
+        res = [s.wait(t) for t in tickets]
+        wall = time.perf_counter() - t0
+        st = s.stats()
+    lat = np.array([r.queue_ms + r.run_ms for r in res])
+    return lat, res, wall, st
+
+
+def _fifo_latency(service_s, arrivals_s):
+    """Latency (ms) of a single serial server (FIFO) given measured service times and arrival times."""
+    free, lat = 0.0, []
+    for sv, at in zip(service_s, arrivals_s):
+        start = max(free, at)
+        free = start + sv
+        lat.append((free - at) * 1e3)
+    return np.array(lat)
+
+
+def run_serve(args):
+    """Serving: open-loop Poisson arrivals (rate swept) into the request loop (admission under a 150 GB HBM budget,
+    resident graphs for re-queries, small requests folded into batch launches, 4 concurrent streams), against serial
+    plain launches (one request at a time: uploaded, counted with the one-thread-per-edge kernel, its peeling or core
+    rounds driven from the host, freed).
+    Results of every request must be identical in both."""
+    import torch
+    import graph_analyzer_b200 as ga
+    R = args.requests
+    rng = np.random.default_rng(SEED)
+    graphs, trace = _serve_trace(ga, R, rng)
+    # serial plain launches: measured service time of every request in trace order
+    service, plain_vals = [], []
+    for gi, kind in trace[: min(R, 8)]:                                 # warm-up (module load, pools)
+        with ga.DeviceGraph(graphs[gi]) as d:
+            d.tc_count()
+    for gi, kind in trace:
+        t0 = time.perf_counter()
+        with ga.DeviceGraph(graphs[gi]) as d:
+            for opt, v in ((ga.OPT_TC_KERNEL, 1), (ga.OPT_LOOP_MODE, 1)):
+                d.set_option(opt, v)
+            if kind == ga.REQ_TC:
+                val = (d.tc_count(),)
+            elif kind == ga.REQ_PEEL:
+                val = _peel_key(d.batch_peel(1, 10, want_removed=False))
+            else:
+                c = d.core_decomposition(want_core=False)
+                val = (c.kmax, c.rounds)
+        torch.cuda.synchronize()
+        service.append(time.perf_counter() - t0)
+        plain_vals.append(val)
+    serial_s = float(sum(service))
+    # closed-loop burst (all requests at t = 0): the server's capacity; also warms the kernel-choice cache
+    lat, res, wall, st = _serve_run(ga, graphs, trace, np.zeros(R))
+    capacity = R / wall
+    identical = all(_serve_value(ga, k, r) == v and r.status == 0 for (_, k), r, v in zip(trace, res, plain_vals))
+    burst = {"req_s": capacity, "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+             "folded_launches": st["folded_launches"], "evictions": st["evictions"],
+             "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9}
+    sweep = []
+    for frac in args.rate_fracs:
+        rate = frac * capacity
+        arr = np.cumsum(rng.exponential(1.0 / rate, R))
+        arr -= arr[0]
+        lat, res, wall, st = _serve_run(ga, graphs, trace, arr)
+        identical &= all(_serve_value(ga, k, r) == v and r.status == 0
+                         for (_, k), r, v in zip(trace, res, plain_vals))
+        slat = _fifo_latency(service, arr)
+        sweep.append({"offered_req_s": rate, "achieved_req_s": R / wall,
+                      "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                      "serial_plain_p50_ms": float(np.percentile(slat, 50)),
+                      "serial_plain_p99_ms": float(np.percentile(slat, 99)),
+                      "folded_launches": st["folded_launches"], "evictions": st["evictions"],
+                      "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9})
+        log(f"serve: offered {rate:.1f} req/s -> p50 {sweep[-1]['p50_ms']:.2f} ms p99 {sweep[-1]['p99_ms']:.2f} ms "
+            f"(serial plain p99 {sweep[-1]['serial_plain_p99_ms']:.1f} ms)")
+    kinds = np.bincount([k for _, k in trace], minlength=3)
+    line = {"workload": "serve_poisson", "metric": "serving requests/s and p50/p99 latency vs serial plain launches",
+            "value": capacity, "unit": "req/s", "higher_is_better": True, "serial_plain_req_s": R / serial_s,
+            "speedup_vs_serial_plain": capacity / (R / serial_s), "requests": R, "graphs": len(graphs),
+            "mix": {"tc": int(kinds[0]), "peel_eps_1_10": int(kinds[1]), "cores": int(kinds[2])},
+            "hbm_budget_gb": 150, "slots": 4, "burst": burst, "sweep": sweep, "bit_identical": bool(identical)}
+    print(json.dumps(line), flush=True)
+    return 0 if identical else 1
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -464,9 +592,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", choices=["rmat22", "hk2", "rmat22-full", "batch"], default="rmat22",
+    ap.add_argument("--workload", choices=["rmat22", "hk2", "rmat22-full", "batch", "serve"], default="rmat22",
                     help="rmat22 (default, the headline line) or a secondary workload")
     ap.add_argument("--graphs", type=int, default=4096, help="graphs in the batch workload")
+    ap.add_argument("--requests", type=int, default=600, help="requests in the serve workload")
+    ap.add_argument("--rate-fracs", type=float, nargs="+", default=[0.25, 0.5, 0.75, 0.9],
+                    help="serve workload: offered Poisson rates as fractions of the measured burst capacity")
     args = ap.parse_args()
     if args.warmup < 3:
         log("warm-up raised to 3 steps")
@@ -479,6 +610,8 @@ def main():
         return run_rmat22_full(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "serve":
+        return run_serve(args)
     return run_ours(args)
 
 

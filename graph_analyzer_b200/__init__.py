@@ -81,6 +81,22 @@ class _CoreRes(C.Structure):
     _fields_ = [("kmax", C.c_uint32), ("rounds", C.c_uint32)]
 
 
+class _ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int), ("hbm_budget_bytes", C.c_uint64), ("slots", C.c_uint32),
+                ("fold_max_graphs", C.c_uint32), ("fold_max_edges", C.c_uint32)]
+
+
+class _RequestResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("triangles", C.c_uint64), ("peel", _PeelRes), ("core", _CoreRes),
+                ("queue_ms", C.c_double), ("run_ms", C.c_double), ("folded", C.c_uint32),
+                ("resident_hit", C.c_uint32)]
+
+
+class _ServerStats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("submitted", "completed", "folded_launches", "evictions",
+                                          "resident_graphs", "resident_bytes", "peak_reserved_bytes")]
+
+
 class _HostBatch(C.Structure):
     _fields_ = [("num_graphs", C.c_uint32), ("total_vertices", C.c_uint64), ("total_edges", C.c_uint64),
                 ("vtx_off", C.POINTER(C.c_uint64)), ("edge_off", C.POINTER(C.c_uint64)),
@@ -125,6 +141,13 @@ SIGNATURES: dict[str, list] = {
     "ga_batch_device_bytes": [_vp, C.POINTER(C.c_uint64)],
     "ga_batch_tc": [_vp, _vp],
     "ga_batch_tc_peel": [_vp, C.c_uint64, C.c_uint64, _vp, _vp, _vp, _vp],
+    "ga_server_create": [C.POINTER(_ServerConfig), C.POINTER(_vp)],
+    "ga_server_destroy": [_vp],
+    "ga_server_add_graph": [_vp, _u32p, _vp, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64)],
+    "ga_server_submit": [_vp, C.c_uint64, C.c_int, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)],
+    "ga_server_poll": [_vp, C.c_uint64, C.POINTER(_RequestResult)],
+    "ga_server_wait": [_vp, C.c_uint64, C.POINTER(_RequestResult)],
+    "ga_server_stats_get": [_vp, C.POINTER(_ServerStats)],
 }
 _RESTYPE = {"ga_status_string": C.c_char_p, "ga_last_error": C.c_char_p, "ga_host_graph_free": None,
             "ga_host_batch_free": None}
@@ -584,3 +607,89 @@ class DeviceBatch:
                          np.array([r.best_round for r in res], np.uint32),
                          np.array([r.rounds for r in res], np.uint32), st,
                          rr[: self.N] if rr is not None else np.zeros(0, np.uint32))
+
+
+# ------------------------------------------------------------------------------------------------------------------
+# serving: request loop with admission by HBM budget, resident graphs and folded batch launches (ga_server)
+# ------------------------------------------------------------------------------------------------------------------
+
+REQ_TC, REQ_PEEL, REQ_CORE = 0, 1, 2
+GA_ERR_NOT_READY = 12
+
+
+@dataclass
+class RequestResult:
+    status: int
+    triangles: int
+    peel: PeelResult            # REQ_PEEL (integer fields; removed_round is not returned by the server)
+    core: tuple[int, int]       # REQ_CORE: (kmax, rounds)
+    queue_ms: float
+    run_ms: float
+    folded: int                 # graphs served by the same launch (1 = alone)
+    resident_hit: bool
+
+
+def _request_result(r: _RequestResult) -> RequestResult:
+    return RequestResult(r.status, r.triangles,
+                         PeelResult(r.peel.best_num, r.peel.best_den, r.peel.best_round, r.peel.rounds),
+                         (r.core.kmax, r.core.rounds), r.queue_ms, r.run_ms, r.folded, bool(r.resident_hit))
+
+
+class Server:
+    """A request loop on one GPU (ga_server): graphs are registered once, requests are submitted without waiting and
+    run concurrently on `slots` streams; small count/peel requests queued together share one batch launch."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, slots: int = 0, fold_max_graphs: int = 0,
+                 fold_max_edges: int = 0):
+        cfg = _ServerConfig(device, hbm_budget_bytes, slots, fold_max_graphs, fold_max_edges)
+        h = _vp()
+        _check(lib().ga_server_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        """Waits for every submitted request, then frees the device memory."""
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().ga_server_destroy(self._h)
+            self._h = _vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_graph(self, g: Graph) -> int:
+        gid = C.c_uint64(0)
+        rowptr = np.ascontiguousarray(g.rowptr, np.uint32)
+        col = np.ascontiguousarray(g.col, np.uint32)
+        _check(lib().ga_server_add_graph(self._h, rowptr, _ptr(col) if g.m else None, g.n, g.m, C.byref(gid)))
+        return gid.value
+
+    def submit(self, graph_id: int, kind: int, num: int = 1, den: int = 10) -> int:
+        t = C.c_uint64(0)
+        _check(lib().ga_server_submit(self._h, graph_id, kind, num, den, C.byref(t)))
+        return t.value
+
+    def poll(self, ticket: int) -> RequestResult | None:
+        r = _RequestResult()
+        st = lib().ga_server_poll(self._h, ticket, C.byref(r))
+        if st == GA_ERR_NOT_READY:
+            return None
+        _check(st)
+        return _request_result(r)
+
+    def wait(self, ticket: int) -> RequestResult:
+        r = _RequestResult()
+        _check(lib().ga_server_wait(self._h, ticket, C.byref(r)))
+        return _request_result(r)
+
+    def stats(self) -> dict:
+        st = _ServerStats()
+        _check(lib().ga_server_stats_get(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in _ServerStats._fields_}

@@ -252,6 +252,56 @@ typedef struct ga_core_result {
  * Refuses T >= 2^32 with GA_ERR_ARITH (dsg.h:727). */
 ga_status ga_core_decomposition(ga_graph* g, uint32_t* core, ga_core_result* res);
 
+/* ---- serving: a request loop with continuous batching (no counterpart in the reference) ----
+ * Requests (triangle count, batch peeling, (k,triangle)-cores) on registered graphs are admitted while device memory
+ * under the HBM budget and a free slot allow: each slot is a host worker with its own CUDA stream, so admitted
+ * requests overlap on the device. Graphs stay resident after a request (re-queries skip the upload and the derived
+ * index) until the budget needs their memory (least recently used first). Small count/peel requests that are queued
+ * together are folded into one batch launch (ga_batch). Every request's result equals the result of running it
+ * alone. */
+typedef struct ga_server ga_server;
+
+typedef struct ga_server_config {
+    int device;
+    uint64_t hbm_budget_bytes;   /* admission budget for resident graphs and running requests (0 = 150 GB)      */
+    uint32_t slots;              /* concurrent requests (0 = 4)                                                  */
+    uint32_t fold_max_graphs;    /* small requests folded into one batch launch (0 = 64; 1 disables folding)     */
+    uint32_t fold_max_edges;     /* a graph with at most this many edges counts as small (0 = 65536)             */
+} ga_server_config;
+
+typedef enum ga_request_kind { GA_REQ_TC = 0, GA_REQ_PEEL = 1, GA_REQ_CORE = 2 } ga_request_kind;
+
+typedef struct ga_request_result {
+    ga_status status;
+    uint64_t triangles;          /* every kind                                                  */
+    ga_peel_result peel;         /* GA_REQ_PEEL                                                 */
+    ga_core_result core;         /* GA_REQ_CORE                                                 */
+    double queue_ms;             /* submit -> start of execution                                */
+    double run_ms;               /* start -> completion                                         */
+    uint32_t folded;             /* graphs in the batch launch that served it (1 = alone)       */
+    uint32_t resident_hit;       /* the graph was already resident on the device                */
+} ga_request_result;
+
+typedef struct ga_server_stats {
+    uint64_t submitted, completed, folded_launches, evictions, resident_graphs;
+    uint64_t resident_bytes, peak_reserved_bytes;
+} ga_server_stats;
+
+ga_status ga_server_create(const ga_server_config* config, ga_server** out);
+/* Waits for every submitted request, then frees all device memory. */
+ga_status ga_server_destroy(ga_server* s);
+/* Registers a graph (host CSR, copied; oriented like build_graph_from_edges). GA_ERR_BUDGET if it alone can never
+ * fit the budget. */
+ga_status ga_server_add_graph(ga_server* s, const uint32_t* rowptr, const uint32_t* col, uint32_t n, uint32_t m,
+                              uint64_t* graph_id);
+/* Queues a request; returns at once with a ticket. eps = num/den for GA_REQ_PEEL. */
+ga_status ga_server_submit(ga_server* s, uint64_t graph_id, ga_request_kind kind, uint64_t num, uint64_t den,
+                           uint64_t* ticket);
+/* GA_ERR_NOT_READY while the request is pending; otherwise fills *out (out->status is the request's own status). */
+ga_status ga_server_poll(ga_server* s, uint64_t ticket, ga_request_result* out);
+ga_status ga_server_wait(ga_server* s, uint64_t ticket, ga_request_result* out);
+ga_status ga_server_stats_get(ga_server* s, ga_server_stats* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,158 @@
+"""GPU tests of the request loop (ga_server): every request served in a concurrent mix - folded into batch launches,
+run on resident graphs, after evictions - returns exactly what the same request returns alone, and what the oracle
+gives for that graph (triangle count, PeelResult fields (densest.h:46-59), kmax and rounds of CoreLoopResult
+(dsg.h:687-691))."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import random_pairs
+
+pytestmark = pytest.mark.gpu
+
+EPS = [(1, 10), (1, 2)]
+
+
+def _graphs(ga, seed):
+    rng = np.random.default_rng(seed)
+    gs = [ga.build_graph_from_edges(9, np.zeros((0, 2), np.uint32))]                        # no edges
+    iu, iv = np.triu_indices(30, 1)
+    gs.append(ga.build_graph_from_edges(30, np.stack([iu, iv], 1).astype(np.uint32)))     # a clique
+    for _ in range(5):
+        n = int(rng.integers(20, 300))
+        gs.append(ga.build_graph_from_edges(n, ga.canonical_edges(random_pairs(rng, n, 0.1))))
+    hk = ga.gen_holme_kim_batch(24, 64, 6000, 4.0, 20.0, 0.1, 0.7, seed=seed)               # small: folded
+    gs += [hk.graph(i) for i in range(hk.num_graphs)]
+    gs.append(ga.graph_from_pairs(40000, ga.gen_holme_kim(40000, 8, 24, 0.1, 0.7, seed=seed)))  # above the fold size
+    gs.append(ga.graph_from_pairs(1 << 14, ga.gen_rmat(14, 16 << 14, seed=seed)))
+    return gs
+
+
+def _alone(ga, g):
+    """Each request kind on its own device graph, one at a time."""
+    out = {}
+    with ga.DeviceGraph(g) as d:
+        T = d.tc_count()
+        out["tc"] = T
+        for num, den in EPS:
+            r = d.batch_peel(num, den, want_removed=False)
+            out[("peel", num, den)] = (T, r.best_num, r.best_den, r.best_round, r.rounds)
+    with ga.DeviceGraph(g) as d:
+        c = d.core_decomposition(want_core=False)
+        out["core"] = (T, c.kmax, c.rounds)
+        out["bytes"] = d.device_bytes()   # resident with loop state and incidence lists
+    return out
+
+
+def _key(kind, num, den):
+    return "tc" if kind == 0 else ("peel", num, den) if kind == 1 else "core"
+
+
+def _value(ga, kind, r):
+    if kind == ga.REQ_TC:
+        return r.triangles
+    if kind == ga.REQ_PEEL:
+        return (r.triangles, r.peel.best_num, r.peel.best_den, r.peel.best_round, r.peel.rounds)
+    return (r.triangles, r.core[0], r.core[1])
+
+
+def _mix(rng, ngraphs, requery):
+    """Request list: every graph once per kind and eps, plus re-queries of random graphs, shuffled."""
+    reqs = [(i, 0, 1, 1) for i in range(ngraphs)]
+    reqs += [(i, 1, num, den) for i in range(ngraphs) for num, den in EPS]
+    reqs += [(i, 2, 1, 1) for i in range(ngraphs)]
+    extra = [reqs[j] for j in rng.integers(0, len(reqs), int(requery * len(reqs)))]
+    reqs += extra
+    return [reqs[j] for j in rng.permutation(len(reqs))]
+
+
+@pytest.fixture(scope="module")
+def served(ga, cuda_ok):
+    gs = _graphs(ga, 5)
+    alone = [_alone(ga, g) for g in gs]
+    return gs, alone
+
+
+def test_alone_matches_oracle(ga, oracle, served):
+    gs, alone = served
+    for g, a in zip(gs, alone):
+        if g.m > 200000:
+            continue
+        assert a["tc"] == oracle.triangles_serial(g)
+        for num, den in EPS:
+            o = oracle.batch_peel(g, num, den)
+            assert a[("peel", num, den)][1:] == (o.best_num, o.best_den, o.best_round, o.rounds)
+        _, kmax, rounds = oracle.core_levels(g)
+        assert a["core"][1:] == (kmax, rounds)
+
+
+@pytest.mark.parametrize("slots,fold", [(4, 64), (1, 64), (6, 1), (3, 5)])
+def test_mix_equals_alone(ga, served, slots, fold):
+    gs, alone = served
+    rng = np.random.default_rng(slots * 100 + fold)
+    reqs = _mix(rng, len(gs), 0.3)
+    with ga.Server(slots=slots, fold_max_graphs=fold) as s:
+        ids = [s.add_graph(g) for g in gs]
+        tickets = [s.submit(ids[i], kind, num, den) for i, kind, num, den in reqs]
+        for t, (i, kind, num, den) in zip(tickets, reqs):
+            r = s.wait(t)
+            assert r.status == 0, (i, kind)
+            assert _value(ga, kind, r) == alone[i][_key(kind, num, den)], (i, kind, num, den, r.folded)
+        st = s.stats()
+    assert st["submitted"] == st["completed"] == len(reqs)
+    if fold > 1:
+        assert st["folded_launches"] > 0
+    assert st["resident_graphs"] > 0
+
+
+def test_requery_hits_resident_graph(ga, served):
+    gs, alone = served
+    big = len(gs) - 1
+    with ga.Server(slots=2) as s:
+        gid = s.add_graph(gs[big])
+        first = s.wait(s.submit(gid, ga.REQ_TC))
+        again = s.wait(s.submit(gid, ga.REQ_PEEL, 1, 10))
+        core = s.wait(s.submit(gid, ga.REQ_CORE))
+    assert not first.resident_hit and again.resident_hit and core.resident_hit
+    assert first.triangles == alone[big]["tc"]
+    assert _value(ga, ga.REQ_PEEL, again) == alone[big][("peel", 1, 10)]
+    assert _value(ga, ga.REQ_CORE, core) == alone[big]["core"]
+
+
+def test_small_budget_evicts_and_still_matches(ga, served):
+    """Two registrations of the largest graph under a budget that holds one of them with its loop state: requests
+    alternate, graphs are evicted and uploaded again, results stay the same."""
+    gs, alone = served
+    big = len(gs) - 1
+    budget = int(alone[big]["bytes"] * 1.5)
+    rng = np.random.default_rng(9)
+    with ga.Server(slots=2, fold_max_graphs=1, hbm_budget_bytes=budget) as s:
+        ids = [s.add_graph(gs[big]), s.add_graph(gs[big])]
+        reqs = [(c, kind) for _ in range(3) for c in (0, 1) for kind in (0, 1, 2)]
+        reqs = [reqs[j] for j in rng.permutation(len(reqs))]
+        tickets = [s.submit(ids[c], kind, 1, 10) for c, kind in reqs]
+        for t, (c, kind) in zip(tickets, reqs):
+            r = s.wait(t)
+            assert r.status == 0, (c, kind)
+            assert _value(ga, kind, r) == alone[big][_key(kind, 1, 10)]
+        st = s.stats()
+    assert st["peak_reserved_bytes"] <= budget
+    assert st["evictions"] > 0
+
+
+def test_refusals(ga, served):
+    gs, _ = served
+    with ga.Server(hbm_budget_bytes=1 << 16) as s:
+        with pytest.raises(ga.GAError) as e:
+            s.add_graph(gs[-1])                              # can never fit the budget
+        assert e.value.name == "GA_ERR_BUDGET"
+        gid = s.add_graph(gs[0])
+        with pytest.raises(ga.GAError):
+            s.submit(gid + 100, ga.REQ_TC)                   # unknown graph
+        with pytest.raises(ga.GAError):
+            s.submit(gid, ga.REQ_PEEL, 1, 0)                 # eps denominator 0
+        with pytest.raises(ga.GAError):
+            s.wait(12345)                                    # unknown ticket
+        r = s.wait(s.submit(gid, ga.REQ_TC))
+        assert r.status == 0 and r.triangles == 0
