@@ -141,6 +141,17 @@ def dist_setup(args):
     return None, 1, 0, 0
 
 
+def max_over_ranks(dist, x: float, device=None) -> float:
+    """Max of a per-rank time over all ranks (NCCL: a device tensor; gloo: a host tensor); x itself on one rank."""
+    if dist is None:
+        return x
+    import torch
+    on = device if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=on)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def cpu_reference_baseline(g, b_alg: int, steps: int = 1) -> dict:
     """The reference's cpu_triangles_omp (oracle/_ref) with all host threads, full graph, best of `steps`."""
     from oracle import Reference
@@ -161,11 +172,13 @@ def run_reference_arm(args):
     """--impl reference: the reference's own CPU implementation, same metric and config, on rank 0 only."""
     dist, world, rank, _ = dist_setup(args)
     if rank != 0:
+        if dist:
+            dist.destroy_process_group()
         return 0
     import graph_analyzer_b200 as ga
     from oracle import Reference
     ref = Reference()
-    g = make_graph(ga)
+    g = make_graph(ga, args.scale)
     b_alg = algorithmic_bytes(g)
     for _ in range(args.warmup):
         ref.triangles_omp(g)
@@ -181,13 +194,15 @@ def run_reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"rmat{SCALE}_tc", "n": g.n, "m": g.m, "edge_factor": EDGE_FACTOR, "seed": SEED,
+        "config": {"workload": f"rmat{args.scale}_tc", "n": g.n, "m": g.m, "edge_factor": EDGE_FACTOR, "seed": SEED,
                    "triangles": T, "b_alg_bytes": b_alg, "parallelism": "host threads (OpenMP)"},
         "cpu_baseline": {"value": value, "unit": "GB/s", "cores": ref.num_threads(), "kind": "reference",
                          "sample": f"whole graph per step, cpu_triangles_omp (graph.h:123), {args.steps} steps"},
         "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
     return 0
 
 
@@ -197,7 +212,7 @@ def run_ours(args):
     import graph_analyzer_b200 as ga
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    g = make_graph(ga)
+    g = make_graph(ga, args.scale)
     b_alg = algorithmic_bytes(g)
     stream = torch.cuda.Stream(device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
@@ -231,11 +246,7 @@ def run_ours(args):
     step_ms = [a.elapsed_time(b) for a, b in evs]
     if int(d_out.item()) != T:
         raise RuntimeError(f"count changed between launches: {d_out.item()} vs {T}")
-    ms = sum(step_ms) / len(step_ms)
-    if dist:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(dist, sum(step_ms) / len(step_ms), dev)
     value = world * b_alg / (ms / 1e3) / 1e9
 
     # ---- end to end through the public API from pinned host memory ----
@@ -259,11 +270,7 @@ def run_ours(args):
             raise RuntimeError("end-to-end count differs")
         if s >= args.warmup:
             e2e_times.append(dt)
-    e2e_ms = 1e3 * sum(e2e_times) / len(e2e_times)
-    if dist:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(dist, 1e3 * sum(e2e_times) / len(e2e_times), dev)
     e2e_value = world * b_alg / (e2e_ms / 1e3) / 1e9
 
     if rank != 0:
@@ -280,15 +287,15 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"rmat{SCALE}_tc", "n": g.n, "m": g.m, "edge_factor": EDGE_FACTOR, "seed": SEED,
+        "config": {"workload": f"rmat{args.scale}_tc", "n": g.n, "m": g.m, "edge_factor": EDGE_FACTOR, "seed": SEED,
                    "rmat_abc": list(RMAT), "triangles": T, "b_alg_bytes": b_alg, "prep_ms": prep_ms,
-                   "l2": "256 MiB written between steps (untimed); col alone (139 MB) exceeds L2",
+                   "l2": f"256 MiB written between steps (untimed); col alone is {4 * g.m / 1e6:.0f} MB",
                    "parallelism": f"replicas x{world}", "oriented_edges_per_s": world * g.m / (ms / 1e3)},
         "e2e": {"value": e2e_value, "unit": "GB/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(rp_h.numel() * 4 + col_h.numel() * 4), "d2h_bytes_per_step": 8,
                 "path": "ga_graph_create + ga_graph_prepare + ga_tc_count + ga_graph_destroy"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": read_traffic(f"rmat{SCALE}"),
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": read_traffic(f"rmat{args.scale}"),
                      "peak_source": peaks["source"], "kernel": "k_tc_hash<COUNT>"},
         "cpu_baseline": ({k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")} if cpu else None),
         "clocks": clk.summary(),
@@ -595,6 +602,8 @@ def main():
     ap.add_argument("--workload", choices=["rmat22", "hk2", "rmat22-full", "batch", "serve"], default="rmat22",
                     help="rmat22 (default, the headline line) or a secondary workload")
     ap.add_argument("--graphs", type=int, default=4096, help="graphs in the batch workload")
+    ap.add_argument("--scale", type=int, default=SCALE,
+                    help="R-MAT scale of the headline workload (22; smaller only for quick checks)")
     ap.add_argument("--requests", type=int, default=600, help="requests in the serve workload")
     ap.add_argument("--rate-fracs", type=float, nargs="+", default=[0.25, 0.5, 0.75, 0.9],
                     help="serve workload: offered Poisson rates as fractions of the measured burst capacity")

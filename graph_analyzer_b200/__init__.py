@@ -108,6 +108,8 @@ SIGNATURES: dict[str, list] = {
     "ga_status_string": [C.c_int],
     "ga_last_error": [],
     "ga_device_count": [C.POINTER(C.c_int)],
+    "ga_host_pinned_alloc": [C.c_uint64, C.POINTER(_vp)],
+    "ga_host_pinned_free": [_vp],
     "ga_canonical_edges": [_u32p, C.c_uint64, C.POINTER(C.c_uint64)],
     "ga_build_graph_from_edges": [C.c_uint32, _u32p, C.c_uint32, _u32p, _u32p, _u32p, C.POINTER(C.c_uint32)],
     "ga_host_graph_from_edges": [C.c_uint32, _u32p, C.c_uint64, C.c_int, C.POINTER(C.POINTER(_HostGraph))],

@@ -1,8 +1,9 @@
-"""Builds libga_b200.so in-tree (graph_analyzer_b200/_lib/) for sm_100a with nvcc.
+"""Builds libga_b200.so in-tree (graph_analyzer_b200/_lib/) for sm_100a with nvcc, and the command-line drivers.
 
 Every .cu / .cpp under csrc/ is compiled to an object in _build/ (in parallel), then linked into one shared library
 with the CUDA runtime linked statically, so the library does not depend on which libcudart a host process (e.g. torch)
-has loaded. Usage: ``python -m graph_analyzer_b200.build [--force] [--verbose-ptxas]``.
+has loaded. The drivers under cli/ (ga_tc, ga_densest, ga_dsg) are plain C++ over the C ABI, linked against the
+library into graph_analyzer_b200/_bin/. Usage: ``python -m graph_analyzer_b200.build [--force] [--verbose-ptxas]``.
 """
 from __future__ import annotations
 
@@ -17,6 +18,9 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 OUT_DIR = os.path.join(PKG, "_lib")
+BIN_DIR = os.path.join(PKG, "_bin")
+CLI_DIR = os.path.join(PKG, "cli")
+CLIS = ["ga_tc", "ga_densest", "ga_dsg"]
 BUILD_DIR = os.path.join(ROOT, "_build")
 LIB = os.path.join(OUT_DIR, "libga_b200.so")
 INCLUDE = os.path.join(ROOT, "include")
@@ -66,7 +70,26 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
         cmd = [_nvcc(), "-shared", *ARCH, "-o", LIB, *objs, "-cudart", "static", "-Xcompiler", "-fopenmp",
                "-lgomp"]
         subprocess.check_call(cmd)
+    build_cli(force)
     return LIB
+
+
+def build_cli(force: bool = False) -> list[str]:
+    """Compiles the drivers (host C++ only) against the in-tree library; rpath points at ../_lib."""
+    os.makedirs(BIN_DIR, exist_ok=True)
+    deps = [LIB, __file__, os.path.join(CLI_DIR, "cli_common.hpp"), os.path.join(INCLUDE, "graph_analyzer_b200.h"),
+            os.path.join(INCLUDE, "ga", "graph_analyzer.hpp")]
+    out = []
+    for name in CLIS:
+        src = os.path.join(CLI_DIR, name + ".cpp")
+        exe = os.path.join(BIN_DIR, name)
+        out.append(exe)
+        if (not force and os.path.exists(exe)
+                and all(os.path.getmtime(exe) >= os.path.getmtime(d) for d in deps + [src])):
+            continue
+        subprocess.check_call(["g++", "-O2", "-std=c++17", "-Wall", "-I", INCLUDE, "-I", CLI_DIR, src, "-o", exe,
+                               "-L", OUT_DIR, "-lga_b200", "-Wl,-rpath,$ORIGIN/../_lib"])
+    return out
 
 
 if __name__ == "__main__":

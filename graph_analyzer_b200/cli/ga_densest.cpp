@@ -1,0 +1,124 @@
+// ga_densest - triangle-density batch peeling driver over the C ABI; replaces the reference's gpu_densest.cu.
+// usage: ga_densest graph.txt [eps_num eps_den] [--pinned] [--no-burnin] [--repeats N] [--no-greedy] [--verbose]
+//   eps = eps_num/eps_den (default 1/10): a vertex is peeled when its triangle participation is at most (1+eps) times
+//   the average (densest.h:138-160). --no-greedy is accepted for command-line compatibility (the CPU greedy peel is
+//   not part of this library, so there is never a greedy row).
+// Rows (stdout, CSV, the reference's columns, printed only if everything verified):
+//   impl,graph,n,m,best_triangles,best_vertices,density,rounds,time_ms,h2d_ms,total_ms
+//   gpu_batch_peel       the device-resident loop, rounds in a CUDA graph with a conditional node (default)
+//   gpu_batch_peel_host  the same rounds driven from the host, one small read per round (the reference's structure)
+// (suffix "_pinned" with --pinned). time_ms = best of N (default 5) calls of ga_batch_peel after one untimed verified
+// call, host wall clock around the synchronous call: the round-0 count, every round, the final read of the result;
+// EXCLUDES the upload (h2d_ms), the one-time build of the triangle incidence lists (first call) and removed_round's
+// download. Verification: every call of both modes must give the same best_num, best_den, best_round, rounds and the
+// same removed_round array; any difference => MISMATCH on stderr, exit 1, no rows.
+#include "cli_common.hpp"
+
+namespace {
+
+struct Run {
+    ga_peel_result r{};
+    std::vector<uint32_t> removed;
+};
+
+Run peel_once(ga_graph* g, uint32_t n, uint64_t num, uint64_t den, double* ms) {
+    Run run;
+    run.removed.assign(n, UINT32_MAX);
+    const double t0 = cli::now_ms();
+    ga::check(ga_batch_peel(g, num, den, &run.r, run.removed.data()));
+    if (ms) *ms = cli::now_ms() - t0;
+    return run;
+}
+
+bool same(const Run& a, const Run& b) {
+    return a.r.best_num == b.r.best_num && a.r.best_den == b.r.best_den && a.r.best_round == b.r.best_round &&
+           a.r.rounds == b.r.rounds && a.removed == b.removed;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    bool pinned = false, burnin = true, verbose = false;
+    int repeats = 5;
+    std::vector<const char*> pos;
+    for (int i = 1; i < argc; i++) {
+        if (std::strcmp(argv[i], "--pinned") == 0) pinned = true;
+        else if (std::strcmp(argv[i], "--no-burnin") == 0) burnin = false;
+        else if (std::strcmp(argv[i], "--no-greedy") == 0) {}
+        else if (std::strcmp(argv[i], "--verbose") == 0) verbose = true;
+        else if (std::strcmp(argv[i], "--repeats") == 0 && i + 1 < argc) repeats = std::max(1, std::atoi(argv[++i]));
+        else pos.push_back(argv[i]);
+    }
+    if (pos.empty() || pos.size() == 2 || pos.size() > 3) {
+        std::fprintf(stderr, "usage: %s graph.txt [eps_num eps_den] [--pinned] [--no-burnin] [--repeats N] "
+                             "[--no-greedy] [--verbose]\n", argv[0]);
+        return 2;
+    }
+    const char* path = pos[0];
+    const uint64_t num = pos.size() == 3 ? std::strtoull(pos[1], nullptr, 10) : 1;
+    const uint64_t den = pos.size() == 3 ? std::strtoull(pos[2], nullptr, 10) : 10;
+    try {
+        cli::print_device();
+        ga::Graph g;
+        if (!ga::load_graph(path, g)) return 1;
+        std::fprintf(stderr, "loaded n=%u m=%u max_out_deg=%u eps=%llu/%llu\n", g.n, g.m, g.max_out_degree,
+                     (unsigned long long)num, (unsigned long long)den);
+        cli::Upload up(g, pinned);
+        uint64_t T = 0;
+        ga::check(ga_tc_count(up.g, &T));
+        std::string why;
+        if (!ga::peel_arith_ok(g.n, T, num, den, &why)) {   // the reference's refusal (densest.h:65-78)
+            std::fprintf(stderr, "batch peel refused: %s\n", why.c_str());
+            return 1;
+        }
+        if (burnin) cli::burn_in(up.g);
+        struct Mode { const char* name; int64_t loop; };
+        const Mode modes[] = {{"gpu_batch_peel", 2}, {"gpu_batch_peel_host", 1}};
+        std::vector<std::string> rows;
+        bool ok = true;
+        Run first;
+        bool have = false;
+        for (const Mode& md : modes) {
+            ga::check(ga_graph_set_option(up.g, GA_OPT_LOOP_MODE, md.loop));
+            Run last = peel_once(up.g, g.n, num, den, nullptr);   // untimed warm-up + verification
+            if (!have) { first = last; have = true; }
+            double best = 1e300;
+            for (int i = 0; i < repeats && ok; i++) {
+                double ms = 0;
+                last = peel_once(up.g, g.n, num, den, &ms);
+                best = std::min(best, ms);
+                if (!same(last, first)) {
+                    std::fprintf(stderr, "MISMATCH in %s: best %llu/%llu round %u rounds %u vs %llu/%llu round %u "
+                                 "rounds %u\n", md.name, (unsigned long long)last.r.best_num,
+                                 (unsigned long long)last.r.best_den, last.r.best_round, last.r.rounds,
+                                 (unsigned long long)first.r.best_num, (unsigned long long)first.r.best_den,
+                                 first.r.best_round, first.r.rounds);
+                    ok = false;
+                }
+            }
+            if (verbose)
+                std::fprintf(stderr, "%s: best %llu/%llu at round %u of %u, best of %d: %.3f ms\n", md.name,
+                             (unsigned long long)last.r.best_num, (unsigned long long)last.r.best_den,
+                             last.r.best_round, last.r.rounds, repeats, best);
+            const std::string name = std::string(md.name) + (pinned ? "_pinned" : "");
+            char buf[1024];
+            std::snprintf(buf, sizeof buf, "%s,%s,%u,%u,%llu,%llu,%.6f,%u,%.3f,%.3f,%.3f", name.c_str(), path, g.n,
+                          g.m, (unsigned long long)last.r.best_num, (unsigned long long)last.r.best_den,
+                          ga::density_value(last.r.best_num, last.r.best_den), last.r.rounds, best, up.h2d_ms,
+                          best + up.h2d_ms);
+            rows.push_back(buf);
+        }
+        if (!ok) {
+            std::fprintf(stderr, "VERIFICATION FAILED - no timing rows printed\n");
+            return 1;
+        }
+        for (auto& r : rows) std::puts(r.c_str());
+        std::fflush(stdout);
+        std::fprintf(stderr, "both loop modes agree bit-exactly (best %llu triangles / %llu vertices, %u rounds)\n",
+                     (unsigned long long)first.r.best_num, (unsigned long long)first.r.best_den, first.r.rounds);
+    } catch (const ga::Error& e) {
+        std::fprintf(stderr, "%s\n", e.what());
+        return 1;
+    }
+    return 0;
+}

@@ -1,0 +1,119 @@
+// ga_dsg - (k, triangle)-core decomposition driver over the C ABI; replaces the GPU stage of the reference's
+// gpu_dsg.cu (its level-synchronous core decomposition, dsg.h:724-751).
+// usage: ga_dsg graph.txt [--repeats N] [--pinned] [--no-burnin] [--no-exact] [--no-greedy] [--no-greedypp] [--T N]
+//   Only the core decomposition runs here: the reference's CPU stages (greedy lower bound, pruning, CoreExact,
+//   Greedy++) are not part of this library, so --no-exact / --no-greedy / --no-greedypp / --T are accepted for
+//   command-line compatibility and change nothing (the output equals the reference's with all of them off).
+// Rows (stdout, CSV, the reference's dsg_row columns, printed only if everything verified):
+//   impl,graph,n,m,triangles,vertices,density,time_ms,h2d_ms,total_ms,rounds,kmax
+//   gpu_core_decomp       device-resident rounds in a CUDA graph with a conditional node (default)
+//   gpu_core_decomp_host  the same rounds driven from the host, one small read per round
+// (suffix "_pinned" with --pinned). The row describes the kmax-core (its triangle count and vertex count, as
+// core_level_density, dsg.h:169-174, reports it). time_ms = best of N (default 5) calls of ga_core_decomposition after
+// one untimed verified call (which also builds the triangle incidence lists), host wall clock around the synchronous
+// call; EXCLUDES the upload (h2d_ms) and core[]'s download. Verification: every call of both modes must give the same
+// core numbers (element-wise), kmax and rounds; otherwise MISMATCH on stderr, exit 1, no rows.
+#include "cli_common.hpp"
+
+namespace {
+
+struct Run {
+    ga_core_result r{};
+    std::vector<uint32_t> core;
+};
+
+Run cores_once(ga_graph* g, uint32_t n, double* ms) {
+    Run run;
+    run.core.assign(n, 0);
+    const double t0 = cli::now_ms();
+    ga::check(ga_core_decomposition(g, run.core.data(), &run.r));
+    if (ms) *ms = cli::now_ms() - t0;
+    return run;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    bool pinned = false, burnin = true;
+    int repeats = 5;
+    std::vector<const char*> pos;
+    for (int i = 1; i < argc; i++) {
+        if (std::strcmp(argv[i], "--pinned") == 0) pinned = true;
+        else if (std::strcmp(argv[i], "--no-burnin") == 0) burnin = false;
+        else if (!std::strcmp(argv[i], "--no-exact") || !std::strcmp(argv[i], "--no-greedy") ||
+                 !std::strcmp(argv[i], "--no-greedypp")) {}
+        else if (std::strcmp(argv[i], "--T") == 0 && i + 1 < argc) ++i;
+        else if (std::strcmp(argv[i], "--repeats") == 0 && i + 1 < argc) repeats = std::max(1, std::atoi(argv[++i]));
+        else pos.push_back(argv[i]);
+    }
+    if (pos.size() != 1) {
+        std::fprintf(stderr, "usage: %s graph.txt [--repeats N] [--pinned] [--no-burnin] [--no-exact] [--no-greedy] "
+                             "[--no-greedypp] [--T N]\n", argv[0]);
+        return 2;
+    }
+    const char* path = pos[0];
+    try {
+        cli::print_device();
+        ga::Graph g;
+        if (!ga::load_graph(path, g)) return 1;
+        std::fprintf(stderr, "loaded n=%u m=%u max_out_deg=%u\n", g.n, g.m, g.max_out_degree);
+        cli::Upload up(g, pinned);
+        if (burnin) cli::burn_in(up.g);
+        struct Mode { const char* name; int64_t loop; };
+        const Mode modes[] = {{"gpu_core_decomp", 2}, {"gpu_core_decomp_host", 1}};
+        std::vector<std::string> rows;
+        bool ok = true, have = false;
+        Run first;
+        uint64_t kcore_tri = 0, kcore_verts = 0;
+        for (const Mode& md : modes) {
+            ga::check(ga_graph_set_option(up.g, GA_OPT_LOOP_MODE, md.loop));
+            Run last = cores_once(up.g, g.n, nullptr);
+            if (!have) {
+                first = last;
+                have = true;
+                // the kmax-core: triangles of the subgraph induced by {v : core[v] >= kmax} (dsg.h:169-174)
+                std::vector<uint8_t> in(g.n);
+                for (uint32_t v = 0; v < g.n; v++) {
+                    in[v] = first.core[v] >= first.r.kmax;
+                    kcore_verts += in[v];
+                }
+                std::vector<uint32_t> tri(g.n);
+                ga::check(ga_tc_participation(up.g, in.data(), tri.data(), &kcore_tri));
+            }
+            double best = 1e300;
+            for (int i = -1; i < repeats && ok; i++) {
+                double ms = 0;
+                if (i >= 0) {
+                    last = cores_once(up.g, g.n, &ms);
+                    best = std::min(best, ms);
+                }
+                if (last.r.kmax != first.r.kmax || last.r.rounds != first.r.rounds || last.core != first.core) {
+                    size_t v = 0;
+                    while (v < g.n && last.core[v] == first.core[v]) v++;
+                    std::fprintf(stderr, "MISMATCH in %s: kmax %u vs %u, rounds %u vs %u, first differing vertex %zu\n",
+                                 md.name, last.r.kmax, first.r.kmax, last.r.rounds, first.r.rounds, v);
+                    ok = false;
+                }
+            }
+            const std::string name = std::string(md.name) + (pinned ? "_pinned" : "");
+            char buf[1024];
+            std::snprintf(buf, sizeof buf, "%s,%s,%u,%u,%llu,%llu,%.6f,%.3f,%.3f,%.3f,%llu,%llu", name.c_str(), path,
+                          g.n, g.m, (unsigned long long)kcore_tri, (unsigned long long)kcore_verts,
+                          ga::density_value(kcore_tri, kcore_verts), best, up.h2d_ms, best + up.h2d_ms,
+                          (unsigned long long)last.r.rounds, (unsigned long long)last.r.kmax);
+            rows.push_back(buf);
+        }
+        if (!ok) {
+            std::fprintf(stderr, "VERIFICATION FAILED - no timing rows printed\n");
+            return 1;
+        }
+        for (auto& r : rows) std::puts(r.c_str());
+        std::fflush(stdout);
+        std::fprintf(stderr, "both loop modes agree element-wise (kmax %u, %u rounds)\n", first.r.kmax,
+                     first.r.rounds);
+    } catch (const ga::Error& e) {
+        std::fprintf(stderr, "%s\n", e.what());
+        return 1;
+    }
+    return 0;
+}

@@ -453,6 +453,25 @@ ga_status ga_device_count(int* count) {
     return GA_OK;
 }
 
+ga_status ga_host_pinned_alloc(uint64_t bytes, void** out) {
+    if (!out) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (cudaMallocHost(out, bytes ? bytes : 1) != cudaSuccess) {
+        (void)cudaGetLastError();
+        *out = nullptr;
+        return fail(GA_ERR_OUT_OF_MEMORY, "page-locked allocation of %llu bytes failed", (unsigned long long)bytes);
+    }
+    return GA_OK;
+}
+
+ga_status ga_host_pinned_free(void* p) {
+    if (p && cudaFreeHost(p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return fail(GA_ERR_CUDA, "cudaFreeHost failed");
+    }
+    return GA_OK;
+}
+
 ga_status ga_graph_create(const uint32_t* rowptr, const uint32_t* col, uint32_t n, uint32_t m, int device,
                           void* stream, ga_graph** out) {
     return create_common(rowptr, col, n, m, device, stream, false, out);

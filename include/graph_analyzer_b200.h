@@ -54,6 +54,10 @@ const char* ga_status_string(ga_status s);
 const char* ga_last_error(void);
 /* Number of CUDA devices visible (0 without a GPU). */
 ga_status ga_device_count(int* count);
+/* Page-locked host memory for staging uploads (the --pinned staging of the reference's drivers, cudaMallocHost in
+ * gpu_tc.cu:43-62): copies from it to the device run at full link speed and asynchronously. */
+ga_status ga_host_pinned_alloc(uint64_t bytes, void** out);
+ga_status ga_host_pinned_free(void* p);
 
 /* ---------------------------------------------------------------------------------------------------------------
  * Host-side graph construction: the reference's Graph / load_graph / build_graph_from_edges (graph.h:19-96).
