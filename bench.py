@@ -497,10 +497,10 @@ def _serve_value(ga, kind, r):
     return r.core
 
 
-def _serve_run(ga, graphs, trace, arrivals_s):
+def _serve_run(ga, graphs, trace, arrivals_s, slots=0):
     """Submits the trace at the given arrival times (open loop) to a fresh server; returns per-request latency (ms,
     submit to completion), results, wall time of the run and the server statistics."""
-    with ga.Server() as s:
+    with ga.Server(slots=slots) as s:
         ids = [s.add_graph(g) for g in graphs]
         tickets = []
         t0 = time.perf_counter()
@@ -559,8 +559,18 @@ def run_serve(args):
         plain_vals.append(val)
     serial_s = float(sum(service))
     # closed-loop burst (all requests at t = 0): the server's capacity; also warms the kernel-choice cache
-    lat, res, wall, st = _serve_run(ga, graphs, trace, np.zeros(R))
+    lat, res, wall, st = _serve_run(ga, graphs, trace, np.zeros(R), args.slots)
     capacity = R / wall
+    # where the time goes, per request class (graph family x kind): serial service vs the server's run time
+    names = ("tc", "peel", "core")
+    by_class = {}
+    for (gi, kind), sv, r in zip(trace, service, res):
+        c = ("rmat_" if graphs[gi].n > (1 << 19) else "hk_") + names[kind]
+        e = by_class.setdefault(c, {"count": 0, "serial_ms": 0.0, "server_run_ms": 0.0})
+        e["count"] += 1
+        e["serial_ms"] += sv * 1e3
+        e["server_run_ms"] += r.run_ms
+    log("per class: " + json.dumps(by_class))
     identical = all(_serve_value(ga, k, r) == v and r.status == 0 for (_, k), r, v in zip(trace, res, plain_vals))
     burst = {"req_s": capacity, "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
              "folded_launches": st["folded_launches"], "evictions": st["evictions"],
@@ -570,7 +580,7 @@ def run_serve(args):
         rate = frac * capacity
         arr = np.cumsum(rng.exponential(1.0 / rate, R))
         arr -= arr[0]
-        lat, res, wall, st = _serve_run(ga, graphs, trace, arr)
+        lat, res, wall, st = _serve_run(ga, graphs, trace, arr, args.slots)
         identical &= all(_serve_value(ga, k, r) == v and r.status == 0
                          for (_, k), r, v in zip(trace, res, plain_vals))
         slat = _fifo_latency(service, arr)
@@ -587,7 +597,8 @@ def run_serve(args):
             "value": capacity, "unit": "req/s", "higher_is_better": True, "serial_plain_req_s": R / serial_s,
             "speedup_vs_serial_plain": capacity / (R / serial_s), "requests": R, "graphs": len(graphs),
             "mix": {"tc": int(kinds[0]), "peel_eps_1_10": int(kinds[1]), "cores": int(kinds[2])},
-            "hbm_budget_gb": 150, "slots": 4, "burst": burst, "sweep": sweep, "bit_identical": bool(identical)}
+            "hbm_budget_gb": 150, "slots": args.slots or 4, "burst": burst, "sweep": sweep, "by_class": by_class,
+            "bit_identical": bool(identical)}
     print(json.dumps(line), flush=True)
     return 0 if identical else 1
 
@@ -605,6 +616,7 @@ def main():
     ap.add_argument("--scale", type=int, default=SCALE,
                     help="R-MAT scale of the headline workload (22; smaller only for quick checks)")
     ap.add_argument("--requests", type=int, default=600, help="requests in the serve workload")
+    ap.add_argument("--slots", type=int, default=0, help="serve workload: concurrent requests (0 = the default 4)")
     ap.add_argument("--rate-fracs", type=float, nargs="+", default=[0.25, 0.5, 0.75, 0.9],
                     help="serve workload: offered Poisson rates as fractions of the measured burst capacity")
     args = ap.parse_args()

@@ -83,7 +83,8 @@ class _CoreRes(C.Structure):
 
 class _ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int), ("hbm_budget_bytes", C.c_uint64), ("slots", C.c_uint32),
-                ("fold_max_graphs", C.c_uint32), ("fold_max_edges", C.c_uint32)]
+                ("fold_max_graphs", C.c_uint32), ("fold_max_edges", C.c_uint32), ("small_slots", C.c_uint32),
+                ("pin_min_edges", C.c_uint32)]
 
 
 class _RequestResult(C.Structure):
@@ -642,8 +643,9 @@ class Server:
     run concurrently on `slots` streams; small count/peel requests queued together share one batch launch."""
 
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, slots: int = 0, fold_max_graphs: int = 0,
-                 fold_max_edges: int = 0):
-        cfg = _ServerConfig(device, hbm_budget_bytes, slots, fold_max_graphs, fold_max_edges)
+                 fold_max_edges: int = 0, small_slots: int = 0, pin_min_edges: int = 0):
+        cfg = _ServerConfig(device, hbm_budget_bytes, slots, fold_max_graphs, fold_max_edges, small_slots,
+                            pin_min_edges)
         h = _vp()
         _check(lib().ga_server_create(C.byref(cfg), C.byref(h)))
         self._h = h

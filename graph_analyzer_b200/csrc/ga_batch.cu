@@ -83,7 +83,7 @@ ga_status ga_batch_create(uint32_t num_graphs, const uint64_t* vtx_off, const ui
     uint32_t *d_lrow = nullptr, *d_lcol = nullptr, *d_grow = nullptr, *d_gcol = nullptr;
     ga_status s = GA_OK;
     auto tmp = [&](void** p, size_t bytes) {
-        if (s == GA_OK && cudaMallocAsync(p, bytes ? bytes : 1, st) != cudaSuccess) {
+        if (s == GA_OK && pool_malloc(p, bytes ? bytes : 1, st) != cudaSuccess) {
             (void)cudaGetLastError();
             s = fail(GA_ERR_OUT_OF_MEMORY, "batch staging allocation of %zu bytes failed", bytes);
         }

@@ -123,16 +123,26 @@ struct ga_graph {
 
 namespace ga {
 
-// Configures the device's default memory pool once per process and device: freed blocks stay cached (up to
-// 8 GiB) so that graphs created and destroyed repeatedly reuse memory instead of returning it to the driver.
+// Creates the library's own memory pool of a device once per process: freed blocks stay cached (up to 8 GiB) so
+// that graphs created and destroyed repeatedly reuse memory instead of returning it to the driver. A pool of its own
+// leaves the device's default pool (which other code in the process may use) as it was.
 ga_status init_pool(int device);
+
+// The pool of the current device (init_pool must have run for it; every entry point that allocates calls it).
+cudaMemPool_t pool_of_current();
+
+// Stream-ordered allocation from the library's pool of the current device.
+template <class T>
+inline cudaError_t pool_malloc(T** p, size_t bytes, cudaStream_t st) {
+    return cudaMallocFromPoolAsync((void**)p, bytes, pool_of_current(), st);
+}
 
 // Device allocation owned by g (stream-ordered from the pool on g's stream, freed at destroy), counted in g->bytes.
 template <class T>
 inline ga_status dalloc(ga_graph* g, T** p, size_t count) {
     void* q = nullptr;
     const size_t bytes = (count ? count : 1) * sizeof(T);
-    cudaError_t e = cudaMallocAsync(&q, bytes, g->stream);
+    cudaError_t e = pool_malloc(&q, bytes, g->stream);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
         return fail(GA_ERR_OUT_OF_MEMORY, "cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));

@@ -91,7 +91,7 @@ static ga_status scan_impl(cudaStream_t st, const T* in, T* out, uint64_t n, boo
         return GA_OK;
     }
     T* sums = nullptr;
-    GA_CUDA(cudaMallocAsync((void**)&sums, nb * sizeof(T), st));
+    GA_CUDA(pool_malloc((void**)&sums, nb * sizeof(T), st));
     k_tile_reduce<T><<<(unsigned)nb, kScanThreads, 0, st>>>(in, n, sums);
     ga_status s = GA_OK;
     if (cudaGetLastError() != cudaSuccess) s = fail(GA_ERR_CUDA, "scan reduce launch failed");
@@ -255,17 +255,30 @@ ga_status use_device(const ga_graph* g) {
     return GA_OK;
 }
 
+static std::mutex g_pool_mu;
+static cudaMemPool_t g_pools[64] = {};
+
 ga_status init_pool(int device) {
-    static std::mutex mu;
-    static bool done[64] = {};
-    std::lock_guard<std::mutex> lock(mu);
-    if (device < 64 && done[device]) return GA_OK;
+    if (device < 0 || device >= 64) return fail(GA_ERR_INVALID_ARGUMENT, "device %d out of range", device);
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (g_pools[device]) return GA_OK;
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
     cudaMemPool_t pool;
-    GA_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    GA_CUDA(cudaMemPoolCreate(&pool, &props));
     uint64_t keep = 8ull << 30;
     GA_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
-    if (device < 64) done[device] = true;
+    g_pools[device] = pool;
     return GA_OK;
+}
+
+cudaMemPool_t pool_of_current() {
+    int device = 0;
+    cudaGetDevice(&device);
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    return device >= 0 && device < 64 ? g_pools[device] : nullptr;
 }
 
 static ga_status build_items(ga_graph* g, const unsigned long long* prefix, uint32_t* cnt_l, uint32_t* cnt_h,
@@ -322,8 +335,8 @@ ga_status prepare(ga_graph* g) {
     GA_TRY(dalloc(g, &g->in_src, m));
     GA_TRY(dalloc(g, &g->in_eid, m));
     uint32_t *indeg = nullptr, *fill = nullptr;
-    GA_CUDA(cudaMallocAsync((void**)&indeg, ((size_t)n + 1) * 4, st));
-    GA_CUDA(cudaMallocAsync((void**)&fill, ((size_t)n + 1) * 4, st));
+    GA_CUDA(pool_malloc((void**)&indeg, ((size_t)n + 1) * 4, st));
+    GA_CUDA(pool_malloc((void**)&fill, ((size_t)n + 1) * 4, st));
     unsigned long long* err = g->d_scalars + 63;
     GA_CUDA(cudaMemsetAsync(err, 0, 8, st));
     GA_CUDA(cudaMemsetAsync(indeg, 0, ((size_t)n + 1) * 4, st));
@@ -340,17 +353,17 @@ ga_status prepare(ga_graph* g) {
     }
     // work prefix over in-edges (64-bit: the total probe count can exceed 2^32)
     unsigned long long* prefix = nullptr;
-    GA_CUDA(cudaMallocAsync((void**)&prefix, ((size_t)m + 1) * 8, st));
+    GA_CUDA(pool_malloc((void**)&prefix, ((size_t)m + 1) * 8, st));
     if (m) {
         k_in_work<<<ge, 256, 0, st>>>(g->rowptr, g->in_src, m, prefix);
         GA_CUDA(cudaGetLastError());
         GA_TRY(scan_impl<unsigned long long>(st, prefix, prefix, m, true));
     }
     uint32_t *cnt_l = nullptr, *cnt_h = nullptr, *off_l = nullptr, *off_h = nullptr;
-    GA_CUDA(cudaMallocAsync((void**)&cnt_l, ((size_t)n + 1) * 4, st));
-    GA_CUDA(cudaMallocAsync((void**)&cnt_h, ((size_t)n + 1) * 4, st));
-    GA_CUDA(cudaMallocAsync((void**)&off_l, ((size_t)n + 1) * 4, st));
-    GA_CUDA(cudaMallocAsync((void**)&off_h, ((size_t)n + 1) * 4, st));
+    GA_CUDA(pool_malloc((void**)&cnt_l, ((size_t)n + 1) * 4, st));
+    GA_CUDA(pool_malloc((void**)&cnt_h, ((size_t)n + 1) * 4, st));
+    GA_CUDA(pool_malloc((void**)&off_l, ((size_t)n + 1) * 4, st));
+    GA_CUDA(pool_malloc((void**)&off_h, ((size_t)n + 1) * 4, st));
     ga_status s = GA_OK;
     if (n) s = build_items(g, prefix, cnt_l, cnt_h, off_l, off_h, (unsigned*)(g->d_scalars + 62));
     cudaFreeAsync(prefix, st);

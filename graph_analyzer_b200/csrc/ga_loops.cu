@@ -667,7 +667,7 @@ static ga_status build_lists(ga_graph* g, uint64_t T0) {
         if (s == GA_OK) s = dalloc(g, &ic, need_items);
     }
     uint32_t* fill = nullptr;   // n cursors + the overflow counter
-    if (s == GA_OK && cudaMallocAsync((void**)&fill, ((size_t)n + 1) * 4, st) != cudaSuccess) {
+    if (s == GA_OK && pool_malloc((void**)&fill, ((size_t)n + 1) * 4, st) != cudaSuccess) {
         (void)cudaGetLastError();
         s = fail(GA_ERR_OUT_OF_MEMORY, "incidence list cursors do not fit");
     }

@@ -6,11 +6,15 @@
 // resident graphs least-recently-used first; requests on the same graph run one at a time. A worker that takes a
 // count or peeling request on a small graph that is not resident also takes the other queued small requests of the
 // same kind and eps (up to fold_max_graphs) and serves them with one batch launch (ga_batch_*): requests arriving
-// while others are on the GPU are folded into the next launch instead of waiting for a launch each. Every request's
-// result is exactly the result of running it alone (the batch path is bit-identical to the single-graph path).
+// while others are on the GPU are folded into the next launch instead of waiting for a launch each. `small_slots`
+// further workers take only cheap requests (small graphs, counts on resident graphs), so those are not held up by the
+// uploads and loops of large graphs. Large graphs keep a page-locked host copy, so their uploads (first request, and
+// after an eviction) run at link speed. Every request's result is exactly the result of running it alone (the batch
+// path is bit-identical to the single-graph path).
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstring>
 #include <deque>
 #include <map>
 #include <mutex>
@@ -32,7 +36,11 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
 
 struct GraphEntry {
     uint32_t n = 0, m = 0;
-    std::vector<uint32_t> rowptr, col;   // host copy (re-uploaded after an eviction)
+    // host copy, re-uploaded after an eviction: page-locked for large graphs (uploads at link speed), else pageable
+    std::vector<uint32_t> rowptr_v, col_v;
+    uint32_t* pinned = nullptr;          // rowptr (n+1) then col (m), freed by ga_server_destroy
+    const uint32_t* rowptr() const { return pinned ? pinned : rowptr_v.data(); }
+    const uint32_t* col() const { return pinned ? pinned + n + 1 : col_v.data(); }
     ga_graph* dev = nullptr;             // resident device graph
     uint64_t dev_bytes = 0;              // its device bytes (accounted in `reserved`)
     uint64_t triangles = UINT64_MAX;     // known after the first request (sizes the incidence lists)
@@ -107,12 +115,18 @@ struct Work {
     uint64_t reserve = 0;
 };
 
-// Picks the next admissible work (caller holds the lock). Returns false when nothing can start now.
-bool take_work(ga_server* s, Work* w) {
+// A request that never occupies the device for long: any request on a small graph, or a count on a resident one.
+bool cheap(const ga_server* s, const Request& r, const GraphEntry& e) {
+    return e.m <= s->cfg.fold_max_edges || (e.dev && r.kind == GA_REQ_TC);
+}
+
+// Picks the next admissible work (caller holds the lock). Returns false when nothing can start now. Workers of the
+// small lane (`small_only`) take cheap requests only, so those never wait behind uploads and loops of large graphs.
+bool take_work(ga_server* s, Work* w, bool small_only) {
     for (auto it = s->queue.begin(); it != s->queue.end(); ++it) {
         Request& r = s->requests[*it];
         GraphEntry& e = s->graphs[r.gid];
-        if (e.busy) continue;
+        if (e.busy || (small_only && !cheap(s, r, e))) continue;
         const bool small = r.kind != GA_REQ_CORE && !e.dev && e.m <= s->cfg.fold_max_edges &&
                            s->cfg.fold_max_graphs > 1;
         // A loop on a large graph whose triangle count is unknown is admitted in two stages: first the upload and
@@ -133,7 +147,7 @@ bool take_work(ga_server* s, Work* w) {
             s->stats.completed++;
             s->queue.erase(it);
             s->cv_done.notify_all();
-            return take_work(s, w);
+            return take_work(s, w, small_only);
         }
         if (s->reserved + need > s->cfg.hbm_budget_bytes && !make_room(s, need)) continue;
         w->tickets.assign(1, *it);
@@ -187,7 +201,7 @@ bool run_single(ga_server* s, cudaStream_t st, Work* w, Request& r, GraphEntry& 
     res.resident_hit = e.dev != nullptr;
     ga_status rc = GA_OK;
     if (!e.dev) {
-        rc = ga_graph_create(e.rowptr.data(), e.m ? e.col.data() : nullptr, e.n, e.m, s->cfg.device, st, &e.dev);
+        rc = ga_graph_create(e.rowptr(), e.m ? e.col() : nullptr, e.n, e.m, s->cfg.device, st, &e.dev);
         if (rc != GA_OK) e.dev = nullptr;
     } else {
         rc = ga_graph_set_stream(e.dev, st);
@@ -234,8 +248,8 @@ void run_folded(ga_server* s, cudaStream_t st, std::vector<Request*>& rs, std::v
     }
     std::vector<uint32_t> rowptr(voff[G] + G), col(eoff[G] + 1);
     for (uint32_t i = 0; i < G; i++) {
-        std::copy(es[i]->rowptr.begin(), es[i]->rowptr.end(), rowptr.begin() + voff[i] + i);
-        std::copy(es[i]->col.begin(), es[i]->col.end(), col.begin() + eoff[i]);
+        std::copy(es[i]->rowptr(), es[i]->rowptr() + es[i]->n + 1, rowptr.begin() + voff[i] + i);
+        std::copy(es[i]->col(), es[i]->col() + es[i]->m, col.begin() + eoff[i]);
     }
     std::vector<uint64_t> tri(G, 0);
     std::vector<ga_peel_result> peel(G);
@@ -258,7 +272,7 @@ void run_folded(ga_server* s, cudaStream_t st, std::vector<Request*>& rs, std::v
     }
 }
 
-void worker_main(ga_server* s) {
+void worker_main(ga_server* s, bool small_only) {
     cudaSetDevice(s->cfg.device);
     cudaStream_t st;
     if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return;
@@ -266,7 +280,7 @@ void worker_main(ga_server* s) {
         Work w;
         {
             std::unique_lock<std::mutex> lock(s->mu);
-            s->cv_work.wait(lock, [&] { return s->stop || take_work(s, &w); });
+            s->cv_work.wait(lock, [&] { return s->stop || take_work(s, &w, small_only); });
             if (w.tickets.empty()) break;   // stop requested and nothing admissible
             s->running++;
         }
@@ -351,7 +365,11 @@ ga_status ga_server_create(const ga_server_config* config, ga_server** out) {
     if (!s->cfg.slots) s->cfg.slots = 4;
     if (!s->cfg.fold_max_graphs) s->cfg.fold_max_graphs = 64;
     if (!s->cfg.fold_max_edges) s->cfg.fold_max_edges = 65536;
-    for (uint32_t i = 0; i < s->cfg.slots; i++) s->workers.emplace_back(worker_main, s);
+    if (!s->cfg.small_slots) s->cfg.small_slots = 2;
+    if (s->cfg.small_slots == UINT32_MAX) s->cfg.small_slots = 0;
+    if (!s->cfg.pin_min_edges) s->cfg.pin_min_edges = 1u << 20;
+    for (uint32_t i = 0; i < s->cfg.slots; i++) s->workers.emplace_back(worker_main, s, false);
+    for (uint32_t i = 0; i < s->cfg.small_slots; i++) s->workers.emplace_back(worker_main, s, true);
     *out = s;
     return GA_OK;
 }
@@ -372,6 +390,8 @@ ga_status ga_server_destroy(ga_server* s) {
     }
     s->cv_work.notify_all();
     for (auto& t : s->workers) t.join();
+    for (auto& kv : s->graphs)
+        if (kv.second.pinned) cudaFreeHost(kv.second.pinned);
     delete s;
     return GA_OK;
 }
@@ -383,14 +403,24 @@ ga_status ga_server_add_graph(ga_server* s, const uint32_t* rowptr, const uint32
     GraphEntry e;
     e.n = n;
     e.m = m;
-    e.rowptr.assign(rowptr, rowptr + n + 1);
-    e.col.assign(col, col + m);
+    if (m >= s->cfg.pin_min_edges &&
+        cudaMallocHost((void**)&e.pinned, 4 * ((uint64_t)n + 1 + m)) == cudaSuccess) {
+        std::memcpy(e.pinned, rowptr, 4 * ((uint64_t)n + 1));
+        if (m) std::memcpy(e.pinned + n + 1, col, 4 * (uint64_t)m);
+    } else {
+        (void)cudaGetLastError();
+        e.pinned = nullptr;   // page-locked memory exhausted: keep a pageable copy
+        e.rowptr_v.assign(rowptr, rowptr + n + 1);
+        e.col_v.assign(col, col + m);
+    }
     for (uint32_t v = 0; v < n; v++) {
         const uint64_t d = rowptr[v + 1] - rowptr[v];
         e.tri_bound += d * (d - 1) / 2;
     }
-    if (estimate_bytes(e, GA_REQ_TC) > s->cfg.hbm_budget_bytes)
+    if (estimate_bytes(e, GA_REQ_TC) > s->cfg.hbm_budget_bytes) {
+        if (e.pinned) cudaFreeHost(e.pinned);
         return fail(GA_ERR_BUDGET, "graph needs more than the HBM budget");
+    }
     std::lock_guard<std::mutex> lock(s->mu);
     *graph_id = s->next_gid++;
     s->graphs.emplace(*graph_id, std::move(e));

@@ -518,7 +518,7 @@ ga_status autotune(ga_graph* g) {
     if (g->m == 0) { g->tuned_kernel = 2; return GA_OK; }
     // signature
     unsigned long long* d_hist = nullptr;
-    GA_CUDA(cudaMallocAsync((void**)&d_hist, 33 * 8, st));
+    GA_CUDA(pool_malloc((void**)&d_hist, 33 * 8, st));
     unsigned long long hist[33] = {};
     cudaMemsetAsync(d_hist, 0, 33 * 8, st);
     k_degree_hist<<<grid_for(n, 256, (unsigned)g->sm_count * 8), 256, 0, st>>>(g->rowptr, n, d_hist);
@@ -635,7 +635,7 @@ ga_status ga_tc_support_edges(ga_graph* g, uint32_t* sup, uint64_t* triangles) {
     GA_TRY(use_device(g));
     Scratch s;
     s.st = g->stream;
-    GA_CUDA(cudaMallocAsync(&s.p, ((size_t)g->m + 1) * 4, g->stream));
+    GA_CUDA(pool_malloc(&s.p, ((size_t)g->m + 1) * 4, g->stream));
     GA_TRY(ga_tc_support_edges_device(g, (uint32_t*)s.p, triangles));
     if (g->m) GA_CUDA(cudaMemcpyAsync(sup, s.p, (size_t)g->m * 4, cudaMemcpyDeviceToHost, g->stream));
     GA_CUDA(cudaStreamSynchronize(g->stream));
@@ -648,7 +648,7 @@ ga_status ga_tc_support_vertices(ga_graph* g, uint64_t* deg, uint64_t* triangles
     GA_TRY(ready(g));
     Scratch s;
     s.st = g->stream;
-    GA_CUDA(cudaMallocAsync(&s.p, ((size_t)g->n + 1) * 8, g->stream));
+    GA_CUDA(pool_malloc(&s.p, ((size_t)g->n + 1) * 8, g->stream));
     TcArgs<unsigned long long> a{};
     a.total = g->d_scalars;
     a.vsup = (unsigned long long*)s.p;
@@ -667,7 +667,7 @@ ga_status ga_tc_participation(ga_graph* g, const uint8_t* alive, uint32_t* tri, 
         return fail(GA_ERR_ARITH, "triangle count >= 2^32: uint32 tri[] counters could overflow");
     Scratch s;
     s.st = g->stream;
-    GA_CUDA(cudaMallocAsync(&s.p, ((size_t)g->n + 1) * 5, g->stream));
+    GA_CUDA(pool_malloc(&s.p, ((size_t)g->n + 1) * 5, g->stream));
     uint32_t* d_tri = (uint32_t*)s.p;
     uint8_t* d_alive = (uint8_t*)(d_tri + g->n + 1);
     if (g->n) GA_CUDA(cudaMemcpyAsync(d_alive, alive, g->n, cudaMemcpyHostToDevice, g->stream));

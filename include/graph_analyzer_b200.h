@@ -271,6 +271,11 @@ typedef struct ga_server_config {
     uint32_t slots;              /* concurrent requests (0 = 4)                                                  */
     uint32_t fold_max_graphs;    /* small requests folded into one batch launch (0 = 64; 1 disables folding)     */
     uint32_t fold_max_edges;     /* a graph with at most this many edges counts as small (0 = 65536)             */
+    uint32_t small_slots;        /* extra workers that only take requests on small graphs and counts on resident
+                                    graphs, so those never queue behind large uploads and loops (0 = 2;
+                                    UINT32_MAX = none)                                                            */
+    uint32_t pin_min_edges;      /* graphs with at least this many edges keep their host copy page-locked, so
+                                    uploads run at link speed (0 = 2^20; UINT32_MAX never pins)                   */
 } ga_server_config;
 
 typedef enum ga_request_kind { GA_REQ_TC = 0, GA_REQ_PEEL = 1, GA_REQ_CORE = 2 } ga_request_kind;

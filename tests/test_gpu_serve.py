@@ -87,12 +87,13 @@ def test_alone_matches_oracle(ga, oracle, served):
         assert a["core"][1:] == (kmax, rounds)
 
 
-@pytest.mark.parametrize("slots,fold", [(4, 64), (1, 64), (6, 1), (3, 5)])
-def test_mix_equals_alone(ga, served, slots, fold):
+@pytest.mark.parametrize("slots,fold,small,pin", [(4, 64, 0, 0), (1, 64, 1, 1), (6, 1, 3, 0), (3, 5, 2, 1)])
+def test_mix_equals_alone(ga, served, slots, fold, small, pin):
+    """pin = 1 keeps every graph's host copy page-locked (the path large graphs take)."""
     gs, alone = served
     rng = np.random.default_rng(slots * 100 + fold)
     reqs = _mix(rng, len(gs), 0.3)
-    with ga.Server(slots=slots, fold_max_graphs=fold) as s:
+    with ga.Server(slots=slots, fold_max_graphs=fold, small_slots=small, pin_min_edges=pin) as s:
         ids = [s.add_graph(g) for g in gs]
         tickets = [s.submit(ids[i], kind, num, den) for i, kind, num, den in reqs]
         for t, (i, kind, num, den) in zip(tickets, reqs):
