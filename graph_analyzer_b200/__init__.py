@@ -115,6 +115,8 @@ SIGNATURES: dict[str, list] = {
     "ga_build_graph_from_edges": [C.c_uint32, _u32p, C.c_uint32, _u32p, _u32p, _u32p, C.POINTER(C.c_uint32)],
     "ga_host_graph_from_edges": [C.c_uint32, _u32p, C.c_uint64, C.c_int, C.POINTER(C.POINTER(_HostGraph))],
     "ga_load_graph": [C.c_char_p, C.POINTER(C.POINTER(_HostGraph))],
+    "ga_save_csr": [C.c_char_p, C.c_uint32, C.c_uint32, _u32p, _vp],
+    "ga_load_csr": [C.c_char_p, C.POINTER(C.POINTER(_HostGraph))],
     "ga_host_graph_free": [C.POINTER(_HostGraph)],
     "ga_gen_holme_kim": [C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_uint64, _u32p, C.c_uint64,
                          C.POINTER(C.c_uint64)],
@@ -248,6 +250,20 @@ def load_graph(path: str) -> Graph:
     """load_graph (graph.h:71-96): SNAP text edge list -> cleaned, oriented CSR with n = max_id + 1."""
     hg = C.POINTER(_HostGraph)()
     _check(lib().ga_load_graph(os.fsencode(path), C.byref(hg)))
+    return _from_host_graph(hg)
+
+
+def save_csr(g: Graph, path: str) -> None:
+    """Writes the oriented CSR as a binary file (checked first: sorted rows, ids < n, (degree, id) orientation)."""
+    rowptr = np.ascontiguousarray(g.rowptr, np.uint32)
+    col = np.ascontiguousarray(g.col, np.uint32)
+    _check(lib().ga_save_csr(os.fsencode(path), g.n, g.m, rowptr, _ptr(col) if g.m else None))
+
+
+def load_csr(path: str) -> Graph:
+    """Reads a binary CSR file written by save_csr (header, size, checksum and CSR rules checked)."""
+    hg = C.POINTER(_HostGraph)()
+    _check(lib().ga_load_csr(os.fsencode(path), C.byref(hg)))
     return _from_host_graph(hg)
 
 

@@ -1,7 +1,8 @@
 // cli_common.hpp - shared pieces of the command-line drivers (ga_tc, ga_densest, ga_dsg): argument scanning, the
 // optional page-locked staging of the host CSR (--pinned), host wall-clock timing of the synchronous C-ABI calls and
 // the clock-ramp burn-in. The drivers replace the reference's gpu_tc.cu, gpu_densest.cu and gpu_dsg.cu and print
-// the same CSV columns; they call nothing but the C ABI / the C++ surface over it.
+// the same CSV columns; they call nothing but the C ABI / the C++ surface over it. The graph argument is a text edge
+// list (load_graph's rules) or, when its name ends in ".gacsr", a binary CSR file written by ga_save_csr.
 #pragma once
 
 #include <chrono>

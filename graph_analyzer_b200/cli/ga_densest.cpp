@@ -60,7 +60,7 @@ int main(int argc, char** argv) {
     try {
         cli::print_device();
         ga::Graph g;
-        if (!ga::load_graph(path, g)) return 1;
+        if (!ga::load_any(path, g)) return 1;
         std::fprintf(stderr, "loaded n=%u m=%u max_out_deg=%u eps=%llu/%llu\n", g.n, g.m, g.max_out_degree,
                      (unsigned long long)num, (unsigned long long)den);
         cli::Upload up(g, pinned);

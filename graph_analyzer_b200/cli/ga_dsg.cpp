@@ -55,7 +55,7 @@ int main(int argc, char** argv) {
     try {
         cli::print_device();
         ga::Graph g;
-        if (!ga::load_graph(path, g)) return 1;
+        if (!ga::load_any(path, g)) return 1;
         std::fprintf(stderr, "loaded n=%u m=%u max_out_deg=%u\n", g.n, g.m, g.max_out_degree);
         cli::Upload up(g, pinned);
         if (burnin) cli::burn_in(up.g);

@@ -1,5 +1,5 @@
 // ga_tc - triangle counting driver over the C ABI; replaces the reference's gpu_tc.cu (its kernels v1-v9).
-// usage: ga_tc <edge_list.txt> [repeats] [--pinned] [--no-burnin]   (flags may appear anywhere)
+// usage: ga_tc <edge_list.txt | graph.gacsr> [repeats] [--pinned] [--no-burnin]   (flags may appear anywhere)
 // Rows (stdout, CSV, the reference's columns):  impl,graph,n,m,triangles,kernel_ms,h2d_ms,gpu_total_ms
 //   gpu_hash_binned      the degree-binned shared-memory hash kernel (k_tc_hash)
 //   gpu_edge_per_thread  one thread per oriented edge, two-list merge (k_tc_plain)
@@ -29,7 +29,7 @@ int main(int argc, char** argv) {
         cli::print_device();
         ga::Graph g;
         const double tl = cli::now_ms();
-        if (!ga::load_graph(path, g)) return 1;
+        if (!ga::load_any(path, g)) return 1;
         std::fprintf(stderr, "loaded n=%u m=%u max_out_deg=%u (%.1f ms)\n", g.n, g.m, g.max_out_degree,
                      cli::now_ms() - tl);
         cli::Upload up(g, pinned);

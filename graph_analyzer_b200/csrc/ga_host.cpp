@@ -5,11 +5,16 @@
 // endpoint with the smaller (degree, id); rows sorted ascending; src[e] = row owner. The construction is parallel
 // (OpenMP radix sort and scatter) but its output does not depend on thread count or order, because rows hold unique
 // ids and are sorted at the end.
+#include <fcntl.h>
 #include <omp.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <atomic>
 #include <cerrno>
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -18,6 +23,12 @@
 #include <vector>
 
 #include "ga_internal.h"
+
+#define GA_TRY_HOST(call)            \
+    do {                             \
+        const ga_status s_ = (call); \
+        if (s_ != GA_OK) return s_;  \
+    } while (0)
 
 namespace ga {
 
@@ -248,9 +259,166 @@ ga_status ga_host_graph_from_edges(uint32_t n, const uint32_t* pairs, uint64_t n
     return GA_OK;
 }
 
-ga_status ga_load_graph(const char* path, ga_host_graph** out) {
+}  // extern "C"
+
+// ---- text loader ---------------------------------------------------------------------------------------------
+namespace {
+ga_status load_graph_fgets(const char* path, ga_host_graph** out);
+// The line rules of load_graph (graph.h:77-89): fgets into a 512-byte buffer, lines whose first byte is '#', '%' or
+// '\n' skipped, two base-10 strtoul fields, pairs with a == b skipped, ids stored as (min, max). The fast path maps
+// the file and parses line ranges on all host threads with a restatement of strtoul's base-10 rules (leading
+// white space, optional sign, saturation at ULONG_MAX, negation for '-'); it applies when every line fits the
+// 511-byte fgets chunk and the file holds no NUL byte, which is when the two paths see the same lines. Otherwise the
+// sequential fgets path below runs. Order of the pairs does not matter: they are sorted and deduplicated next.
+
+static inline bool is_space(char c) { return c == ' ' || (c >= '\t' && c <= '\r'); }
+
+// strtoul(p, &end, 10) on the range [p, e): returns the end of the number, or nullptr when nothing was converted.
+static const char* parse_ul(const char* p, const char* e, unsigned long* out) {
+    const char* q = p;
+    while (q < e && is_space(*q)) q++;
+    bool neg = false;
+    if (q < e && (*q == '+' || *q == '-')) {
+        neg = *q == '-';
+        q++;
+    }
+    if (q >= e || *q < '0' || *q > '9') return nullptr;
+    unsigned long v = 0;
+    bool ovf = false;
+    for (; q < e && *q >= '0' && *q <= '9'; q++) {
+        const unsigned long d = (unsigned long)(*q - '0');
+        if (v > (ULONG_MAX - d) / 10) ovf = true;
+        else v = v * 10 + d;
+    }
+    *out = ovf ? ULONG_MAX : (neg ? 0ul - v : v);
+    return q;
+}
+
+struct ParsedChunk {
+    std::vector<uint32_t> pairs;
+    uint32_t max_id = 0;
+    bool big = false;
+};
+
+// Parses the complete lines of [s, e) (s at a line start; e at a line start or the end of the file).
+static void parse_lines(const char* s, const char* e, ParsedChunk* out) {
+    const char* p = s;
+    while (p < e) {
+        const char* nl = static_cast<const char*>(std::memchr(p, '\n', (size_t)(e - p)));
+        const char* le = nl ? nl + 1 : e;   // the line, its newline included (what fgets returns)
+        if (!(*p == '#' || *p == '%' || *p == '\n')) {
+            unsigned long a, b;
+            const char* q = parse_ul(p, le, &a);
+            const char* q2 = q ? parse_ul(q, le, &b) : nullptr;
+            if (q2 && a != b) {
+                if (a > UINT32_MAX || b > UINT32_MAX) {
+                    out->big = true;
+                    return;
+                }
+                const uint32_t u = (uint32_t)std::min(a, b), v = (uint32_t)std::max(a, b);
+                out->pairs.push_back(u);
+                out->pairs.push_back(v);
+                out->max_id = std::max(out->max_id, v);
+            }
+        }
+        p = le;
+    }
+}
+
+// The fast path; returns false (nothing loaded) when the file must go through fgets instead.
+static bool load_text_parallel(const char* path, std::vector<uint32_t>* pairs, uint32_t* max_id, bool* big) {
+    const int fd = open(path, O_RDONLY);
+    if (fd < 0) return false;
+    struct stat st;
+    if (fstat(fd, &st) != 0 || !S_ISREG(st.st_mode)) {
+        close(fd);
+        return false;
+    }
+    const size_t size = (size_t)st.st_size;
+    if (size == 0) {
+        close(fd);
+        pairs->clear();
+        *max_id = 0;
+        *big = false;
+        return true;
+    }
+    void* map = mmap(nullptr, size, PROT_READ, MAP_PRIVATE, fd, 0);
+    close(fd);
+    if (map == MAP_FAILED) return false;
+    const char* buf = static_cast<const char*>(map);
+    const int T = std::max(1, std::min(omp_get_max_threads(), (int)(size >> 20) + 1));
+    // chunk boundaries at line starts; every line must fit fgets' 511 bytes, and no NUL byte may appear
+    std::vector<size_t> cut(T + 1, size);
+    cut[0] = 0;
+    for (int t = 1; t < T; t++) {
+        size_t c = size * (size_t)t / (size_t)T;
+        const char* nl = static_cast<const char*>(std::memchr(buf + c, '\n', size - c));
+        cut[t] = nl ? (size_t)(nl - buf) + 1 : size;
+    }
+    for (int t = 1; t <= T; t++) cut[t] = std::max(cut[t], cut[t - 1]);
+    std::atomic<bool> ok{true};
+#pragma omp parallel for num_threads(T) schedule(static)
+    for (int t = 0; t < T; t++) {
+        const char* p = buf + cut[t];
+        const char* e = buf + cut[t + 1];
+        if (std::memchr(p, '\0', (size_t)(e - p))) { ok = false; continue; }
+        while (p < e) {
+            const char* nl = static_cast<const char*>(std::memchr(p, '\n', (size_t)(e - p)));
+            const char* le = nl ? nl + 1 : e;
+            if (le - p > 511) { ok = false; break; }
+            p = le;
+        }
+    }
+    if (!ok) {
+        munmap(map, size);
+        return false;
+    }
+    std::vector<ParsedChunk> parts(T);
+#pragma omp parallel for num_threads(T) schedule(static)
+    for (int t = 0; t < T; t++) parse_lines(buf + cut[t], buf + cut[t + 1], &parts[t]);
+    munmap(map, size);
+    size_t total = 0;
+    *max_id = 0;
+    *big = false;
+    for (auto& c : parts) {
+        total += c.pairs.size();
+        *max_id = std::max(*max_id, c.max_id);
+        *big = *big || c.big;
+    }
+    if (*big) return true;
+    pairs->resize(total);
+    std::vector<size_t> off(T + 1, 0);
+    for (int t = 0; t < T; t++) off[t + 1] = off[t] + parts[t].pairs.size();
+#pragma omp parallel for num_threads(T) schedule(static)
+    for (int t = 0; t < T; t++)
+        if (!parts[t].pairs.empty())
+            std::memcpy(pairs->data() + off[t], parts[t].pairs.data(), parts[t].pairs.size() * 4);
+    return true;
+}
+
+}  // namespace
+
+extern "C" ga_status ga_load_graph(const char* path, ga_host_graph** out) {
     if (!path || !out) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
     *out = nullptr;
+    try {
+        std::vector<uint32_t> pairs;
+        uint32_t max_id = 0;
+        bool big = false;
+        if (load_text_parallel(path, &pairs, &max_id, &big)) {
+            if (big) return fail(GA_ERR_INVALID_GRAPH, "%s: vertex id does not fit uint32", path);
+            if (max_id == UINT32_MAX) return fail(GA_ERR_INVALID_GRAPH, "%s: n = max_id + 1 overflows uint32", path);
+            return ga_host_graph_from_edges(max_id + 1, pairs.data(), pairs.size() / 2, 1, out);
+        }
+    } catch (const std::bad_alloc&) {
+        return fail(GA_ERR_OUT_OF_MEMORY, "host allocation failed");
+    }
+    return load_graph_fgets(path, out);
+}
+
+namespace {
+// The sequential path: fgets line by line exactly as graph.h:76-89 reads.
+ga_status load_graph_fgets(const char* path, ga_host_graph** out) {
     FILE* f = std::fopen(path, "r");
     if (!f) return fail(GA_ERR_IO, "cannot open %s", path);
     std::vector<uint32_t> pairs;
@@ -277,6 +445,138 @@ ga_status ga_load_graph(const char* path, ga_host_graph** out) {
     if (big) return fail(GA_ERR_INVALID_GRAPH, "%s: vertex id does not fit uint32", path);
     if (max_id == UINT32_MAX) return fail(GA_ERR_INVALID_GRAPH, "%s: n = max_id + 1 overflows uint32", path);
     return ga_host_graph_from_edges(max_id + 1, pairs.data(), pairs.size() / 2, 1, out);
+}
+}  // namespace
+
+// ---- binary CSR files ------------------------------------------------------------------------------------------
+// Layout (little endian): "GACSR001", u32 n, u32 m, u32 max_out_degree, u32 0, u64 checksum, u32 rowptr[n+1],
+// u32 col[m]. The checksum is sum over i of mix64(word_i ^ (i * golden)) over the words of rowptr then col, so it is
+// computed in parallel and any changed or moved word changes it. Loading validates the CSR as the device does
+// (rowptr monotone from 0 to m, ids < n, rows strictly ascending, no self loop) plus the (degree, id) orientation
+// of every edge, so a file that loads is exactly a CSR that build_graph_from_edges can produce.
+namespace {
+
+constexpr char kCsrMagic[8] = {'G', 'A', 'C', 'S', 'R', '0', '0', '1'};
+
+struct CsrHeader {
+    char magic[8];
+    uint32_t n, m, max_out_degree, reserved;
+    uint64_t checksum;
+};
+static_assert(sizeof(CsrHeader) == 32, "packed header");
+
+uint64_t csr_checksum(const uint32_t* rowptr, const uint32_t* col, uint32_t n, uint32_t m) {
+    const uint64_t words = (uint64_t)n + 1 + m;
+    uint64_t sum = 0;
+#pragma omp parallel for reduction(+ : sum) schedule(static)
+    for (int64_t i = 0; i < (int64_t)words; i++) {
+        const uint32_t w = (uint64_t)i <= n ? rowptr[i] : col[i - n - 1];
+        sum += mix64((uint64_t)w ^ ((uint64_t)i * 0x9E3779B97F4A7C15ull));
+    }
+    return sum;
+}
+
+// The CSR checks of the loader; fills src and the maximum out-degree.
+ga_status validate_csr(const uint32_t* rowptr, const uint32_t* col, uint32_t n, uint32_t m, uint32_t* src,
+                       uint32_t* max_out) {
+    if (rowptr[0] != 0 || rowptr[n] != m) return fail(GA_ERR_INVALID_GRAPH, "rowptr[0] must be 0 and rowptr[n] = m");
+    bool bad = false;
+    uint32_t mx = 0;
+#pragma omp parallel for reduction(|| : bad) reduction(max : mx) schedule(static)
+    for (int64_t v = 0; v < (int64_t)n; v++) {
+        const uint32_t b = rowptr[v], e = rowptr[v + 1];
+        if (e < b || e > m) { bad = true; continue; }
+        mx = std::max(mx, e - b);
+        for (uint32_t i = b; i < e; i++) {
+            if (col[i] >= n || col[i] == (uint32_t)v || (i > b && col[i] <= col[i - 1])) bad = true;
+            src[i] = (uint32_t)v;
+        }
+    }
+    if (bad) return fail(GA_ERR_INVALID_GRAPH, "not a valid CSR (rows must be sorted, ids < n, no self loops)");
+    // (degree, id) orientation: every edge u->v has (deg(u), u) < (deg(v), v) with deg = out + in degree
+    std::vector<uint32_t> deg(n, 0);
+    for (uint32_t v = 0; v < n; v++) deg[v] = rowptr[v + 1] - rowptr[v];
+    for (uint32_t i = 0; i < m; i++) deg[col[i]]++;
+#pragma omp parallel for reduction(|| : bad) schedule(static)
+    for (int64_t i = 0; i < (int64_t)m; i++) {
+        const uint32_t u = src[i], v = col[i];
+        if (!(deg[u] < deg[v] || (deg[u] == deg[v] && u < v))) bad = true;
+    }
+    if (bad) return fail(GA_ERR_INVALID_GRAPH, "edges are not oriented by (degree, id)");
+    *max_out = mx;
+    return GA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+ga_status ga_save_csr(const char* path, uint32_t n, uint32_t m, const uint32_t* rowptr, const uint32_t* col) {
+    if (!path || !rowptr || (m && !col)) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    try {
+        std::vector<uint32_t> src((size_t)m + 1);
+        uint32_t mx = 0;
+        GA_TRY_HOST(validate_csr(rowptr, col, n, m, src.data(), &mx));
+        CsrHeader h = {};
+        std::memcpy(h.magic, kCsrMagic, 8);
+        h.n = n;
+        h.m = m;
+        h.max_out_degree = mx;
+        h.checksum = csr_checksum(rowptr, col, n, m);
+        FILE* f = std::fopen(path, "wb");
+        if (!f) return fail(GA_ERR_IO, "cannot create %s", path);
+        bool ok = std::fwrite(&h, sizeof h, 1, f) == 1 &&
+                  std::fwrite(rowptr, 4, (size_t)n + 1, f) == (size_t)n + 1 &&
+                  (m == 0 || std::fwrite(col, 4, m, f) == m);
+        ok = (std::fclose(f) == 0) && ok;
+        if (!ok) return fail(GA_ERR_IO, "write to %s failed", path);
+    } catch (const std::bad_alloc&) {
+        return fail(GA_ERR_OUT_OF_MEMORY, "host allocation failed");
+    }
+    return GA_OK;
+}
+
+ga_status ga_load_csr(const char* path, ga_host_graph** out) {
+    if (!path || !out) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(GA_ERR_IO, "cannot open %s", path);
+    CsrHeader h;
+    if (std::fread(&h, sizeof h, 1, f) != 1 || std::memcmp(h.magic, kCsrMagic, 8) != 0) {
+        std::fclose(f);
+        return fail(GA_ERR_INVALID_GRAPH, "%s is not a binary CSR file (GACSR001)", path);
+    }
+    struct stat st;
+    const uint64_t want = sizeof h + 4 * ((uint64_t)h.n + 1 + h.m);
+    if (fstat(fileno(f), &st) != 0 || (uint64_t)st.st_size != want || h.n == UINT32_MAX || h.m == UINT32_MAX) {
+        std::fclose(f);
+        return fail(GA_ERR_INVALID_GRAPH, "%s: size does not match its header (n %u, m %u)", path, h.n, h.m);
+    }
+    ga_host_graph* g = new_host_graph(h.n, h.m);
+    if (!g) {
+        std::fclose(f);
+        return fail(GA_ERR_OUT_OF_MEMORY, "host allocation failed");
+    }
+    const bool ok = std::fread(g->rowptr, 4, (size_t)h.n + 1, f) == (size_t)h.n + 1 &&
+                    (h.m == 0 || std::fread(g->col, 4, h.m, f) == h.m);
+    std::fclose(f);
+    if (!ok) {
+        ga_host_graph_free(g);
+        return fail(GA_ERR_IO, "%s: read failed", path);
+    }
+    if (csr_checksum(g->rowptr, g->col, h.n, h.m) != h.checksum) {
+        ga_host_graph_free(g);
+        return fail(GA_ERR_INVALID_GRAPH, "%s: checksum mismatch (file damaged)", path);
+    }
+    uint32_t mx = 0;
+    const ga_status s = validate_csr(g->rowptr, g->col, h.n, h.m, g->src, &mx);
+    if (s != GA_OK || mx != h.max_out_degree) {
+        ga_host_graph_free(g);
+        return s != GA_OK ? s : fail(GA_ERR_INVALID_GRAPH, "%s: max out-degree differs from its header", path);
+    }
+    g->max_out_degree = mx;
+    *out = g;
+    return GA_OK;
 }
 
 void ga_host_graph_free(ga_host_graph* g) {

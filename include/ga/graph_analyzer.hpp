@@ -3,6 +3,7 @@
 // for the GPU path (paths relative to that project):
 //
 //   Graph, build_graph_from_edges, load_graph            graph.h:19-96    (host CSR, same layout and orientation)
+//   load_csr / save_csr / load_any                       binary CSR files (no counterpart in the reference)
 //   PeelResult, operator==, density_value,               densest.h:46-78
 //     peel_arith_ok, peel_improves
 //   CoreLoopResult                                       dsg.h:687-691
@@ -82,6 +83,33 @@ inline bool load_graph(const char* path, Graph& g) {
     g.src.assign(h->src, h->src + h->m);
     ga_host_graph_free(h);
     return true;
+}
+
+// Binary CSR files (ga_save_csr / ga_load_csr): the oriented CSR without re-parsing. Same bool/stderr convention.
+inline bool load_csr(const char* path, Graph& g) {
+    ga_host_graph* h = nullptr;
+    if (ga_load_csr(path, &h) != GA_OK) {
+        std::fprintf(stderr, "%s\n", ga_last_error());
+        return false;
+    }
+    g.n = h->n;
+    g.m = h->m;
+    g.max_out_degree = h->max_out_degree;
+    g.rowptr.assign(h->rowptr, h->rowptr + h->n + 1);
+    g.col.assign(h->col, h->col + h->m);
+    g.src.assign(h->src, h->src + h->m);
+    ga_host_graph_free(h);
+    return true;
+}
+inline void save_csr(const char* path, const Graph& g) {
+    check(ga_save_csr(path, g.n, g.m, g.rowptr.data(), g.m ? g.col.data() : nullptr));
+}
+// A path ending in ".gacsr" is a binary CSR file, anything else a text edge list.
+inline bool load_any(const char* path, Graph& g) {
+    const std::string p(path);
+    const std::string ext = ".gacsr";
+    if (p.size() >= ext.size() && p.compare(p.size() - ext.size(), ext.size(), ext) == 0) return load_csr(path, g);
+    return load_graph(path, g);
 }
 
 // ---- densest.h helpers (integer decisions; densest.h:62-78) ----------------------------------------------------

@@ -91,6 +91,13 @@ ga_status ga_host_graph_from_edges(uint32_t n, const uint32_t* pairs, uint64_t n
  * (the reference truncates larger ids silently; this returns GA_ERR_INVALID_GRAPH). */
 ga_status ga_load_graph(const char* path, ga_host_graph** out);
 
+/* Binary CSR files (no counterpart in the reference, which parses the text edge list on every run): the oriented
+ * CSR written once, read back without parsing, sorting or orienting. ga_save_csr checks the CSR first (sorted rows,
+ * ids < n, no self loops, (degree, id) orientation); ga_load_csr checks the header, the file size, a checksum of
+ * rowptr and col and the same CSR rules, and rebuilds src. A damaged or foreign file gives GA_ERR_INVALID_GRAPH. */
+ga_status ga_save_csr(const char* path, uint32_t n, uint32_t m, const uint32_t* rowptr, const uint32_t* col);
+ga_status ga_load_csr(const char* path, ga_host_graph** out);
+
 void ga_host_graph_free(ga_host_graph* g);
 
 /* ---------------------------------------------------------------------------------------------------------------

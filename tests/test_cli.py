@@ -70,6 +70,18 @@ def test_ga_tc_rows(golden, cuda_ok, fx):
     assert all(x["impl"].endswith("_pinned") for x in _rows("ga_tc", r.stdout))
 
 
+def test_binary_csr_input_reaches_the_device_step(ga, tmp_path):
+    """A .gacsr path is read by the binary loader (on a machine without a GPU the run then stops at the device)."""
+    p = str(tmp_path / "g.gacsr")
+    ga.save_csr(ga.load_graph(fixture_path("t_er300")), p)
+    r = _run("ga_tc", p, "--no-burnin")
+    assert "loaded n=300 m=2314" in r.stderr
+    if ga.device_count() == 0:
+        assert r.returncode == 1 and "GA_ERR_NO_DEVICE" in r.stderr
+    else:
+        assert r.returncode == 0 and all(int(x["triangles"]) == 652 for x in _rows("ga_tc", r.stdout))
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("fx", FIXTURES)
 @pytest.mark.parametrize("eps", [(1, 10), (1, 2)])
