@@ -274,8 +274,11 @@ void run_folded(ga_server* s, cudaStream_t st, std::vector<Request*>& rs, std::v
 
 void worker_main(ga_server* s, bool small_only) {
     cudaSetDevice(s->cfg.device);
+    // the small lane's blocks are dispatched first whenever SMs free up, so short requests overtake long kernels
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
     cudaStream_t st;
-    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return;
+    if (cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, small_only ? greatest : least) != cudaSuccess) return;
     for (;;) {
         Work w;
         {
