@@ -603,6 +603,77 @@ def run_serve(args):
     return 0 if identical else 1
 
 
+def _write_edge_text(g, path):
+    """The graph as a SNAP-style text edge list ("u<TAB>v" per oriented edge)."""
+    with open(path, "w") as f:
+        f.write(f"# n={g.n} m={g.m}\n")
+        step = 1 << 22
+        for i in range(0, g.m, step):
+            f.write("\n".join(f"{a}\t{b}" for a, b in zip(g.src[i:i + step].tolist(), g.col[i:i + step].tolist())))
+            f.write("\n")
+
+
+def _csv_rows(text):
+    return [ln.split(",") for ln in text.splitlines() if ln and not ln.startswith(("#", "impl"))]
+
+
+def run_reference_gpu(args):
+    """The reference's own GPU drivers (baseline/_ref/bin, built from its sources for sm_100a by
+    baseline/build_reference_gpu.py) against this library's drivers, on the same text files and the same GPU:
+    gpu_tc vs ga_tc on R-MAT 22 (kernels v1-v9), gpu_densest vs ga_densest (eps 1/10) on the Holme-Kim n 1.70M graph,
+    gpu_dsg vs ga_dsg (core decomposition) on the Holme-Kim n 8,298 graph. Every program verifies its own results
+    (the reference's against its CPU code); the triangle counts, peel results and core rows must agree."""
+    import tempfile
+    import graph_analyzer_b200 as ga
+    ref_bin = os.path.join(ROOT, "baseline", "_ref", "bin")
+    our_bin = os.path.join(ROOT, "graph_analyzer_b200", "_bin")
+    if not os.path.exists(os.path.join(ref_bin, "gpu_tc")):
+        print(json.dumps({"workload": "reference_gpu", "unavailable": "baseline/_ref/bin not built "
+                          "(python baseline/build_reference_gpu.py)"}), flush=True)
+        return 0
+    tmp = tempfile.mkdtemp(prefix="ga_refgpu_")
+    out = {"workload": "reference_gpu", "metric": "reference GPU drivers vs this library's drivers, same files, same GPU"}
+    runs = [
+        ("tc_rmat22", lambda: make_graph(ga), ["gpu_tc", "ga_tc"], lambda p: [p, str(max(3, args.steps // 2))]),
+        ("peel_hk1.7M", lambda: ga.graph_from_pairs(1_700_000, ga.gen_holme_kim(1_700_000, 6, 7, 0.54, 0.3, seed=SEED)),
+         ["gpu_densest", "ga_densest"], lambda p: [p, "1", "10", "--repeats", "3", "--no-greedy"]),
+        ("cores_hk8298", lambda: ga.graph_from_pairs(8298, ga.gen_holme_kim(8298, 12, 12, 0.0, 0.5, seed=SEED)),
+         ["gpu_dsg", "ga_dsg"], lambda p: [p, "--repeats", "3", "--no-exact", "--no-greedy", "--no-greedypp"]),
+    ]
+    ok = True
+    for name, make, (ref_prog, our_prog), argv in runs:
+        g = make()
+        path = os.path.join(tmp, name + ".txt")
+        t0 = time.time()
+        _write_edge_text(g, path)
+        log(f"{name}: n={g.n} m={g.m} written ({time.time() - t0:.1f} s)")
+        res = {}
+        for who, exe in (("reference", os.path.join(ref_bin, ref_prog)), ("ours", os.path.join(our_bin, our_prog))):
+            t0 = time.time()
+            r = subprocess.run([exe, *argv(path)], capture_output=True, text=True, timeout=1800)
+            log(f"{name} {who}: rc {r.returncode} in {time.time() - t0:.1f} s")
+            if r.returncode != 0:
+                log(r.stderr[-2000:])
+                ok = False
+            res[who] = _csv_rows(r.stdout)
+        out[name] = res
+        os.remove(path)
+    os.rmdir(tmp)
+    # headline comparison: best kernel time of each side on the TC file
+    tc = out.get("tc_rmat22", {})
+    if tc.get("reference") and tc.get("ours"):
+        ref_best = min(tc["reference"], key=lambda r: float(r[5]))
+        our_best = min(tc["ours"], key=lambda r: float(r[5]))
+        out["tc_best"] = {"reference": {"impl": ref_best[0], "kernel_ms": float(ref_best[5])},
+                          "ours": {"impl": our_best[0], "kernel_ms": float(our_best[5])},
+                          "speedup": float(ref_best[5]) / float(our_best[5]),
+                          "same_triangles": len({r[4] for r in tc["reference"] + tc["ours"]}) == 1}
+        ok &= out["tc_best"]["same_triangles"]
+    out["all_verified"] = bool(ok)
+    print(json.dumps(out), flush=True)
+    return 0 if ok else 1
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -610,7 +681,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", choices=["rmat22", "hk2", "rmat22-full", "batch", "serve"], default="rmat22",
+    ap.add_argument("--workload", choices=["rmat22", "hk2", "rmat22-full", "batch", "serve", "reference-gpu"],
+                    default="rmat22",
                     help="rmat22 (default, the headline line) or a secondary workload")
     ap.add_argument("--graphs", type=int, default=4096, help="graphs in the batch workload")
     ap.add_argument("--scale", type=int, default=SCALE,
@@ -633,6 +705,8 @@ def main():
         return run_batch(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "reference-gpu":
+        return run_reference_gpu(args)
     return run_ours(args)
 
 

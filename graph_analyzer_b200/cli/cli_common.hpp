@@ -28,6 +28,12 @@ struct Upload {
     double prepare_ms = 0;
 
     Upload(const ga::Graph& host, bool pinned) {
+        {   // untimed: CUDA context, module load and memory pool set-up happen on the first graph of the process
+            const uint32_t zero[2] = {0, 0};
+            ga_graph* w = nullptr;
+            ga::check(ga_graph_create(zero, nullptr, 1, 0, 0, nullptr, &w));
+            ga_graph_destroy(w);
+        }
         const uint32_t* rp = host.rowptr.data();
         const uint32_t* cl = host.m ? host.col.data() : nullptr;
         void* prp = nullptr;
