@@ -85,6 +85,7 @@ struct ga_server {
     bool stop = false;
     ga_server_stats stats{};
     std::vector<std::thread> workers;
+    cudaStream_t evict_stream = nullptr;   // idle stream handed to a graph being freed (its last stream may be busy)
 };
 
 namespace {
@@ -100,6 +101,9 @@ bool make_room(ga_server* s, uint64_t need) {
             if (e.dev && !e.busy && (!victim || e.last_use < victim->last_use)) victim = &e;
         }
         if (!victim) return false;
+        // the victim's work is complete, but the worker stream it last ran on may be busy with another request:
+        // free it on an idle stream so that this (locked) call does not wait for unrelated work
+        ga_graph_set_stream(victim->dev, s->evict_stream);
         ga_graph_destroy(victim->dev);
         victim->dev = nullptr;
         s->reserved -= std::min(s->reserved, victim->dev_bytes);
@@ -371,6 +375,12 @@ ga_status ga_server_create(const ga_server_config* config, ga_server** out) {
     if (!s->cfg.small_slots) s->cfg.small_slots = 2;
     if (s->cfg.small_slots == UINT32_MAX) s->cfg.small_slots = 0;
     if (!s->cfg.pin_min_edges) s->cfg.pin_min_edges = 1u << 20;
+    cudaSetDevice(s->cfg.device);
+    if (cudaStreamCreateWithFlags(&s->evict_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        (void)cudaGetLastError();
+        delete s;
+        return fail(GA_ERR_CUDA, "stream creation failed");
+    }
     for (uint32_t i = 0; i < s->cfg.slots; i++) s->workers.emplace_back(worker_main, s, false);
     for (uint32_t i = 0; i < s->cfg.small_slots; i++) s->workers.emplace_back(worker_main, s, true);
     *out = s;
@@ -395,6 +405,7 @@ ga_status ga_server_destroy(ga_server* s) {
     for (auto& t : s->workers) t.join();
     for (auto& kv : s->graphs)
         if (kv.second.pinned) cudaFreeHost(kv.second.pinned);
+    cudaStreamDestroy(s->evict_stream);
     delete s;
     return GA_OK;
 }
@@ -462,6 +473,7 @@ ga_status ga_server_poll(ga_server* s, uint64_t ticket, ga_request_result* out) 
     if (it == s->requests.end()) return fail(GA_ERR_INVALID_ARGUMENT, "unknown ticket");
     if (!it->second.done) return GA_ERR_NOT_READY;
     *out = it->second.result;
+    s->requests.erase(it);   // a result is handed out once
     return GA_OK;
 }
 
@@ -473,6 +485,7 @@ ga_status ga_server_wait(ga_server* s, uint64_t ticket, ga_request_result* out) 
     const Request& r = it->second;   // element references survive a rehash by later submits; iterators do not
     s->cv_done.wait(lock, [&] { return r.done; });
     *out = r.result;
+    s->requests.erase(ticket);   // a result is handed out once
     return GA_OK;
 }
 

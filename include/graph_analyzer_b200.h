@@ -313,7 +313,9 @@ ga_status ga_server_add_graph(ga_server* s, const uint32_t* rowptr, const uint32
 /* Queues a request; returns at once with a ticket. eps = num/den for GA_REQ_PEEL. */
 ga_status ga_server_submit(ga_server* s, uint64_t graph_id, ga_request_kind kind, uint64_t num, uint64_t den,
                            uint64_t* ticket);
-/* GA_ERR_NOT_READY while the request is pending; otherwise fills *out (out->status is the request's own status). */
+/* GA_ERR_NOT_READY while the request is pending; otherwise fills *out (out->status is the request's own status).
+ * A result is handed out once: after a successful poll or wait the ticket is forgotten (a second call on it gives
+ * GA_ERR_INVALID_ARGUMENT), so a long-running server keeps no state for collected requests. One thread per ticket. */
 ga_status ga_server_poll(ga_server* s, uint64_t ticket, ga_request_result* out);
 ga_status ga_server_wait(ga_server* s, uint64_t ticket, ga_request_result* out);
 ga_status ga_server_stats_get(ga_server* s, ga_server_stats* out);

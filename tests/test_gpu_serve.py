@@ -155,5 +155,13 @@ def test_refusals(ga, served):
             s.submit(gid, ga.REQ_PEEL, 1, 0)                 # eps denominator 0
         with pytest.raises(ga.GAError):
             s.wait(12345)                                    # unknown ticket
-        r = s.wait(s.submit(gid, ga.REQ_TC))
+        t = s.submit(gid, ga.REQ_TC)
+        r = s.wait(t)
         assert r.status == 0 and r.triangles == 0
+        with pytest.raises(ga.GAError):
+            s.wait(t)                                        # a result is handed out once
+        t = s.submit(gid, ga.REQ_TC)
+        while s.poll(t) is None:
+            pass
+        with pytest.raises(ga.GAError):
+            s.poll(t)
