@@ -207,6 +207,14 @@ class Reference(_Base):
             getattr(L, f).restype = C.c_uint64
             getattr(L, f).argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, _u32p]
         L.ref_num_threads.restype = C.c_int
+        L.ref_graph_new.restype = C.c_void_p
+        L.ref_graph_new.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, _u32p]
+        L.ref_graph_free.restype = None
+        L.ref_graph_free.argtypes = [C.c_void_p]
+        L.ref_graph_triangles_omp.restype = C.c_uint64
+        L.ref_graph_triangles_omp.argtypes = [C.c_void_p]
+        L.ref_graph_triangles_omp_rows.restype = C.c_uint64
+        L.ref_graph_triangles_omp_rows.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
         L.ref_participation.restype = C.c_uint64
         L.ref_participation.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, _u32p, _u8p, _u32p, C.c_int]
         L.ref_edge_support.restype = C.c_uint64
@@ -231,6 +239,10 @@ class Reference(_Base):
         L.ref_core_level_density.restype = None
         L.ref_core_level_density.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, _u32p, _u32p, C.c_uint32,
                                              C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+
+    def resident(self, g: CSR) -> "RefGraph":
+        """A copy of g held in the reference's own Graph, for timing its counter without the copy-in."""
+        return RefGraph(self, g)
 
     def build_graph_from_edges(self, n: int, pairs: np.ndarray) -> CSR:
         p = np.ascontiguousarray(pairs, dtype=np.uint32).reshape(-1)
@@ -331,3 +343,29 @@ def _src(g: CSR) -> np.ndarray:
 def _alive(alive: np.ndarray, n: int) -> np.ndarray:
     a = np.ascontiguousarray(alive, dtype=np.uint8)
     return a if n else np.zeros(1, np.uint8)
+
+
+class RefGraph:
+    """The reference's Graph resident in its library: cpu_triangles_omp (graph.h:123) on the whole graph or on a row
+    range (the same loop with other bounds)."""
+
+    def __init__(self, ref: Reference, g: CSR):
+        self.ref, self.n = ref, g.n
+        self.h = ref.lib.ref_graph_new(g.n, g.m, g.rowptr, _col(g), _src(g))
+
+    def triangles_omp(self) -> int:
+        return int(self.ref.lib.ref_graph_triangles_omp(self.h))
+
+    def triangles_omp_rows(self, u0: int, u1: int) -> int:
+        return int(self.ref.lib.ref_graph_triangles_omp_rows(self.h, u0, u1))
+
+    def close(self) -> None:
+        if self.h:
+            self.ref.lib.ref_graph_free(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -2,8 +2,9 @@
 //
 // Compiled by oracle/build_oracle.py against the reference's headers where they lie (src/graph.h, src/densest.h,
 // src/dsg.h of VijayPraneethSai/graph_analyzer; header-only, stdlib + OpenMP), into oracle/_ref/libga_ref.so.
-// Nothing here re-implements an algorithm: each wrapper copies plain arrays into the reference's Graph and calls the
-// reference function named in its comment. Used to pin oracle/ga_oracle.c and as the timed reference CPU baseline.
+// Each wrapper copies plain arrays into the reference's Graph and calls the reference function named in its comment
+// (one, ref_graph_triangles_omp_rows, runs cpu_triangles_omp's loop over a row range). Used to pin oracle/ga_oracle.c
+// and as the timed reference CPU baseline.
 #include <cstring>
 
 #include "dsg.h"
@@ -55,6 +56,31 @@ int ref_load_graph(const char* path, uint32_t* rowptr, uint32_t* col, uint32_t* 
     if (!load_graph(path, g)) return -1;
     copy_out(g, rowptr, col, src, maxdeg);
     return 0;
+}
+
+// A resident copy of the reference's Graph, so that timing its counter excludes the copy-in (the timed CPU baseline).
+void* ref_graph_new(uint32_t n, uint32_t m, const uint32_t* rowptr, const uint32_t* col, const uint32_t* src) {
+    return new Graph(make_graph(n, m, rowptr, col, src));
+}
+void ref_graph_free(void* h) { delete static_cast<Graph*>(h); }
+// cpu_triangles_omp (graph.h:123-136) on the resident copy
+uint64_t ref_graph_triangles_omp(void* h) { return cpu_triangles_omp(*static_cast<const Graph*>(h)); }
+// The same loop (schedule, intersect_count of graph.h:99) restricted to the rows [u0, u1): a bounded sample of the
+// whole count for the timed baseline. The loop body is cpu_triangles_omp's, only the bounds differ.
+uint64_t ref_graph_triangles_omp_rows(void* h, uint32_t u0, uint32_t u1) {
+    const Graph& g = *static_cast<const Graph*>(h);
+    uint64_t t = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : t)
+    for (long long ui = u0; ui < (long long)u1; ui++) {
+        const uint32_t u = (uint32_t)ui;
+        const uint32_t* nu = g.col.data() + g.rowptr[u];
+        const uint32_t du = g.rowptr[u + 1] - g.rowptr[u];
+        for (uint32_t k = 0; k < du; k++) {
+            const uint32_t v = nu[k];
+            t += intersect_count(nu, du, g.col.data() + g.rowptr[v], g.rowptr[v + 1] - g.rowptr[v]);
+        }
+    }
+    return t;
 }
 
 // cpu_triangles_serial / cpu_triangles_omp (graph.h:110,123)
