@@ -16,10 +16,11 @@
 // recount of the reference's loops exactly, so rounds, removed_round[], best density and core[] are bit-identical.
 //
 // Round structure (one kernel boundary = one grid-wide barrier, no host sync):
-//   peel : k_peel_mark -> k_frontier_update -> k_retire_tail
-//   core : k_core_min  -> k_core_mark -> k_frontier_update -> k_retire_tail
+//   peel : k_peel_mark -> k_frontier_update
+//   core : k_core_min  -> k_core_mark -> k_frontier_update
 // The alive set is kept as a compacted id list (double-buffered, parity on the device), so late rounds scan only the
-// survivors. k_retire_tail's last block advances the round and decides whether to continue. In GA_OPT_LOOP_MODE 2
+// survivors. The last block of the update kernel advances the round and decides whether to continue; the frontier
+// (double-buffered by round parity) is retired by the next round's first kernel. In GA_OPT_LOOP_MODE 2
 // the round is the body of a CUDA graph conditional WHILE node (cudaGraphSetConditional from the tail), so the
 // whole loop is one graph launch; mode 1 launches the same kernels round by round and reads the 100-byte round state
 // back after each (the reference's host loop with its one sync per round).
@@ -43,6 +44,7 @@ struct LoopScalars {
     uint32_t round, best_round, parity, max_rounds;
     uint32_t alive_count[2];
     uint32_t fcount, nitems, kcur, kround, min_tri;
+    uint32_t fprev;   // frontier size of the previous round (retired by the next round's first kernel)
     uint32_t status, done_blocks, cont;
     uint32_t iters;   // rounds started, counted independently of the tail (loop bound of last resort)
 };
@@ -88,7 +90,7 @@ struct ga_loops {
     uint8_t* state = nullptr;         // n: 0 removed, 1 alive, 2 frontier of this round
     uint32_t* out = nullptr;          // n: removed_round (peel) or core (core)
     uint32_t* alive[2] = {nullptr, nullptr};
-    uint32_t* frontier = nullptr;     // n
+    uint32_t* frontier[2] = {nullptr, nullptr};   // n each: the frontier of even / odd rounds
     uint32_t* item_x = nullptr;       // item capacity
     uint32_t* item_c = nullptr;
     uint64_t item_cap = 0;
@@ -96,7 +98,7 @@ struct ga_loops {
     ga::LoopScalars h_sc = {};         // host copy of the round state
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     cudaGraph_t graph[2] = {nullptr, nullptr};
-    unsigned grid_scan = 1, grid_update = 1, grid_retire = 1;
+    unsigned grid_scan = 1, grid_update = 1;
     // triangle incidence lists (built once per graph when memory allows): for every vertex v the other two corners
     // of each triangle through v, in inc[inc_ptr[v] .. inc_ptr[v+1])
     int lists = -1;                    // -1 undecided, 0 enumeration update, 1 incidence-list update
@@ -166,6 +168,14 @@ __device__ __forceinline__ void append_frontier(bool take, uint32_t v, const uin
     }
 }
 
+// The previous round's frontier leaves for good (state 2 -> 0). Run by the first kernel of a round, before any
+// kernel of the round reads state[] of frontier corners.
+__device__ __forceinline__ void retire_previous(const LoopScalars* sc, uint8_t* __restrict__ state,
+                                                const uint32_t* __restrict__ prev) {
+    const uint32_t F = sc->fprev;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x) state[prev[i]] = 0;
+}
+
 // Survivors go to the next alive list (one atomic per warp).
 __device__ __forceinline__ void append_survivor(bool keep, uint32_t v, uint32_t* __restrict__ out_list,
                                                 uint32_t* out_count, uint32_t lane) {
@@ -183,12 +193,14 @@ __device__ __forceinline__ void append_survivor(bool keep, uint32_t v, uint32_t*
 // the vertices of a graph that was refused or failed leave the loop silently.
 __global__ void __launch_bounds__(256) k_peel_mark(LoopScalars* sc, const uint32_t* __restrict__ tri,
                                                    uint8_t* __restrict__ state, uint32_t* __restrict__ removed_round,
-                                                   uint32_t* alive0, uint32_t* alive1,
-                                                   uint32_t* __restrict__ frontier, uint32_t* __restrict__ item_x,
+                                                   uint32_t* alive0, uint32_t* alive1, uint32_t* fr0, uint32_t* fr1,
+                                                   uint32_t* __restrict__ item_x,
                                                    uint32_t* __restrict__ item_c, const uint32_t* __restrict__ rowptr,
                                                    const uint32_t* __restrict__ in_ptr,
                                                    const unsigned long long* __restrict__ inc_ptr, Segs sg) {
     const uint32_t p = sc->parity;
+    uint32_t* frontier = (sc->round & 1) ? fr1 : fr0;
+    retire_previous(sc, state, (sc->round & 1) ? fr0 : fr1);
     const uint32_t* in = p ? alive1 : alive0;
     uint32_t* outl = p ? alive0 : alive1;
     const uint32_t na = sc->alive_count[p];
@@ -243,8 +255,11 @@ __global__ void __launch_bounds__(256) k_peel_mark(LoopScalars* sc, const uint32
 
 // Core round, step 1: minimum of tri over the alive list (core_min_alive_tri, kernels.cuh:484-491).
 __global__ void __launch_bounds__(256) k_core_min(LoopScalars* sc, const uint32_t* __restrict__ tri,
-                                                  const uint32_t* alive0, const uint32_t* alive1) {
+                                                  const uint32_t* alive0, const uint32_t* alive1,
+                                                  uint8_t* __restrict__ state, const uint32_t* fr0,
+                                                  const uint32_t* fr1) {
     const uint32_t p = sc->parity;
+    retire_previous(sc, state, (sc->round & 1) ? fr0 : fr1);
     const uint32_t* in = p ? alive1 : alive0;
     const uint32_t na = sc->alive_count[p];
     uint32_t mn = 0xFFFFFFFFu;
@@ -258,12 +273,13 @@ __global__ void __launch_bounds__(256) k_core_min(LoopScalars* sc, const uint32_
 // kernels.cuh:549-562).
 __global__ void __launch_bounds__(256) k_core_mark(LoopScalars* sc, const uint32_t* __restrict__ tri,
                                                    uint8_t* __restrict__ state, uint32_t* __restrict__ core,
-                                                   uint32_t* alive0, uint32_t* alive1,
-                                                   uint32_t* __restrict__ frontier, uint32_t* __restrict__ item_x,
+                                                   uint32_t* alive0, uint32_t* alive1, uint32_t* fr0, uint32_t* fr1,
+                                                   uint32_t* __restrict__ item_x,
                                                    uint32_t* __restrict__ item_c, const uint32_t* __restrict__ rowptr,
                                                    const uint32_t* __restrict__ in_ptr,
                                                    const unsigned long long* __restrict__ inc_ptr) {
     const uint32_t p = sc->parity;
+    uint32_t* frontier = (sc->round & 1) ? fr1 : fr0;
     const uint32_t* in = p ? alive1 : alive0;
     uint32_t* outl = p ? alive0 : alive1;
     const uint32_t na = sc->alive_count[p];
@@ -288,6 +304,100 @@ __global__ void __launch_bounds__(256) k_core_mark(LoopScalars* sc, const uint32
     }
 }
 
+// Independent bound on the loop: block 0 of the update kernel counts every round started; past max_rounds + 1 the
+// loop is forced to stop even if the round bookkeeping were broken (a WHILE node keeps its last condition otherwise).
+__device__ __forceinline__ void count_iteration(LoopScalars* sc, cudaGraphConditionalHandle handle, int use_handle) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const uint32_t it = atomicAdd(&sc->iters, 1u) + 1;
+        if (it > sc->max_rounds + 1) {
+            atomicMax(&sc->status, (uint32_t)LS_ROUND_LIMIT);
+            sc->cont = 0;
+            if (use_handle) cudaGraphSetConditional(handle, 0);
+        }
+    }
+}
+
+// The last block of the update kernel to finish closes the round: nalive -= |F|, T -= destroyed, the checks of
+// densest.h:298 / dsg.h:744, per-graph closing of a batch, reset of the per-round counters, the alive-list parity
+// flip and the loop condition (cudaGraphSetConditional when running as a graph body). The frontier itself is retired
+// by the next round's first kernel (retire_previous).
+__device__ __forceinline__ void close_round_if_last(LoopScalars* sc, int kind, cudaGraphConditionalHandle handle,
+                                                    int use_handle, const Segs& sg) {
+    __shared__ bool s_last;
+    __shared__ unsigned long long s_alive[32];
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(&sc->done_blocks, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const uint32_t F = sc->fcount;
+    // every graph of a batch closes its own round (all threads of the last block): removed and destroyed counts,
+    // the checks of densest.h:298, then peel_improves for the alive set the next round starts from
+    unsigned long long alive = 0;
+    if (sg.count) {
+        const uint32_t ran = sc->round;
+        for (uint32_t s = threadIdx.x; s < sg.count; s += blockDim.x) {
+            if (sg.status[s] == LS_OK && sg.nalive[s] > 0) {
+                const unsigned long long rem = sg.removed[s], des = sg.destroyed[s];
+                uint32_t st = LS_OK;
+                if (rem == 0) st = LS_NO_PROGRESS;
+                if (rem > sg.nalive[s] || des > sg.T[s]) st = LS_OVER_REMOVED;
+                const unsigned long long na = sg.nalive[s] - min(rem, sg.nalive[s]);
+                const unsigned long long T = sg.T[s] - min(des, sg.T[s]);
+                sg.nalive[s] = na;
+                sg.T[s] = T;
+                sg.rounds[s] = ran + 1;
+                if (st == LS_OK && na > 0 && ran + 1 >= sc->max_rounds) st = LS_ROUND_LIMIT;
+                if (st == LS_OK && na > 0 && (sg.best_den[s] == 0 || T * sg.best_den[s] > sg.best_num[s] * na)) {
+                    sg.best_num[s] = T;
+                    sg.best_den[s] = na;
+                    sg.best_round[s] = ran + 1;
+                }
+                sg.status[s] = st;
+                if (st == LS_OK) alive += na;
+            }
+            sg.removed[s] = 0;
+            sg.destroyed[s] = 0;
+        }
+        alive = warp_sum_u64(alive);
+        if ((threadIdx.x & 31) == 0) s_alive[threadIdx.x >> 5] = alive;
+        __syncthreads();
+        alive = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) alive += s_alive[w];
+    }
+    if (threadIdx.x != 0) return;
+    LoopScalars s = *sc;   // written by earlier kernels of this round and by this kernel's blocks (fenced above)
+    uint32_t status = s.status;
+    if (sg.count) {
+        s.nalive = alive;
+    } else {
+        if (F == 0 && s.nalive > 0) status = LS_NO_PROGRESS;
+        if (F > s.nalive) status = LS_OVER_REMOVED;
+        if (s.destroyed > s.T) status = LS_OVER_REMOVED;
+        s.nalive -= min((unsigned long long)F, s.nalive);
+        s.T -= min(s.destroyed, s.T);
+    }
+    if (kind == LOOP_CORE) {
+        if (s.kround < s.kcur) status = LS_LEVEL_DOWN;
+        s.kcur = s.kround;
+    }
+    s.round += 1;
+    s.parity ^= 1;
+    s.alive_count[s.parity ^ 1] = 0;   // the next round's output list
+    s.fprev = F;
+    s.fcount = 0;
+    s.nitems = 0;
+    s.destroyed = 0;
+    s.done_blocks = 0;
+    s.min_tri = 0xFFFFFFFFu;
+    if (status == LS_OK && s.nalive > 0 && s.round >= s.max_rounds) status = LS_ROUND_LIMIT;
+    s.status = status;
+    s.cont = (status == LS_OK && s.nalive > 0 && s.iters <= s.max_rounds) ? 1u : 0u;
+    *sc = s;
+    if (use_handle) cudaGraphSetConditional(handle, s.cont);
+}
+
 // Enumerates the triangles through the frontier vertices (see the file comment). One warp per item = up to kChunk
 // consecutive entries of the virtual neighbour list N(x) = [N+(x) | In(x)]. Vertices with deg(x) <= kChunk use a
 // per-warp shared hash set of their live neighbours; larger ones test an edge {x, w} by binary search in the sorted
@@ -295,8 +405,10 @@ __global__ void __launch_bounds__(256) k_core_mark(LoopScalars* sc, const uint32
 __global__ void __launch_bounds__(kUpdWarps * 32) k_frontier_update(
     LoopScalars* sc, const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ col,
     const uint32_t* __restrict__ in_ptr, const uint32_t* __restrict__ in_src, const uint32_t* __restrict__ item_x,
-    const uint32_t* __restrict__ item_c, const uint8_t* __restrict__ state, uint32_t* __restrict__ tri, Segs sg) {
+    const uint32_t* __restrict__ item_c, const uint8_t* __restrict__ state, uint32_t* __restrict__ tri, Segs sg,
+    int kind, cudaGraphConditionalHandle handle, int use_handle) {
     constexpr uint32_t kSlots = 2 * kChunk;   // 512 slots, load <= 1/2
+    count_iteration(sc, handle, use_handle);
     constexpr uint32_t kBits = 9;
     __shared__ uint32_t s_key[kUpdWarps][kSlots];
     __shared__ uint32_t s_incl[kUpdWarps][32], s_rb[kUpdWarps][32], s_y[kUpdWarps][32];
@@ -393,6 +505,7 @@ __global__ void __launch_bounds__(kUpdWarps * 32) k_frontier_update(
         for (int i = 0; i < kUpdWarps; i++) t += s_red[i];
         if (t) atomicAdd(&sc->destroyed, t);
     }
+    close_round_if_last(sc, kind, handle, use_handle, sg);
 }
 
 // Incidence-list update: one warp per item = up to kListChunk entries (y, w) of frontier vertex x's list, read
@@ -404,8 +517,10 @@ __global__ void __launch_bounds__(256) k_frontier_update_list(LoopScalars* sc, c
                                                               const uint32_t* __restrict__ item_x,
                                                               const uint32_t* __restrict__ item_c,
                                                               const uint8_t* __restrict__ state,
-                                                              uint32_t* __restrict__ tri, Segs sg) {
+                                                              uint32_t* __restrict__ tri, Segs sg, int kind,
+                                                              cudaGraphConditionalHandle handle, int use_handle) {
     __shared__ unsigned long long s_red[8];
+    count_iteration(sc, handle, use_handle);
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t nitems = sc->nitems;
     const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -437,99 +552,7 @@ __global__ void __launch_bounds__(256) k_frontier_update_list(LoopScalars* sc, c
         for (int i = 0; i < 8; i++) t += s_red[i];
         if (t) atomicAdd(&sc->destroyed, t);
     }
-}
-
-// Retires the frontier (state 2 -> 0); the last block to finish closes the round: nalive -= |F|, T -= destroyed,
-// checks (densest.h:298, dsg.h:744), resets the per-round counters, flips the alive-list parity and sets the loop
-// condition (cudaGraphSetConditional when running as a graph body).
-template <int KIND>
-__global__ void __launch_bounds__(256) k_retire_tail(LoopScalars* sc, uint8_t* __restrict__ state,
-                                                     const uint32_t* __restrict__ frontier,
-                                                     cudaGraphConditionalHandle handle, int use_handle, Segs sg) {
-    __shared__ bool s_last;
-    __shared__ unsigned long long s_alive[8];
-    const uint32_t F = sc->fcount;
-    // independent bound: block 0 counts every execution of this kernel; past max_rounds + 1 the loop is forced to
-    // stop even if the round bookkeeping below were broken (a WHILE node keeps its last condition value otherwise)
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        const uint32_t it = atomicAdd(&sc->iters, 1u) + 1;
-        if (it > sc->max_rounds + 1) {
-            atomicMax(&sc->status, (uint32_t)LS_ROUND_LIMIT);
-            sc->cont = 0;
-            if (use_handle) cudaGraphSetConditional(handle, 0);
-        }
-    }
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x)
-        state[frontier[i]] = 0;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) s_last = atomicAdd(&sc->done_blocks, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    // every graph of a batch closes its own round (all threads of the last block): removed and destroyed counts,
-    // the checks of densest.h:298, then peel_improves for the alive set the next round starts from
-    unsigned long long alive = 0;
-    if (sg.count) {
-        const uint32_t ran = sc->round;
-        for (uint32_t s = threadIdx.x; s < sg.count; s += blockDim.x) {
-            if (sg.status[s] == LS_OK && sg.nalive[s] > 0) {
-                const unsigned long long rem = sg.removed[s], des = sg.destroyed[s];
-                uint32_t st = LS_OK;
-                if (rem == 0) st = LS_NO_PROGRESS;
-                if (rem > sg.nalive[s] || des > sg.T[s]) st = LS_OVER_REMOVED;
-                const unsigned long long na = sg.nalive[s] - min(rem, sg.nalive[s]);
-                const unsigned long long T = sg.T[s] - min(des, sg.T[s]);
-                sg.nalive[s] = na;
-                sg.T[s] = T;
-                sg.rounds[s] = ran + 1;
-                if (st == LS_OK && na > 0 && ran + 1 >= sc->max_rounds) st = LS_ROUND_LIMIT;
-                if (st == LS_OK && na > 0 && (sg.best_den[s] == 0 || T * sg.best_den[s] > sg.best_num[s] * na)) {
-                    sg.best_num[s] = T;
-                    sg.best_den[s] = na;
-                    sg.best_round[s] = ran + 1;
-                }
-                sg.status[s] = st;
-                if (st == LS_OK) alive += na;
-            }
-            sg.removed[s] = 0;
-            sg.destroyed[s] = 0;
-        }
-        alive = warp_sum_u64(alive);
-        if ((threadIdx.x & 31) == 0) s_alive[threadIdx.x >> 5] = alive;
-        __syncthreads();
-        alive = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) alive += s_alive[w];
-    }
-    if (threadIdx.x != 0) return;
-    LoopScalars s = *sc;   // written by earlier kernels of this round (visible at the kernel boundary)
-    uint32_t status = s.status;
-    if (sg.count) {
-        s.nalive = alive;
-    } else {
-        if (F == 0 && s.nalive > 0) status = LS_NO_PROGRESS;
-        if (F > s.nalive) status = LS_OVER_REMOVED;
-        if (s.destroyed > s.T) status = LS_OVER_REMOVED;
-        s.nalive -= min((unsigned long long)F, s.nalive);
-        s.T -= min(s.destroyed, s.T);
-    }
-    if (KIND == LOOP_CORE) {
-        if (s.kround < s.kcur) status = LS_LEVEL_DOWN;
-        s.kcur = s.kround;
-    }
-    s.round += 1;
-    s.parity ^= 1;
-    s.alive_count[s.parity ^ 1] = 0;   // the next round's output list
-    s.fcount = 0;
-    s.nitems = 0;
-    s.destroyed = 0;
-    s.done_blocks = 0;
-    s.min_tri = 0xFFFFFFFFu;
-    if (status == LS_OK && s.nalive > 0 && s.round >= s.max_rounds) status = LS_ROUND_LIMIT;
-    s.status = status;
-    s.cont = (status == LS_OK && s.nalive > 0 && s.iters <= s.max_rounds) ? 1u : 0u;
-    *sc = s;
-    if (use_handle) cudaGraphSetConditional(handle, s.cont);
+    close_round_if_last(sc, kind, handle, use_handle, sg);
 }
 
 // Per graph: T0 = (sum of its vertices' triangle counts) / 3. One block per graph.
@@ -580,7 +603,8 @@ static ga_status ensure_loops(ga_graph* g) {
     GA_TRY(dalloc(g, &L->out, n));
     GA_TRY(dalloc(g, &L->alive[0], n));
     GA_TRY(dalloc(g, &L->alive[1], n));
-    GA_TRY(dalloc(g, &L->frontier, n));
+    GA_TRY(dalloc(g, &L->frontier[0], n));
+    GA_TRY(dalloc(g, &L->frontier[1], n));
     // every vertex enters one frontier per run and brings ceil(deg / kChunk) items
     L->item_cap = (uint64_t)n + (2ull * g->m) / kChunk + 1;
     GA_TRY(dalloc(g, &L->item_x, L->item_cap));
@@ -607,7 +631,6 @@ static ga_status ensure_loops(ga_graph* g) {
     GA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_frontier_update, kUpdWarps * 32, 0));
     L->grid_scan = (unsigned)g->sm_count * 4;
     L->grid_update = (unsigned)g->sm_count * (unsigned)std::max(occ, 1);
-    L->grid_retire = (unsigned)g->sm_count;
     return GA_OK;
 }
 
@@ -628,7 +651,8 @@ void reset_loops(ga_graph* g) {
     ga_loops* L = g->loops;
     if (!L) return;
     cudaStreamSynchronize(g->stream);
-    void* bufs[] = {L->tri, L->state, L->out, L->alive[0], L->alive[1], L->frontier, L->item_x, L->item_c, L->sc,
+    void* bufs[] = {L->tri, L->state, L->out, L->alive[0], L->alive[1], L->frontier[0], L->frontier[1], L->item_x,
+                    L->item_c, L->sc,
                     L->inc, L->inc_ptr, L->segs.T, L->segs.nalive, L->segs.removed, L->segs.destroyed,
                     L->segs.best_num, L->segs.best_den, L->segs.T0, L->segs.best_round, L->segs.rounds,
                     L->segs.status};
@@ -712,20 +736,24 @@ static ga_status enqueue_round(ga_graph* g, cudaStream_t st, cudaGraphConditiona
     const unsigned long long* inc_ptr = L->lists == 1 ? L->inc_ptr : nullptr;
     const Segs sg = KIND == LOOP_PEEL ? L->segs : Segs{};
     if (KIND == LOOP_PEEL) {
-        k_peel_mark<<<L->grid_scan, 256, 0, st>>>(L->sc, L->tri, L->state, L->out, L->alive[0], L->alive[1], L->frontier,
-                                             L->item_x, L->item_c, g->rowptr, g->in_ptr, inc_ptr, sg);
+        k_peel_mark<<<L->grid_scan, 256, 0, st>>>(L->sc, L->tri, L->state, L->out, L->alive[0], L->alive[1],
+                                                  L->frontier[0], L->frontier[1], L->item_x, L->item_c, g->rowptr,
+                                                  g->in_ptr, inc_ptr, sg);
     } else {
-        k_core_min<<<L->grid_scan, 256, 0, st>>>(L->sc, L->tri, L->alive[0], L->alive[1]);
-        k_core_mark<<<L->grid_scan, 256, 0, st>>>(L->sc, L->tri, L->state, L->out, L->alive[0], L->alive[1], L->frontier,
-                                             L->item_x, L->item_c, g->rowptr, g->in_ptr, inc_ptr);
+        k_core_min<<<L->grid_scan, 256, 0, st>>>(L->sc, L->tri, L->alive[0], L->alive[1], L->state, L->frontier[0],
+                                                 L->frontier[1]);
+        k_core_mark<<<L->grid_scan, 256, 0, st>>>(L->sc, L->tri, L->state, L->out, L->alive[0], L->alive[1],
+                                                  L->frontier[0], L->frontier[1], L->item_x, L->item_c, g->rowptr,
+                                                  g->in_ptr, inc_ptr);
     }
+    // the update kernel's last block closes the round and sets the loop condition
     if (L->lists == 1)
         k_frontier_update_list<<<L->grid_update, 256, 0, st>>>(L->sc, L->inc, L->inc_ptr, L->item_x, L->item_c,
-                                                               L->state, L->tri, sg);
+                                                               L->state, L->tri, sg, KIND, h, use_h);
     else
         k_frontier_update<<<L->grid_update, kUpdWarps * 32, 0, st>>>(L->sc, g->rowptr, g->col, g->in_ptr, g->in_src,
-                                                                L->item_x, L->item_c, L->state, L->tri, sg);
-    k_retire_tail<KIND><<<L->grid_retire, 256, 0, st>>>(L->sc, L->state, L->frontier, h, use_h, sg);
+                                                                L->item_x, L->item_c, L->state, L->tri, sg, KIND,
+                                                                h, use_h);
     GA_CUDA(cudaGetLastError());
     return GA_OK;
 }
