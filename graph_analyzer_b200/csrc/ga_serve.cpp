@@ -278,11 +278,10 @@ void run_folded(ga_server* s, cudaStream_t st, std::vector<Request*>& rs, std::v
 
 void worker_main(ga_server* s, bool small_only) {
     cudaSetDevice(s->cfg.device);
-    // the small lane's blocks are dispatched first whenever SMs free up, so short requests overtake long kernels
-    int least = 0, greatest = 0;
-    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    // all lanes at the same stream priority: a higher one for the small lane starved the many short kernels of
+    // the general lane's peeling and core loops (each round waits for SMs), 4x slower core requests when measured
     cudaStream_t st;
-    if (cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, small_only ? greatest : least) != cudaSuccess) return;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return;
     for (;;) {
         Work w;
         {
