@@ -451,7 +451,9 @@ ga_status run_tc(ga_graph* g, const TcArgs<CT>& a, bool zero_outputs) {
         if (MODE == TC_VSUP && g->n) GA_CUDA(cudaMemsetAsync(a.vsup, 0, (size_t)g->n * sizeof(CT), st));
         if (MODE == TC_ESUP && g->m) GA_CUDA(cudaMemsetAsync(a.esup, 0, (size_t)g->m * sizeof(uint32_t), st));
     }
-    const int64_t kernel = g->opt_tc_kernel ? g->opt_tc_kernel : g->tuned_kernel;
+    // automatic choice: the autotuned kernel, except for the incidence lists, whose per-triangle list appends
+    // contend on hub vertices in the one-thread-per-edge form (Holme-Kim 1.7M: 154 ms plain vs 4 ms hash)
+    const int64_t kernel = g->opt_tc_kernel ? g->opt_tc_kernel : (MODE == TC_LIST ? 2 : g->tuned_kernel);
     if (kernel == 1) return launch_plain<MODE, ALIVE, CT>(g, a);
     if (g->heavy.count == 0 && g->light.count == 0) return GA_OK;
     return launch_hash<MODE, ALIVE, CT>(g, a);
