@@ -561,9 +561,10 @@ def _fifo_latency(service_s, arrivals_s):
 
 def run_serve(args):
     """Serving: open-loop Poisson arrivals (rate swept) into the request loop (admission under a 150 GB HBM budget,
-    resident graphs for re-queries, small requests folded into batch launches, 4 concurrent streams), against serial
-    plain launches (one request at a time: uploaded, counted with the one-thread-per-edge kernel, its peeling or core
-    rounds driven from the host, freed).
+    resident graphs for re-queries, small requests folded into batch launches, 4 + 2 concurrent streams), against
+    serial plain launches of the same library (one request at a time: uploaded, counted with the kernel the autotuner
+    picks, its peeling or core rounds driven from the host, freed), so the comparison isolates what the serving loop
+    adds: concurrency, residency, folding and page-locked uploads.
     Results of every request must be identical in both."""
     import torch
     import graph_analyzer_b200 as ga
@@ -578,8 +579,7 @@ def run_serve(args):
     for gi, kind in trace:
         t0 = time.perf_counter()
         with ga.DeviceGraph(graphs[gi]) as d:
-            for opt, v in ((ga.OPT_TC_KERNEL, 1), (ga.OPT_LOOP_MODE, 1)):
-                d.set_option(opt, v)
+            d.set_option(ga.OPT_LOOP_MODE, 1)
             if kind == ga.REQ_TC:
                 val = (d.tc_count(),)
             elif kind == ga.REQ_PEEL:
