@@ -156,3 +156,47 @@ def test_lists_reused_across_calls(ga, oracle, cuda_ok):
         d.set_option(ga.OPT_UPDATE_MODE, 1)                      # switching frees them
         _core_eq(oracle, g, d)
         assert d.device_bytes() < b1
+
+
+def _ties():
+    import json
+    import os
+
+    from conftest import GOLDEN
+    with open(os.path.join(GOLDEN, "ties.json")) as f:
+        return json.load(f)["graphs"]
+
+
+@pytest.mark.parametrize("mode", list(MODES))
+def test_density_ties_match_reference(ga, cuda_ok, mode):
+    """Graphs whose peeling meets one density in two rounds: best_round follows the strict improvement rule
+    (densest.h:76-78); expected outputs are the reference's own (tests/golden/ties.json)."""
+    for t in _ties():
+        g = ga.build_graph_from_edges(t["n"], np.array(t["pairs"], np.uint32).reshape(-1, 2))
+        with ga.DeviceGraph(g) as d:
+            _set_mode(ga, d, mode)
+            assert d.tc_count() == t["triangles"]
+            for key, want in t["peel"].items():
+                num, den = map(int, key.split("/"))
+                r = d.batch_peel(num, den)
+                assert (r.best_num, r.best_den, r.best_round, r.rounds) == (
+                    want["best_num"], want["best_den"], want["best_round"], want["rounds"]), key
+                assert r.removed_round.tolist() == want["removed_round"]
+            c = d.core_decomposition()
+            assert (c.kmax, c.rounds, c.core.tolist()) == (t["kmax"], t["core_rounds"], t["core"])
+
+
+def test_density_ties_in_one_batch(ga, cuda_ok):
+    ties = _ties()
+    graphs = [ga.build_graph_from_edges(t["n"], np.array(t["pairs"], np.uint32).reshape(-1, 2)) for t in ties]
+    b = ga.pack_batch(graphs)
+    with ga.DeviceBatch(b) as db:
+        for key in ties[0]["peel"]:
+            num, den = map(int, key.split("/"))
+            r = db.tc_peel(num, den)
+            for i, t in enumerate(ties):
+                want = t["peel"][key]
+                got = r.result(b, i)
+                assert (got.best_num, got.best_den, got.best_round, got.rounds) == (
+                    want["best_num"], want["best_den"], want["best_round"], want["rounds"]), (i, key)
+                assert got.removed_round.tolist() == want["removed_round"]

@@ -10,11 +10,13 @@
 from __future__ import annotations
 
 import itertools
+import json
+import os
 
 import numpy as np
 import pytest
 
-from conftest import FIXTURES, fixture_path, golden_arrays, hub_pairs, random_pairs
+from conftest import FIXTURES, GOLDEN, fixture_path, golden_arrays, hub_pairs, random_pairs
 
 EPS = [(1, 10), (1, 1), (0, 1), (3, 7), (1, 20), (1, 2)]
 
@@ -164,3 +166,25 @@ def test_oracle_against_brute_force(oracle, seed):
     assert T == T2 and np.array_equal(tri, tri2)
     core, _ = oracle.core_decomposition(g)
     assert np.array_equal(core, _brute_cores(n, edges))
+
+
+def _ties():
+    with open(os.path.join(GOLDEN, "ties.json")) as f:
+        return json.load(f)["graphs"]
+
+
+@pytest.mark.parametrize("i", range(8))
+def test_oracle_matches_reference_on_density_ties(oracle, i):
+    """ties.json: outputs of the reference's own code on graphs where peeling meets one density twice (the strict
+    improvement rule of densest.h:76-78 decides best_round)."""
+    t = _ties()[i]
+    g = oracle.build_graph_from_edges(t["n"], np.array(t["pairs"], np.uint32).reshape(-1, 2))
+    assert oracle.triangles_serial(g) == t["triangles"]
+    for key, want in t["peel"].items():
+        num, den = map(int, key.split("/"))
+        r = oracle.batch_peel(g, num, den)
+        assert (r.best_num, r.best_den, r.best_round, r.rounds) == (want["best_num"], want["best_den"],
+                                                                    want["best_round"], want["rounds"])
+        assert r.removed_round.tolist() == want["removed_round"]
+    core, kmax, rounds = oracle.core_levels(g)
+    assert (kmax, rounds, core.tolist()) == (t["kmax"], t["core_rounds"], t["core"])
