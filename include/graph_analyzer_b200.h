@@ -269,7 +269,8 @@ ga_status ga_core_decomposition(ga_graph* g, uint32_t* core, ga_core_result* res
  * requests overlap on the device. Graphs stay resident after a request (re-queries skip the upload and the derived
  * index) until the budget needs their memory (least recently used first). Small count/peel requests that are queued
  * together are folded into one batch launch (ga_batch). Every request's result equals the result of running it
- * alone. */
+ * alone. The ga_server_* calls may come from any host threads concurrently (one internal lock); the server owns the
+ * device memory of its graphs, so a registered graph is not also used through a ga_graph handle. */
 typedef struct ga_server ga_server;
 
 typedef struct ga_server_config {
