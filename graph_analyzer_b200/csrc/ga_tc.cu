@@ -451,9 +451,10 @@ ga_status run_tc(ga_graph* g, const TcArgs<CT>& a, bool zero_outputs) {
         if (MODE == TC_VSUP && g->n) GA_CUDA(cudaMemsetAsync(a.vsup, 0, (size_t)g->n * sizeof(CT), st));
         if (MODE == TC_ESUP && g->m) GA_CUDA(cudaMemsetAsync(a.esup, 0, (size_t)g->m * sizeof(uint32_t), st));
     }
-    // automatic choice: the autotuned kernel, except for the incidence lists, whose per-triangle list appends
-    // contend on hub vertices in the one-thread-per-edge form (Holme-Kim 1.7M: 154 ms plain vs 4 ms hash)
-    const int64_t kernel = g->opt_tc_kernel ? g->opt_tc_kernel : (MODE == TC_LIST ? 2 : g->tuned_kernel);
+    // automatic choice: the autotuned kernel for counts; the hash kernel for supports and incidence lists, whose
+    // per-triangle appends and increments contend on hub vertices in the one-thread-per-edge form (lists of the
+    // Holme-Kim 1.7M graph: 154 ms plain vs 4 ms hash; first peel of the 4,096-graph batch: 3.2 s vs 1.1 s)
+    const int64_t kernel = g->opt_tc_kernel ? g->opt_tc_kernel : (MODE == TC_COUNT ? g->tuned_kernel : 2);
     if (kernel == 1) return launch_plain<MODE, ALIVE, CT>(g, a);
     if (g->heavy.count == 0 && g->light.count == 0) return GA_OK;
     return launch_hash<MODE, ALIVE, CT>(g, a);
@@ -465,7 +466,7 @@ ga_status run_tc(ga_graph* g, const TcArgs<CT>& a, bool zero_outputs) {
 // kernel wins by several times. The choice is cached per degree-distribution signature: log2 of n and m and the
 // fraction of edges whose source has out-degree in each log2 bucket, in sixteenths. A signature seen before is
 // answered from the cache (process-wide; also kept in the file named by GA_TUNE_CACHE when that is set); a new one
-// is decided by timing both kernels on the graph (each after one untimed launch).
+// is decided by timing both kernels once on the graph (their code loaded beforehand).
 
 __global__ void k_degree_hist(const uint32_t* __restrict__ rowptr, uint32_t n, unsigned long long* hist) {
     __shared__ unsigned long long s_h[33];
@@ -550,11 +551,12 @@ ga_status autotune(ga_graph* g) {
     TcArgs<unsigned int> a{};
     a.total = g->d_scalars + 2;
     ga_status s = GA_OK;
+    // a kernel's first launch in the process would also load its code (lazy module loading): load both first
+    cudaFuncAttributes fa;
+    cudaFuncGetAttributes(&fa, k_tc_hash<TC_COUNT, false, unsigned int>);
+    cudaFuncGetAttributes(&fa, k_tc_plain<TC_COUNT, false, unsigned int>);
     for (int k = 1; k <= 2 && s == GA_OK; k++) {
         g->tuned_kernel = k;
-        // one untimed launch first: a kernel's first launch in the process also loads its code
-        s = run_tc<TC_COUNT, false, unsigned int>(g, a, true);
-        if (s != GA_OK) break;
         cudaEventRecord(e0, st);
         s = run_tc<TC_COUNT, false, unsigned int>(g, a, true);
         cudaEventRecord(e1, st);

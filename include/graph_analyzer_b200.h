@@ -162,7 +162,8 @@ ga_status ga_graph_prepare(ga_graph* g);
 /* Tuning knobs (the reference's compile-time macros SM_CAP / HASH_SLOTS / TASK_CHUNK, kernels.cuh:23-34, become
  * run-time options; GA_OPT_*_AUTO lets the autotuner choose). */
 typedef enum ga_option {
-    GA_OPT_TC_KERNEL = 1,     /* 0 auto, 1 plain merge (one thread per oriented edge), 2 degree-binned hash probe */
+    GA_OPT_TC_KERNEL = 1,     /* 0 auto (counts: the autotuned kernel; supports and incidence lists: the hash
+                                 kernel), 1 plain merge (one thread per oriented edge), 2 degree-binned hash probe */
     GA_OPT_LOOP_MODE = 2,     /* 0 auto, 1 host-driven rounds (one sync per round), 2 CUDA graph with a device
                                  while-node (no host sync inside the loop)                                          */
     GA_OPT_MAX_ROUNDS = 3,    /* round cap of device-resident loops (0 = n + 1)                                    */
