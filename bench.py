@@ -571,11 +571,11 @@ def run_serve(args):
     R = args.requests
     rng = np.random.default_rng(SEED)
     graphs, trace = _serve_trace(ga, R, rng)
+    # warm-up, untimed: one pass of the whole trace through a server fills the kernel-choice cache (one timing per
+    # degree-distribution signature) and the memory pool, so neither side below pays those first-time costs
+    _serve_run(ga, graphs, trace, np.zeros(R), args.slots)
     # serial plain launches: measured service time of every request in trace order
     service, plain_vals = [], []
-    for gi, kind in trace[: min(R, 8)]:                                 # warm-up (module load, pools)
-        with ga.DeviceGraph(graphs[gi]) as d:
-            d.tc_count()
     for gi, kind in trace:
         t0 = time.perf_counter()
         with ga.DeviceGraph(graphs[gi]) as d:
@@ -591,8 +591,11 @@ def run_serve(args):
         service.append(time.perf_counter() - t0)
         plain_vals.append(val)
     serial_s = float(sum(service))
-    # closed-loop burst (all requests at t = 0): the server's capacity; also warms the kernel-choice cache
-    lat, res, wall, st = _serve_run(ga, graphs, trace, np.zeros(R), args.slots)
+    # closed-loop bursts (all requests at t = 0): the server's capacity, median of three runs (run-to-run spread on a
+    # shared host is large; every run is reported)
+    bursts = [_serve_run(ga, graphs, trace, np.zeros(R), args.slots) for _ in range(3)]
+    walls = [b[2] for b in bursts]
+    lat, res, wall, st = bursts[int(np.argsort(walls)[1])]
     capacity = R / wall
     # where the time goes, per request class (graph family x kind): serial service vs the server's run time
     names = ("tc", "peel", "core")
@@ -605,9 +608,12 @@ def run_serve(args):
         e["server_run_ms"] += r.run_ms
     log("per class: " + json.dumps(by_class))
     identical = all(_serve_value(ga, k, r) == v and r.status == 0 for (_, k), r, v in zip(trace, res, plain_vals))
-    burst = {"req_s": capacity, "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-             "folded_launches": st["folded_launches"], "evictions": st["evictions"],
-             "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9}
+    for b in bursts:
+        identical &= all(_serve_value(ga, k, r) == v and r.status == 0
+                         for (_, k), r, v in zip(trace, b[1], plain_vals))
+    burst = {"req_s": capacity, "runs_req_s": [R / w for w in walls], "p50_ms": float(np.percentile(lat, 50)),
+             "p99_ms": float(np.percentile(lat, 99)), "folded_launches": st["folded_launches"],
+             "evictions": st["evictions"], "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9}
     sweep = []
     for frac in args.rate_fracs:
         rate = frac * capacity
