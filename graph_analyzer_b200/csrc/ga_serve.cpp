@@ -124,44 +124,43 @@ bool cheap(const ga_server* s, const Request& r, const GraphEntry& e) {
     return e.m <= s->cfg.fold_max_edges || (e.dev && r.kind == GA_REQ_TC);
 }
 
+// Bytes a request must reserve now (`need`) and its whole estimate (`full`), and whether it may be folded.
+void plan(const ga_server* s, const Request& r, const GraphEntry& e, uint64_t* need, uint64_t* full, bool* small) {
+    *small = r.kind != GA_REQ_CORE && !e.dev && e.m <= s->cfg.fold_max_edges && s->cfg.fold_max_graphs > 1;
+    // A loop on a large graph whose triangle count is unknown is admitted in two stages: first the upload and
+    // the count (reserving the graph's own bytes), then, with the count known, the loop state and incidence
+    // lists (run_single grows the reservation or puts the request back at the head of the queue).
+    const bool staged = r.kind != GA_REQ_TC && e.triangles == UINT64_MAX && !*small;
+    *full = estimate_bytes(e, staged ? GA_REQ_TC : r.kind);
+    // bytes to reserve: the whole estimate for an upload; for a resident graph only what a loop may still add
+    *need = 0;
+    if (!e.dev) *need = *full;
+    else if (r.kind != GA_REQ_TC) *need = *full > e.dev_bytes ? *full - e.dev_bytes : 0;
+}
+
+// Rough device work of a request, for ordering the general lane: edges times a factor per kind, plus the upload.
+uint64_t work_of(const Request& r, const GraphEntry& e) {
+    const uint64_t f = r.kind == GA_REQ_CORE ? 64 : (r.kind == GA_REQ_PEEL ? 8 : 1);
+    return (uint64_t)e.m * f + (e.dev ? 0 : e.m);
+}
+
 // Picks the next admissible work (caller holds the lock). Returns false when nothing can start now. Workers of the
-// small lane (`small_only`) take cheap requests only, so those never wait behind uploads and loops of large graphs.
+// small lane (`small_only`) take cheap requests only, first come first served, so those never wait behind uploads
+// and loops of large graphs. The general lane takes the largest admissible request first (largest work first keeps
+// the makespan and the tail of a burst short: a long request that starts last would end last), falling back to
+// queue order when only an eviction can make room.
 bool take_work(ga_server* s, Work* w, bool small_only) {
-    for (auto it = s->queue.begin(); it != s->queue.end(); ++it) {
+    auto admit = [&](std::deque<uint64_t>::iterator it, uint64_t need, bool small) {
         Request& r = s->requests[*it];
         GraphEntry& e = s->graphs[r.gid];
-        if (e.busy || (small_only && !cheap(s, r, e))) continue;
-        const bool small = r.kind != GA_REQ_CORE && !e.dev && e.m <= s->cfg.fold_max_edges &&
-                           s->cfg.fold_max_graphs > 1;
-        // A loop on a large graph whose triangle count is unknown is admitted in two stages: first the upload and
-        // the count (reserving the graph's own bytes), then, with the count known, the loop state and incidence
-        // lists (run_single grows the reservation or puts the request back at the head of the queue).
-        const bool staged = r.kind != GA_REQ_TC && e.triangles == UINT64_MAX && !small;
-        const uint64_t full = estimate_bytes(e, staged ? GA_REQ_TC : r.kind);
-        // bytes to reserve: the whole estimate for an upload; for a resident graph only what a loop may still add
-        uint64_t need = 0;
-        if (!e.dev) need = full;
-        else if (r.kind != GA_REQ_TC) need = full > e.dev_bytes ? full - e.dev_bytes : 0;
-        if (full > s->cfg.hbm_budget_bytes) {
-            // can never fit: fail this request right away
-            r.result.status = ga::fail(GA_ERR_BUDGET, "request needs %llu bytes, budget %llu",
-                                       (unsigned long long)full, (unsigned long long)s->cfg.hbm_budget_bytes);
-            r.done = true;
-            r.started = r.finished = Clock::now();
-            s->stats.completed++;
-            s->queue.erase(it);
-            s->cv_done.notify_all();
-            return take_work(s, w, small_only);
-        }
-        if (s->reserved + need > s->cfg.hbm_budget_bytes && !make_room(s, need)) continue;
         w->tickets.assign(1, *it);
         w->reserve = need;
         e.busy = true;
-        auto first = it;
         if (small) {
             // fold other queued small requests of the same kind and eps on other idle, non-resident graphs
-            for (auto jt = std::next(first); jt != s->queue.end() && w->tickets.size() < s->cfg.fold_max_graphs;
+            for (auto jt = s->queue.begin(); jt != s->queue.end() && w->tickets.size() < s->cfg.fold_max_graphs;
                  ++jt) {
+                if (jt == it) continue;
                 Request& q = s->requests[*jt];
                 GraphEntry& f = s->graphs[q.gid];
                 if (q.kind != r.kind || f.busy || f.dev || f.m > s->cfg.fold_max_edges) continue;
@@ -177,6 +176,50 @@ bool take_work(ga_server* s, Work* w, bool small_only) {
         s->reserved += w->reserve;
         s->peak_reserved = std::max(s->peak_reserved, s->reserved);
         return true;
+    };
+    if (!small_only) {
+        // largest admissible request that fits without evicting anything
+        auto best = s->queue.end();
+        uint64_t best_work = 0, best_need = 0;
+        bool best_small = false;
+        for (auto it = s->queue.begin(); it != s->queue.end(); ++it) {
+            const Request& r = s->requests[*it];
+            const GraphEntry& e = s->graphs[r.gid];
+            if (e.busy) continue;
+            uint64_t need, full;
+            bool small;
+            plan(s, r, e, &need, &full, &small);
+            if (full > s->cfg.hbm_budget_bytes || s->reserved + need > s->cfg.hbm_budget_bytes) continue;
+            const uint64_t wk = work_of(r, e);
+            if (best == s->queue.end() || wk > best_work) {
+                best = it;
+                best_work = wk;
+                best_need = need;
+                best_small = small;
+            }
+        }
+        if (best != s->queue.end()) return admit(best, best_need, best_small);
+    }
+    for (auto it = s->queue.begin(); it != s->queue.end(); ++it) {
+        Request& r = s->requests[*it];
+        GraphEntry& e = s->graphs[r.gid];
+        if (e.busy || (small_only && !cheap(s, r, e))) continue;
+        uint64_t need, full;
+        bool small;
+        plan(s, r, e, &need, &full, &small);
+        if (full > s->cfg.hbm_budget_bytes) {
+            // can never fit: fail this request right away
+            r.result.status = ga::fail(GA_ERR_BUDGET, "request needs %llu bytes, budget %llu",
+                                       (unsigned long long)full, (unsigned long long)s->cfg.hbm_budget_bytes);
+            r.done = true;
+            r.started = r.finished = Clock::now();
+            s->stats.completed++;
+            s->queue.erase(it);
+            s->cv_done.notify_all();
+            return take_work(s, w, small_only);
+        }
+        if (s->reserved + need > s->cfg.hbm_budget_bytes && !make_room(s, need)) continue;
+        return admit(it, need, small);
     }
     return false;
 }
