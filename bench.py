@@ -14,8 +14,10 @@ Reported (one JSON line, rank 0):
   roofline     B_alg per launch / CUDA-event launch time vs the measured HBM copy bandwidth;
   cpu_baseline the reference's own cpu_triangles_omp (oracle/_ref, compiled from its sources) on the host cores.
 ``--impl reference`` times the reference's CPU implementation alone with the same metric.
-Multi-GPU (torchrun, one rank per GPU): replicas only - every rank counts its own copy of the graph, no collective
-on the data path; the max over ranks of the device time gives the whole-job value (weak scaling).
+Multi-GPU (torchrun, one rank per GPU): replicas by default - every rank counts its own copy of the graph, no
+collective on the data path; the max over ranks of the device time gives the whole-job value (weak scaling). With
+--shard the ranks count ONE graph together, rank r its shard r of N (ga_tc_count_shard), summed by one 8-byte
+all-reduce (strong scaling).
 """
 from __future__ import annotations
 
@@ -255,8 +257,10 @@ def run_ours(args):
     torch.cuda.synchronize(dev)
     prep_ms = (time.perf_counter() - t0) * 1e3
     T = dg.tc_count()
+    shard = dist is not None and args.shard   # strong scaling: rank r counts shard r of world, one sum at the end
+    count_async = ((lambda p: dg.tc_count_shard_async(rank, world, p)) if shard else dg.tc_count_async)
     for _ in range(args.warmup):
-        dg.tc_count_async(d_out.data_ptr())
+        count_async(d_out.data_ptr())
     torch.cuda.synchronize(dev)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     if dist:
@@ -267,17 +271,23 @@ def run_ours(args):
             with torch.cuda.stream(stream):
                 flush.zero_()                                   # L2 flush between steps (not timed)
             evs[s][0].record(stream)
-            dg.tc_count_async(d_out.data_ptr())
+            count_async(d_out.data_ptr())
             evs[s][1].record(stream)
         torch.cuda.synchronize(dev)
         time.sleep(0.25)
     if dist:
         dist.barrier()
     step_ms = [a.elapsed_time(b) for a, b in evs]
-    if int(d_out.item()) != T:
-        raise RuntimeError(f"count changed between launches: {d_out.item()} vs {T}")
+    if shard:
+        total = d_out.clone()
+        dist.all_reduce(total)   # the one exchange of a sharded count: 8 bytes
+        got = int(total.item())
+    else:
+        got = int(d_out.item())
+    if got != T:
+        raise RuntimeError(f"count changed between launches: {got} vs {T}")
     ms = max_over_ranks(dist, sum(step_ms) / len(step_ms), dev)
-    value = world * b_alg / (ms / 1e3) / 1e9
+    value = (1 if shard else world) * b_alg / (ms / 1e3) / 1e9
 
     # ---- end to end through the public API from pinned host memory ----
     rp_h = torch.from_numpy(g.rowptr.view(np.int32)).pin_memory()
@@ -293,7 +303,13 @@ def run_ours(args):
                                     C.byref(hd)))
         ga._check(h.ga_graph_prepare(hd))
         out = C.c_uint64(0)
-        ga._check(h.ga_tc_count(hd, C.byref(out)))
+        if shard:
+            ga._check(h.ga_tc_count_shard(hd, rank, world, C.byref(out)))
+            part = torch.tensor([out.value], dtype=torch.int64, device=dev)
+            dist.all_reduce(part)
+            out = C.c_uint64(int(part.item()))
+        else:
+            ga._check(h.ga_tc_count(hd, C.byref(out)))
         ga._check(h.ga_graph_destroy(hd))
         dt = time.perf_counter() - t0
         if out.value != T:
@@ -301,7 +317,7 @@ def run_ours(args):
         if s >= args.warmup:
             e2e_times.append(dt)
     e2e_ms = max_over_ranks(dist, 1e3 * sum(e2e_times) / len(e2e_times), dev)
-    e2e_value = world * b_alg / (e2e_ms / 1e3) / 1e9
+    e2e_value = (1 if shard else world) * b_alg / (e2e_ms / 1e3) / 1e9
 
     if rank != 0:
         dg.close()
@@ -315,12 +331,14 @@ def run_ours(args):
         raise RuntimeError(f"GPU count {T} differs from the reference CPU count {cpu['triangles']}")
     line = {
         "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "strong" if shard else "weak", "vs_baseline": None,
         "dtype": "u32", "data": "synthetic",
         "config": {"workload": f"rmat{args.scale}_tc", "n": g.n, "m": g.m, "edge_factor": EDGE_FACTOR, "seed": SEED,
                    "rmat_abc": list(RMAT), "triangles": T, "b_alg_bytes": b_alg, "prep_ms": prep_ms,
                    "l2": f"256 MiB written between steps (untimed); col alone is {4 * g.m / 1e6:.0f} MB",
-                   "parallelism": f"replicas x{world}", "oriented_edges_per_s": world * g.m / (ms / 1e3)},
+                   "parallelism": f"shards x{world} (one 8-byte all-reduce)" if shard else f"replicas x{world}",
+                   "oriented_edges_per_s": (1 if shard else world) * g.m / (ms / 1e3)},
         "e2e": {"value": e2e_value, "unit": "GB/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(rp_h.numel() * 4 + col_h.numel() * 4), "d2h_bytes_per_step": 8,
                 "path": "ga_graph_create + ga_graph_prepare + ga_tc_count + ga_graph_destroy"},
@@ -724,6 +742,8 @@ def main():
                     default="rmat22",
                     help="rmat22 (default, the headline line) or a secondary workload")
     ap.add_argument("--graphs", type=int, default=4096, help="graphs in the batch workload")
+    ap.add_argument("--shard", action="store_true",
+                    help="with N > 1 GPUs: count ONE graph split into N shards (strong scaling) instead of N replicas")
     ap.add_argument("--scale", type=int, default=SCALE,
                     help="R-MAT scale of the headline workload (22; smaller only for quick checks)")
     ap.add_argument("--requests", type=int, default=600, help="requests in the serve workload")

@@ -131,6 +131,8 @@ SIGNATURES: dict[str, list] = {
     "ga_graph_set_option": [_vp, C.c_int, C.c_int64],
     "ga_tc_count": [_vp, C.POINTER(C.c_uint64)],
     "ga_tc_count_async": [_vp, _vp],
+    "ga_tc_count_shard": [_vp, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64)],
+    "ga_tc_count_shard_async": [_vp, C.c_uint32, C.c_uint32, _vp],
     "ga_tc_support_edges": [_vp, _vp, C.POINTER(C.c_uint64)],
     "ga_tc_support_edges_device": [_vp, _vp, C.POINTER(C.c_uint64)],
     "ga_tc_support_vertices": [_vp, _vp, C.POINTER(C.c_uint64)],
@@ -437,6 +439,15 @@ class DeviceGraph:
         t = C.c_uint64(0)
         _check(lib().ga_tc_count(self._h, C.byref(t)))
         return t.value
+
+    def tc_count_shard(self, shard: int, nshards: int) -> int:
+        """Triangles of shard `shard` of `nshards`; the shards' sum is tc_count()."""
+        t = C.c_uint64(0)
+        _check(lib().ga_tc_count_shard(self._h, shard, nshards, C.byref(t)))
+        return t.value
+
+    def tc_count_shard_async(self, shard: int, nshards: int, d_out: int) -> None:
+        _check(lib().ga_tc_count_shard_async(self._h, shard, nshards, d_out))
 
     def tc_count_async(self, d_out: int) -> None:
         """Enqueues the count on the graph's stream; the result lands in 8 bytes of device memory at d_out."""

@@ -358,9 +358,10 @@ __global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const ui
 template <int MODE, bool ALIVE, class CT>
 __global__ void __launch_bounds__(256) k_tc_plain(const uint32_t* __restrict__ rowptr,
                                                   const uint32_t* __restrict__ col,
-                                                  const uint32_t* __restrict__ src, uint32_t m, TcArgs<CT> a) {
+                                                  const uint32_t* __restrict__ src, uint32_t e_begin, uint32_t e_end,
+                                                  TcArgs<CT> a) {
     unsigned long long local = 0;
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
+    for (uint32_t e = e_begin + blockIdx.x * blockDim.x + threadIdx.x; e < e_end; e += gridDim.x * blockDim.x) {
         const uint32_t u = src[e], v = col[e];
         if (ALIVE && (!a.alive[u] || !a.alive[v])) continue;
         uint32_t i = rowptr[u], iend = rowptr[u + 1], j = rowptr[v], jend = rowptr[v + 1];
@@ -422,11 +423,24 @@ static ga_status launch_hash(ga_graph* g, const TcArgs<CT>& a) {
     int occ = 0;
     GA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, smem));
     occ = std::max(occ, 1);
-    const uint64_t want = std::max<uint64_t>(g->heavy.count, (g->light.count + kWarps - 1) / kWarps);
+    ga_items heavy = g->heavy, light = g->light;
+    if (a.nshards > 1) {   // this shard's equal part of each bin's item list (a view: offset pointers)
+        auto cut = [&](ga_items& it) {
+            const uint32_t lo = (uint32_t)((uint64_t)it.count * a.shard / a.nshards);
+            const uint32_t hi = (uint32_t)((uint64_t)it.count * (a.shard + 1) / a.nshards);
+            it.v += lo;
+            it.k0 += lo;
+            it.k1 += lo;
+            it.count = hi - lo;
+        };
+        cut(heavy);
+        cut(light);
+    }
+    const uint64_t want = std::max<uint64_t>(heavy.count, (light.count + kWarps - 1) / kWarps);
     const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)g->sm_count * occ, want));
     GA_CUDA(cudaMemsetAsync(g->d_queue, 0, 8 * sizeof(uint32_t), g->stream));
-    kern<<<grid, kThreads, smem, g->stream>>>(g->rowptr, g->col, g->in_src, g->in_eid, g->heavy, g->light, hb,
-                                              g->d_queue, a);
+    kern<<<grid, kThreads, smem, g->stream>>>(g->rowptr, g->col, g->in_src, g->in_eid, heavy, light, hb, g->d_queue,
+                                              a);
     GA_CUDA(cudaGetLastError());
     return GA_OK;
 }
@@ -436,8 +450,14 @@ static ga_status launch_plain(ga_graph* g, const TcArgs<CT>& a) {
     if (!g->m) return GA_OK;
     int occ = 0;
     GA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tc_plain<MODE, ALIVE, CT>, 256, 0));
-    const unsigned grid = grid_for(g->m, 256, (unsigned)g->sm_count * std::max(occ, 1) * 4);
-    k_tc_plain<MODE, ALIVE, CT><<<grid, 256, 0, g->stream>>>(g->rowptr, g->col, g->src, g->m, a);
+    uint32_t e0 = 0, e1 = g->m;
+    if (a.nshards > 1) {   // this shard's equal part of the edges
+        e0 = (uint32_t)((uint64_t)g->m * a.shard / a.nshards);
+        e1 = (uint32_t)((uint64_t)g->m * (a.shard + 1) / a.nshards);
+    }
+    if (e1 <= e0) return GA_OK;
+    const unsigned grid = grid_for(e1 - e0, 256, (unsigned)g->sm_count * std::max(occ, 1) * 4);
+    k_tc_plain<MODE, ALIVE, CT><<<grid, 256, 0, g->stream>>>(g->rowptr, g->col, g->src, e0, e1, a);
     GA_CUDA(cudaGetLastError());
     return GA_OK;
 }
@@ -454,7 +474,10 @@ ga_status run_tc(ga_graph* g, const TcArgs<CT>& a, bool zero_outputs) {
     // automatic choice: the autotuned kernel for counts; the hash kernel for supports and incidence lists, whose
     // per-triangle appends and increments contend on hub vertices in the one-thread-per-edge form (lists of the
     // Holme-Kim 1.7M graph: 154 ms plain vs 4 ms hash; first peel of the 4,096-graph batch: 3.2 s vs 1.1 s)
-    const int64_t kernel = g->opt_tc_kernel ? g->opt_tc_kernel : (MODE == TC_COUNT ? g->tuned_kernel : 2);
+    // A sharded count always uses the hash kernel unless one is forced: every GPU must cut the same partition, and
+    // an autotuned choice could differ between GPUs.
+    const int64_t kernel = g->opt_tc_kernel ? g->opt_tc_kernel
+                                            : (MODE == TC_COUNT && a.nshards <= 1 ? g->tuned_kernel : 2);
     if (kernel == 1) return launch_plain<MODE, ALIVE, CT>(g, a);
     if (g->heavy.count == 0 && g->light.count == 0) return GA_OK;
     return launch_hash<MODE, ALIVE, CT>(g, a);
@@ -616,6 +639,30 @@ ga_status ga_tc_count(ga_graph* g, uint64_t* triangles) {
     a.total = g->d_scalars;
     GA_TRY((run_tc<TC_COUNT, false, unsigned int>(g, a, true)));
     return read_total(g, a.total, triangles);
+}
+
+ga_status ga_tc_count_shard(ga_graph* g, uint32_t shard, uint32_t nshards, uint64_t* partial) {
+    if (!g || !partial) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    if (nshards == 0 || shard >= nshards) return fail(GA_ERR_INVALID_ARGUMENT, "need shard < nshards");
+    GA_TRY(use_device(g));
+    GA_TRY(ready(g));
+    TcArgs<unsigned int> a{};
+    a.total = g->d_scalars;
+    a.shard = shard;
+    a.nshards = nshards;
+    GA_TRY((run_tc<TC_COUNT, false, unsigned int>(g, a, true)));
+    return read_total(g, a.total, partial);
+}
+
+ga_status ga_tc_count_shard_async(ga_graph* g, uint32_t shard, uint32_t nshards, uint64_t* d_partial) {
+    if (!g || !d_partial) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    if (nshards == 0 || shard >= nshards) return fail(GA_ERR_INVALID_ARGUMENT, "need shard < nshards");
+    GA_TRY(use_device(g));
+    TcArgs<unsigned int> a{};
+    a.total = (unsigned long long*)d_partial;
+    a.shard = shard;
+    a.nshards = nshards;
+    return run_tc<TC_COUNT, false, unsigned int>(g, a, true);
 }
 
 ga_status ga_tc_count_async(ga_graph* g, uint64_t* d_triangles) {

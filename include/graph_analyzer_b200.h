@@ -185,6 +185,15 @@ ga_status ga_tc_count(ga_graph* g, uint64_t* triangles);
  * the launch must not include the one-time preparation. */
 ga_status ga_tc_count_async(ga_graph* g, uint64_t* d_triangles);
 
+/* Sharded count, for counting one graph on several GPUs (no counterpart in the reference, which runs on one GPU):
+ * the triangles found by shard `shard` of `nshards` equal parts of the work items (hash kernel) or of the oriented
+ * edges (plain kernel, when forced with GA_OPT_TC_KERNEL). The shards of a graph partition its triangles: with the
+ * graph resident on every GPU, count one shard per GPU and sum the partial counts (one 8-byte all-reduce). Shards
+ * use the hash kernel unless a kernel is forced, so every GPU cuts the same partition. The _async form writes the
+ * partial count to device memory on the graph's stream. */
+ga_status ga_tc_count_shard(ga_graph* g, uint32_t shard, uint32_t nshards, uint64_t* partial);
+ga_status ga_tc_count_shard_async(ga_graph* g, uint32_t shard, uint32_t nshards, uint64_t* d_partial);
+
 /* Triangle count that allocates no memory at all. It has no counterpart in the reference; it exists for callers that
  * cannot call cudaMalloc: a process whose device memory is entirely claimed by another allocator (for example a
  * framework's caching pool that reserved the free HBM up front), or a latency-critical path that must not pay for

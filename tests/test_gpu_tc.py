@@ -148,3 +148,29 @@ def test_device_create_and_streams(ga, oracle, cuda_ok):
         assert d.support_edges_device(sup.data_ptr()) == oracle.triangles_serial(g)
         assert np.array_equal(sup.cpu().numpy().view(np.uint32), oracle.edge_support(g)[1])
         assert d.device_bytes() > 0
+
+
+@pytest.mark.parametrize("kernel", [0, 1, 2])
+def test_shards_partition_the_triangles(ga, oracle, cuda_ok, kernel):
+    """One shard per GPU in a multi-GPU count: the shards' partial counts sum to the whole count for any number of
+    shards, with either kernel (0 = automatic: the hash kernel for shards)."""
+    rng = np.random.default_rng(17)
+    graphs = [ga.load_graph(fixture_path("t_pl900")),
+              ga.graph_from_pairs(1 << 13, ga.gen_rmat(13, 16 << 13, seed=3)),
+              ga.build_graph_from_edges(200, ga.canonical_edges(random_pairs(rng, 200, 0.3)))]
+    import torch
+    for g in graphs:
+        T = oracle.triangles_serial(g)
+        with ga.DeviceGraph(g) as d:
+            if kernel:
+                d.set_option(ga.OPT_TC_KERNEL, kernel)
+            for k in (1, 2, 3, 8, 64):
+                parts = [d.tc_count_shard(s, k) for s in range(k)]
+                assert sum(parts) == T, (k, parts)
+            out = torch.zeros(4, dtype=torch.int64, device="cuda")
+            for s in range(4):
+                d.tc_count_shard_async(s, 4, out[s:].data_ptr())
+            torch.cuda.synchronize()
+            assert int(out.sum()) == T
+            with pytest.raises(ga.GAError):
+                d.tc_count_shard(3, 3)
