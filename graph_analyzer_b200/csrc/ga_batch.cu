@@ -162,6 +162,7 @@ ga_status ga_batch_device_bytes(const ga_batch* b, uint64_t* bytes) {
 
 ga_status ga_batch_tc(ga_batch* b, uint64_t* triangles) {
     if (!b || !triangles) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    GA_GRAPH_LOCK(b->g);
     GA_TRY(use_device(b->g));
     return count_segments(b->g, triangles);
 }
@@ -171,6 +172,7 @@ ga_status ga_batch_tc_peel(ga_batch* b, uint64_t num, uint64_t den, uint64_t* tr
     if (!b) return fail(GA_ERR_INVALID_ARGUMENT, "null batch");
     if (den < 1 || den > (1ull << 20) || num > (1ull << 20))
         return fail(GA_ERR_INVALID_ARGUMENT, "eps = num/den needs 1 <= den <= 2^20 and num <= 2^20");
+    GA_GRAPH_LOCK(b->g);
     GA_TRY(use_device(b->g));
     return peel_segments(b->g, num, den, triangles, res, status, removed_round);
 }

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <vector>
 
 #include "ga_internal.h"
@@ -119,7 +120,12 @@ struct ga_graph {
     // every device allocation, freed by ga_graph_destroy
     std::vector<std::pair<void*, size_t>> allocations;
     uint64_t bytes = 0;
+    // every C-ABI call on this graph holds it (recursive: some entry points call others), so calls from several
+    // host threads on one handle are serialised instead of racing on its scratch arrays and stream
+    mutable std::recursive_mutex mu;
 };
+
+#define GA_GRAPH_LOCK(g) std::lock_guard<std::recursive_mutex> ga_graph_lock_((g)->mu)
 
 namespace ga {
 

@@ -497,6 +497,7 @@ ga_status ga_graph_create_device(const uint32_t* d_rowptr, const uint32_t* d_col
 
 ga_status ga_graph_destroy(ga_graph* g) {
     if (!g) return GA_OK;
+    { GA_GRAPH_LOCK(g); }   // calls in flight on other threads finish first (none may start after this one)
     cudaSetDevice(g->device);
     if (g->stream) cudaStreamSynchronize(g->stream);
     destroy_loops(g);
@@ -509,6 +510,7 @@ ga_status ga_graph_destroy(ga_graph* g) {
 
 ga_status ga_graph_set_stream(ga_graph* g, void* stream) {
     if (!g) return fail(GA_ERR_INVALID_ARGUMENT, "null graph");
+    GA_GRAPH_LOCK(g);
     GA_TRY(use_device(g));
     GA_CUDA(cudaStreamSynchronize(g->stream));
     if (g->own_stream) { cudaStreamDestroy(g->stream); g->own_stream = false; }
@@ -523,18 +525,21 @@ ga_status ga_graph_set_stream(ga_graph* g, void* stream) {
 
 ga_status ga_graph_device_bytes(const ga_graph* g, uint64_t* bytes) {
     if (!g || !bytes) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    GA_GRAPH_LOCK(g);
     *bytes = g->bytes;
     return GA_OK;
 }
 
 ga_status ga_graph_prepare(ga_graph* g) {
     if (!g) return fail(GA_ERR_INVALID_ARGUMENT, "null graph");
+    GA_GRAPH_LOCK(g);
     GA_TRY(use_device(g));
     return ready(g);
 }
 
 ga_status ga_graph_set_option(ga_graph* g, ga_option opt, int64_t value) {
     if (!g) return fail(GA_ERR_INVALID_ARGUMENT, "null graph");
+    GA_GRAPH_LOCK(g);
     if (value < 0) return fail(GA_ERR_INVALID_ARGUMENT, "option values are >= 0");
     switch (opt) {
         case GA_OPT_TC_KERNEL:

@@ -934,6 +934,7 @@ extern "C" {
 
 ga_status ga_batch_peel(ga_graph* g, uint64_t num, uint64_t den, ga_peel_result* res, uint32_t* removed_round) {
     if (!g || !res) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    GA_GRAPH_LOCK(g);
     if (den < 1 || den > (1ull << 20) || num > (1ull << 20))
         return fail(GA_ERR_INVALID_ARGUMENT, "eps = num/den needs 1 <= den <= 2^20 and num <= 2^20");
     GA_TRY(use_device(g));
@@ -952,6 +953,7 @@ ga_status ga_batch_peel(ga_graph* g, uint64_t num, uint64_t den, ga_peel_result*
 
 ga_status ga_core_decomposition(ga_graph* g, uint32_t* core, ga_core_result* res) {
     if (!g || !res) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    GA_GRAPH_LOCK(g);
     GA_TRY(use_device(g));
     LoopScalars s;
     GA_TRY(run_loop<LOOP_CORE>(g, 0, 1, &s));

@@ -633,6 +633,7 @@ extern "C" {
 
 ga_status ga_tc_count(ga_graph* g, uint64_t* triangles) {
     if (!g || !triangles) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    GA_GRAPH_LOCK(g);
     GA_TRY(use_device(g));
     GA_TRY(ready(g));
     TcArgs<unsigned int> a{};
@@ -644,6 +645,7 @@ ga_status ga_tc_count(ga_graph* g, uint64_t* triangles) {
 ga_status ga_tc_count_shard(ga_graph* g, uint32_t shard, uint32_t nshards, uint64_t* partial) {
     if (!g || !partial) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
     if (nshards == 0 || shard >= nshards) return fail(GA_ERR_INVALID_ARGUMENT, "need shard < nshards");
+    GA_GRAPH_LOCK(g);
     GA_TRY(use_device(g));
     GA_TRY(ready(g));
     TcArgs<unsigned int> a{};
@@ -657,6 +659,7 @@ ga_status ga_tc_count_shard(ga_graph* g, uint32_t shard, uint32_t nshards, uint6
 ga_status ga_tc_count_shard_async(ga_graph* g, uint32_t shard, uint32_t nshards, uint64_t* d_partial) {
     if (!g || !d_partial) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
     if (nshards == 0 || shard >= nshards) return fail(GA_ERR_INVALID_ARGUMENT, "need shard < nshards");
+    GA_GRAPH_LOCK(g);
     GA_TRY(use_device(g));
     TcArgs<unsigned int> a{};
     a.total = (unsigned long long*)d_partial;
@@ -667,6 +670,7 @@ ga_status ga_tc_count_shard_async(ga_graph* g, uint32_t shard, uint32_t nshards,
 
 ga_status ga_tc_count_async(ga_graph* g, uint64_t* d_triangles) {
     if (!g || !d_triangles) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    GA_GRAPH_LOCK(g);
     GA_TRY(use_device(g));
     TcArgs<unsigned int> a{};
     a.total = (unsigned long long*)d_triangles;
@@ -675,6 +679,7 @@ ga_status ga_tc_count_async(ga_graph* g, uint64_t* d_triangles) {
 
 ga_status ga_tc_support_edges_device(ga_graph* g, uint32_t* d_sup, uint64_t* triangles) {
     if (!g || (!d_sup && g->m)) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    GA_GRAPH_LOCK(g);
     GA_TRY(use_device(g));
     GA_TRY(ready(g));
     TcArgs<unsigned int> a{};
@@ -686,6 +691,7 @@ ga_status ga_tc_support_edges_device(ga_graph* g, uint32_t* d_sup, uint64_t* tri
 
 ga_status ga_tc_support_edges(ga_graph* g, uint32_t* sup, uint64_t* triangles) {
     if (!g || (!sup && g->m)) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    GA_GRAPH_LOCK(g);
     GA_TRY(use_device(g));
     Scratch s;
     s.st = g->stream;
@@ -698,6 +704,7 @@ ga_status ga_tc_support_edges(ga_graph* g, uint32_t* sup, uint64_t* triangles) {
 
 ga_status ga_tc_support_vertices(ga_graph* g, uint64_t* deg, uint64_t* triangles) {
     if (!g || (!deg && g->n)) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    GA_GRAPH_LOCK(g);
     GA_TRY(use_device(g));
     GA_TRY(ready(g));
     Scratch s;
@@ -713,6 +720,7 @@ ga_status ga_tc_support_vertices(ga_graph* g, uint64_t* deg, uint64_t* triangles
 
 ga_status ga_tc_participation(ga_graph* g, const uint8_t* alive, uint32_t* tri, uint64_t* triangles) {
     if (!g || ((!alive || !tri) && g->n)) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    GA_GRAPH_LOCK(g);
     GA_TRY(use_device(g));
     // T of the alive subgraph is at most T of the graph; refuse when uint32 counters could overflow (densest.h:68)
     uint64_t T_full = 0;

@@ -17,7 +17,9 @@
  *    GA_ERR_CUDA).
  *  - The library owns the device memory behind a ga_graph handle (the reference's backends leak theirs,
  *    gpu_densest.cu:82-96); ga_graph_destroy frees it.
- *  - A ga_graph is used by one host thread at a time; different handles may be used from different threads.
+ *  - Handles are thread-safe: calls on one ga_graph or ga_batch from several host threads are serialised by a lock
+ *    inside the handle (for the _async calls, only the enqueueing); different handles run in parallel. Destroy a
+ *    handle only once no other thread can still call it.
  */
 #ifndef GRAPH_ANALYZER_B200_H
 #define GRAPH_ANALYZER_B200_H

@@ -174,3 +174,34 @@ def test_shards_partition_the_triangles(ga, oracle, cuda_ok, kernel):
             assert int(out.sum()) == T
             with pytest.raises(ga.GAError):
                 d.tc_count_shard(3, 3)
+
+
+def test_one_handle_from_many_threads(ga, oracle, cuda_ok):
+    """Calls on one ga_graph from several host threads are serialised by the handle's lock: every call returns the
+    same results as a lone call (the counts, supports and peeling share the handle's scratch and stream)."""
+    import threading
+    g = ga.graph_from_pairs(1 << 12, ga.gen_rmat(12, 16 << 12, seed=4))
+    T = oracle.triangles_serial(g)
+    _, sup = oracle.edge_support(g)
+    o = oracle.batch_peel(g, 1, 10)
+    errors = []
+    with ga.DeviceGraph(g) as d:
+        def work(i):
+            try:
+                for _ in range(5):
+                    if i % 3 == 0:
+                        assert d.tc_count() == T
+                    elif i % 3 == 1:
+                        t, s = d.support_edges()
+                        assert t == T and np.array_equal(s, sup)
+                    else:
+                        r = d.batch_peel(1, 10)
+                        assert (r.best_num, r.best_den, r.rounds) == (o.best_num, o.best_den, o.rounds)
+            except Exception as e:   # reported below: an assert in a thread does not fail the test by itself
+                errors.append(repr(e))
+        threads = [threading.Thread(target=work, args=(i,)) for i in range(6)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+    assert not errors, errors
