@@ -1,0 +1,44 @@
+// api_check.cpp - the reference-names C++ surface (include/ga/graph_analyzer.hpp) used the way the reference's own
+// drivers use graph.h / densest.h / dsg.h: load_graph, a device graph, batch_peel_loop with the CPU count as T_full,
+// core_decomp_loop_inc, and the support helpers. Prints one line per result for the test to compare with the golden
+// outputs. usage: api_check graph.txt eps_num eps_den T_full
+#define GA_B200_GLOBAL_NAMES
+#include "ga/graph_analyzer.hpp"
+
+#include <cstdlib>
+
+int main(int argc, char** argv) {
+    if (argc != 5) return 2;
+    Graph g;
+    if (!load_graph(argv[1], g)) return 1;
+    const uint64_t num = std::strtoull(argv[2], nullptr, 10), den = std::strtoull(argv[3], nullptr, 10);
+    const uint64_t T_full = std::strtoull(argv[4], nullptr, 10);
+    try {
+        ga::DeviceGraph d(g);
+        std::printf("triangles %llu\n", (unsigned long long)d.triangles());
+        PeelResult r = batch_peel_loop(g.n, T_full, num, den, d);
+        if (!r.ok) { std::fprintf(stderr, "peel: %s\n", r.error.c_str()); return 1; }
+        unsigned long long rr = 0;
+        for (uint32_t v = 0; v < g.n; v++) rr = rr * 1000003ull + r.removed_round[v];
+        std::printf("peel %llu %llu %u %u %llx\n", (unsigned long long)r.best_num, (unsigned long long)r.best_den,
+                    r.best_round, r.rounds, rr);
+        std::vector<uint32_t> core;
+        CoreLoopResult c = core_decomp_loop_inc(g.n, T_full, d, core);
+        if (!c.ok) { std::fprintf(stderr, "cores: %s\n", c.error.c_str()); return 1; }
+        unsigned long long ch = 0;
+        for (uint32_t v = 0; v < g.n; v++) ch = ch * 1000003ull + core[v];
+        std::printf("cores %u %u %llx\n", c.kmax, c.rounds, ch);
+        std::vector<uint32_t> sup;
+        std::vector<uint64_t> deg;
+        std::printf("supports %llu %llu\n", (unsigned long long)d.edge_support(sup),
+                    (unsigned long long)d.triangle_degrees(deg));
+        // the refusals of batch_peel_loop (densest.h:65-78, 283-287): wrong T_full, eps out of range
+        PeelResult bad = batch_peel_loop(g.n, T_full + 1, num, den, d);
+        PeelResult bad_eps = batch_peel_loop(g.n, T_full, 1, 0, d);
+        std::printf("refusals %d %d\n", bad.ok ? 1 : 0, bad_eps.ok ? 1 : 0);
+    } catch (const ga::Error& e) {
+        std::fprintf(stderr, "%s\n", e.what());
+        return 1;
+    }
+    return 0;
+}

@@ -1,0 +1,51 @@
+"""The reference-names C++ surface (include/ga/graph_analyzer.hpp: Graph, load_graph, PeelResult, batch_peel_loop,
+core_decomp_loop_inc) compiled into a small program as a maintainer of the reference would, linked against the
+library; on a GPU its results must equal the golden outputs of the reference's own code."""
+from __future__ import annotations
+
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import FIXTURES, ROOT, fixture_path, golden_arrays
+
+LIB_DIR = os.path.join(ROOT, "graph_analyzer_b200", "_lib")
+
+
+@pytest.fixture(scope="module")
+def api_check(tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("cpp") / "api_check")
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"),
+                           os.path.join(ROOT, "tests", "cpp", "api_check.cpp"), "-o", exe, "-L", LIB_DIR,
+                           "-lga_b200", f"-Wl,-rpath,{LIB_DIR}"])
+    return exe
+
+
+def _hash(a):
+    h = 0
+    for x in a.tolist():
+        h = (h * 1000003 + int(x)) & ((1 << 64) - 1)
+    return format(h, "x")
+
+
+def test_compiles_and_refuses_bad_usage(api_check):
+    assert subprocess.run([api_check], capture_output=True).returncode == 2
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", FIXTURES)
+def test_reference_names_match_golden(api_check, golden, cuda_ok, name):
+    w, a = golden[name], golden_arrays(name)
+    r = subprocess.run([api_check, fixture_path(name), "1", "10", str(w["triangles"])], capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    out = dict(line.split(" ", 1) for line in r.stdout.strip().splitlines())
+    assert int(out["triangles"]) == w["triangles"]
+    p = w["peel"]["1/10"]
+    assert out["peel"].split() == [str(p["best_num"]), str(p["best_den"]), str(p["best_round"]), str(p["rounds"]),
+                                   _hash(a["removed_round_1_10"])]
+    assert out["cores"].split() == [str(w["kmax"]), str(w["core_rounds"]), _hash(a["core"])]
+    assert out["supports"].split() == [str(w["triangles"])] * 2
+    assert out["refusals"].split() == ["0", "0"]
