@@ -425,7 +425,7 @@ def run_rmat22_full(args):
     plain launches (one-thread-per-edge kernel, host-driven rounds) vs autotuned + graph-captured."""
     import torch
     import graph_analyzer_b200 as ga
-    g = make_graph(ga)
+    g = make_graph(ga, args.scale)
     plain = ga.DeviceGraph(g)
     for opt, v in ((ga.OPT_TC_KERNEL, 1), (ga.OPT_LOOP_MODE, 1)):
         plain.set_option(opt, v)
@@ -449,7 +449,7 @@ def run_rmat22_full(args):
                  and np.array_equal(res["plain"].core, res["tuned"].core))
     plain.close()
     tuned.close()
-    line = {"workload": "rmat22_tc_esup_cores", "metric": "TC, per-edge supports, (k,triangle)-cores ms",
+    line = {"workload": f"rmat{args.scale}_tc_esup_cores", "metric": "TC, per-edge supports, (k,triangle)-cores ms",
             "value": out["tc_ms_tuned"] + out["esup_ms_tuned"] + out["cores_ms_tuned"], "unit": "ms",
             "higher_is_better": False, "triangles": T, "kmax": res["tuned"].kmax, "rounds": res["tuned"].rounds,
             "bit_identical": bool(identical), "n": g.n, "m": g.m, **out}
