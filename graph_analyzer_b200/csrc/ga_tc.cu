@@ -47,8 +47,13 @@ namespace ga {
 
 constexpr int kWarps = 8;                 // warps per block of the hash kernel
 constexpr int kThreads = kWarps * 32;
-constexpr int kLightSlots = 512;          // per-warp hash set: 128 buckets of 4 slots, anchors with out-degree <= 128
-constexpr uint32_t kLightBits = 7;        // log2 buckets of the light set
+// Per-warp hash set of the light bin: 128 buckets of 4 slots for counts and lists; 64 buckets in the support modes,
+// whose slots carry counters too (2-3 words each): the smaller set keeps 7-8 blocks resident per SM instead of 4
+// (an anchor of up to 128 out-neighbours then has up to 2 keys per bucket).
+template <int MODE>
+constexpr int light_slots() { return (MODE == TC_VSUP || MODE == TC_ESUP) ? 256 : 512; }
+template <int MODE>
+constexpr uint32_t light_bits() { return (MODE == TC_VSUP || MODE == TC_ESUP) ? 6 : 7; }
 
 // VSUP and ESUP book per-slot and per-in-edge counters; COUNT and LIST do not.
 __host__ __device__ constexpr bool counters(int mode) { return mode == TC_VSUP || mode == TC_ESUP; }
@@ -63,7 +68,7 @@ constexpr int kBatchWords = 160;
 
 // Shared memory of the light phase per warp: slots * words + the batch area.
 template <int MODE>
-constexpr int light_warp_words() { return kLightSlots * SlotLayout<MODE>::words + kBatchWords; }
+constexpr int light_warp_words() { return light_slots<MODE>() * SlotLayout<MODE>::words + kBatchWords; }
 
 // Writes the triangle (u lowest, v middle, x highest) into the incidence list of each corner. A list is sized by the
 // counting pass; an entry that would land past its list's end is dropped and counted in *overflow instead.
@@ -306,13 +311,14 @@ __global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const ui
             __syncthreads();
         }
     }
-    // ---- light bin: one warp per item, private hash set of kLightSlots slots ----
+    // ---- light bin: one warp per item, private hash set of light_slots<MODE>() slots ----
     {
         constexpr int PW = light_warp_words<MODE>();
+        constexpr int LS = light_slots<MODE>();
         uint32_t* key = smem + warp * PW;
-        uint32_t* cnt = key + kLightSlots;
-        uint32_t* pos = cnt + (counters(MODE) ? kLightSlots : 0);
-        uint32_t* s_incl = key + kLightSlots * W;
+        uint32_t* cnt = key + LS;
+        uint32_t* pos = cnt + (counters(MODE) ? LS : 0);
+        uint32_t* s_incl = key + LS * W;
         uint32_t *s_rb = s_incl + 32, *s_ecnt = s_incl + 96;
         s_ecnt[lane] = 0;
         __syncwarp();
@@ -324,20 +330,23 @@ __global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const ui
             const uint32_t v = light.v[item];
             if (ALIVE && !a.alive[v]) continue;
             const uint32_t vb = rowptr[v], dv = rowptr[v + 1] - vb;
-            const uint32_t bits = table_bits(dv, kLightBits);   // dv <= light_max_deg: always a table
-            build_table<MODE, ALIVE, CT>(col, a, vb, dv, key, cnt, pos, bits, lane, 32, false);
+            // a table unless the anchor is too large for this mode's set (GA_OPT_LIGHT_MAX_DEG above 128 in the
+            // support modes): then binary search in the global row
+            const uint32_t bits = table_bits(dv, light_bits<MODE>());
+            const bool global = bits == 0;
+            if (!global) build_table<MODE, ALIVE, CT>(col, a, vb, dv, key, cnt, pos, bits, lane, 32, false);
             unsigned long long h = 0;
             const uint32_t k1 = light.k1[item];
             for (uint32_t kb = light.k0[item]; kb < k1; kb += 32)
                 h += probe_batch<MODE, ALIVE, CT>(rowptr, col, in_src, in_eid, a, kb, min(kb + 32, k1), key, cnt,
-                                                  bits, false, vb, dv, s_incl, s_rb, s_ecnt, lane, v);
+                                                  bits, global, vb, dv, s_incl, s_rb, s_ecnt, lane, v);
             hits += h;
             if (MODE == TC_VSUP) {
                 const unsigned long long t = warp_sum_u64(h);
                 if (lane == 0 && t) atomicAdd(&a.vsup[v], (CT)t);
             }
             __syncwarp();
-            flush_table<MODE, CT>(a, vb, key, cnt, pos, bits, lane, 32);
+            if (!global) flush_table<MODE, CT>(a, vb, key, cnt, pos, bits, lane, 32);
             __syncwarp();
         }
     }
@@ -409,6 +418,9 @@ static uint32_t heavy_bits_for(const ga_graph* g, int mode) {
     uint32_t cap = 3;
     while ((((size_t)words << (cap + 3)) + kWarps * kBatchWords) * 4 <= 200 * 1024) cap++;
     if (g->heavy_bits_cap) cap = std::min(cap, g->heavy_bits_cap);
+    // support modes: at most 512 buckets (anchors of up to 1,024 out-neighbours keep a table), so that the block's
+    // shared memory stays near the light bin's and 7-8 blocks stay resident per SM
+    if (mode == TC_VSUP || mode == TC_ESUP) cap = std::min(cap, 9u);
     uint32_t need = 3;
     while ((1u << need) < g->heavy.max_dv) need++;
     return std::min(need, cap);

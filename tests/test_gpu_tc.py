@@ -17,6 +17,8 @@ CONFIGS = {
     "heavy_global": {6: 8, 5: 3},
     "heavy_table": {6: 4, 5: 10},
     "small_items": {4: 16},
+    # light bin up to out-degree 256: in the support modes anchors above 128 fall back to binary search
+    "light_256": {6: 256, 1: 2},
 }
 
 
