@@ -252,6 +252,8 @@ def run_ours(args):
 
     # ---- device-resident: one count per step on the prepared, resident graph ----
     dg = ga.DeviceGraph(g, device=local, stream=stream.cuda_stream)
+    if args.tc_kernel != "auto":   # e.g. under a profiler, whose overheads can sway the autotuner's timing
+        dg.set_option(ga.OPT_TC_KERNEL, {"plain": 1, "hash": 2}[args.tc_kernel])
     t0 = time.perf_counter()
     dg.prepare()
     torch.cuda.synchronize(dev)
@@ -742,6 +744,8 @@ def main():
                     default="rmat22",
                     help="rmat22 (default, the headline line) or a secondary workload")
     ap.add_argument("--graphs", type=int, default=4096, help="graphs in the batch workload")
+    ap.add_argument("--tc-kernel", choices=["auto", "plain", "hash"], default="auto",
+                    help="count kernel of the headline's timed steps (auto: the autotuner's choice)")
     ap.add_argument("--shard", action="store_true",
                     help="with N > 1 GPUs: count ONE graph split into N shards (strong scaling) instead of N replicas")
     ap.add_argument("--scale", type=int, default=SCALE,
