@@ -274,6 +274,15 @@ ga_status init_pool(int device) {
     return GA_OK;
 }
 
+ga_status pool_keep_at_least(int device, uint64_t bytes) {
+    GA_TRY(init_pool(device));
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    uint64_t keep = 0;
+    GA_CUDA(cudaMemPoolGetAttribute(g_pools[device], cudaMemPoolAttrReleaseThreshold, &keep));
+    if (bytes > keep) GA_CUDA(cudaMemPoolSetAttribute(g_pools[device], cudaMemPoolAttrReleaseThreshold, &bytes));
+    return GA_OK;
+}
+
 cudaMemPool_t pool_of_current() {
     int device = 0;
     cudaGetDevice(&device);

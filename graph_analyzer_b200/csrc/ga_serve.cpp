@@ -418,6 +418,11 @@ ga_status ga_server_create(const ga_server_config* config, ga_server** out) {
     if (s->cfg.small_slots == UINT32_MAX) s->cfg.small_slots = 0;
     if (!s->cfg.pin_min_edges) s->cfg.pin_min_edges = 1u << 20;
     cudaSetDevice(s->cfg.device);
+    const ga_status ps = ga::pool_keep_at_least(s->cfg.device, s->cfg.hbm_budget_bytes);
+    if (ps != GA_OK) {
+        delete s;
+        return ps;
+    }
     if (cudaStreamCreateWithFlags(&s->evict_stream, cudaStreamNonBlocking) != cudaSuccess) {
         (void)cudaGetLastError();
         delete s;
