@@ -256,6 +256,7 @@ ga_status use_device(const ga_graph* g) {
 }
 
 static std::mutex g_pool_mu;
+static constexpr uint64_t kPoolKeepDefault = 8ull << 30;   // bytes the pool keeps cached after frees, by default
 static cudaMemPool_t g_pools[64] = {};
 
 ga_status init_pool(int device) {
@@ -268,11 +269,13 @@ ga_status init_pool(int device) {
     props.location.id = device;
     cudaMemPool_t pool;
     GA_CUDA(cudaMemPoolCreate(&pool, &props));
-    uint64_t keep = 8ull << 30;
+    uint64_t keep = kPoolKeepDefault;
     GA_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
     g_pools[device] = pool;
     return GA_OK;
 }
+
+static uint32_t g_pool_holders[64] = {};   // servers keeping their budget mapped, per device
 
 ga_status pool_keep_at_least(int device, uint64_t bytes) {
     GA_TRY(init_pool(device));
@@ -280,7 +283,18 @@ ga_status pool_keep_at_least(int device, uint64_t bytes) {
     uint64_t keep = 0;
     GA_CUDA(cudaMemPoolGetAttribute(g_pools[device], cudaMemPoolAttrReleaseThreshold, &keep));
     if (bytes > keep) GA_CUDA(cudaMemPoolSetAttribute(g_pools[device], cudaMemPoolAttrReleaseThreshold, &bytes));
+    g_pool_holders[device]++;
     return GA_OK;
+}
+
+void pool_keep_release(int device) {
+    if (device < 0 || device >= 64) return;
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (!g_pools[device] || !g_pool_holders[device] || --g_pool_holders[device]) return;
+    // the last holder is gone: back to the default and hand the rest of the cached memory back to the driver
+    uint64_t keep = kPoolKeepDefault;
+    cudaMemPoolSetAttribute(g_pools[device], cudaMemPoolAttrReleaseThreshold, &keep);
+    cudaMemPoolTrimTo(g_pools[device], keep);
 }
 
 cudaMemPool_t pool_of_current() {

@@ -16,6 +16,8 @@ void clear_error();
 // Raises the bytes the library's memory pool of `device` keeps cached after frees (never lowers them): a server keeps
 // its whole HBM budget mapped, so graphs that come and go do not map and unmap device memory again and again.
 ga_status pool_keep_at_least(int device, uint64_t bytes);
+// Ends one pool_keep_at_least; when the last one ends the pool returns to its default and trims its cache.
+void pool_keep_release(int device);
 
 // 64-bit mixer (splitmix64 finaliser) and a small counter-based stream built on it: every (seed, stream, index)
 // gives an independent value, so generators are deterministic for any thread count.

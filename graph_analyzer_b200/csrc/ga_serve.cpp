@@ -425,6 +425,7 @@ ga_status ga_server_create(const ga_server_config* config, ga_server** out) {
     }
     if (cudaStreamCreateWithFlags(&s->evict_stream, cudaStreamNonBlocking) != cudaSuccess) {
         (void)cudaGetLastError();
+        ga::pool_keep_release(s->cfg.device);
         delete s;
         return fail(GA_ERR_CUDA, "stream creation failed");
     }
@@ -453,6 +454,7 @@ ga_status ga_server_destroy(ga_server* s) {
     for (auto& kv : s->graphs)
         if (kv.second.pinned) cudaFreeHost(kv.second.pinned);
     cudaStreamDestroy(s->evict_stream);
+    ga::pool_keep_release(s->cfg.device);
     delete s;
     return GA_OK;
 }
