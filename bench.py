@@ -591,6 +591,9 @@ def run_serve(args):
     R = args.requests
     rng = np.random.default_rng(SEED)
     graphs, trace = _serve_trace(ga, R, rng)
+    # every run below uses a fresh server (no graph resident yet); one idle server held open for the whole workload
+    # keeps the device's memory pool mapped between them, as in a long-lived serving process
+    holder = ga.Server()
     # warm-up, untimed: one pass of the whole trace through a server fills the kernel-choice cache (one timing per
     # degree-distribution signature) and the memory pool, so neither side below pays those first-time costs
     _serve_run(ga, graphs, trace, np.zeros(R), args.slots)
@@ -658,6 +661,7 @@ def run_serve(args):
             "mix": {"tc": int(kinds[0]), "peel_eps_1_10": int(kinds[1]), "cores": int(kinds[2])},
             "hbm_budget_gb": 150, "slots": args.slots or 4, "burst": burst, "sweep": sweep, "by_class": by_class,
             "bit_identical": bool(identical)}
+    holder.close()
     print(json.dumps(line), flush=True)
     return 0 if identical else 1
 
