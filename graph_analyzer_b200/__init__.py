@@ -81,6 +81,15 @@ class _CoreRes(C.Structure):
     _fields_ = [("kmax", C.c_uint32), ("rounds", C.c_uint32)]
 
 
+class _DsgRes(C.Structure):
+    _fields_ = [("tri", C.c_uint64), ("verts", C.c_uint64), ("flow_calls", C.c_uint32),
+                ("components_searched", C.c_uint32), ("shrinks", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class _DsgSeed(C.Structure):
+    _fields_ = [("set", _vp), ("set_len", C.c_uint64), ("tri", C.c_uint64), ("verts", C.c_uint64)]
+
+
 class _ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int), ("hbm_budget_bytes", C.c_uint64), ("slots", C.c_uint32),
                 ("fold_max_graphs", C.c_uint32), ("fold_max_edges", C.c_uint32), ("small_slots", C.c_uint32),
@@ -139,6 +148,15 @@ SIGNATURES: dict[str, list] = {
     "ga_tc_participation": [_vp, _vp, _vp, C.POINTER(C.c_uint64)],
     "ga_batch_peel": [_vp, C.c_uint64, C.c_uint64, C.POINTER(_PeelRes), _vp],
     "ga_core_decomposition": [_vp, _vp, C.POINTER(_CoreRes)],
+    "ga_greedy_pp": [_vp, C.c_uint32, C.POINTER(_DsgRes), _vp, _vp],
+    "ga_core_exact": [_vp, _vp, C.c_int, C.POINTER(_DsgSeed), C.POINTER(_DsgRes), _vp],
+    "ga_exact_densest": [_vp, C.POINTER(_DsgRes), _vp],
+    "ga_greedy_pp_host": [C.c_uint32, _vp, _vp, _vp, C.c_uint32, C.POINTER(_DsgRes), _vp, _vp],
+    "ga_core_exact_host": [C.c_uint32, _vp, _vp, C.c_uint64, _vp, _vp, C.c_int, C.POINTER(_DsgSeed),
+                           C.POINTER(_DsgRes), _vp],
+    "ga_exact_densest_host": [C.c_uint32, C.c_uint64, _vp, C.POINTER(_DsgRes), _vp],
+    "ga_prune_to_core": [_vp, _vp, C.c_uint32, C.c_uint32, _vp, C.c_uint64, C.POINTER(C.POINTER(_HostGraph)), _vp,
+                         _vp],
     "ga_gen_holme_kim_batch": [C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_double,
                                C.c_uint64, C.POINTER(C.POINTER(_HostBatch))],
     "ga_host_batch_free": [C.POINTER(_HostBatch)],
@@ -368,6 +386,78 @@ class PeelResult:
 
 
 @dataclass
+class DsgResult:
+    """DsgResult (dsg.h:49-59): the returned vertex set (ascending ids) and its triangle count."""
+
+    tri: int = 0
+    verts: int = 0
+    set: np.ndarray = field(default_factory=lambda: np.zeros(0, np.uint32))
+    flow_calls: int = 0
+    components_searched: int = 0
+    shrinks: int = 0
+    per_pass: list = field(default_factory=list)
+
+    def density(self) -> float:
+        return density_value(self.tri, self.verts)
+
+
+def _dsg_result(r: _DsgRes, setbuf: np.ndarray, per: np.ndarray | None = None) -> DsgResult:
+    pp = [(int(per[2 * i]), int(per[2 * i + 1])) for i in range(len(per) // 2)] if per is not None else []
+    return DsgResult(r.tri, r.verts, setbuf[: r.verts].copy(), r.flow_calls, r.components_searched, r.shrinks, pp)
+
+
+def _seed(seed: DsgResult | None):
+    if seed is None:
+        return None, None
+    arr = np.ascontiguousarray(seed.set, np.uint32)
+    return C.byref(_DsgSeed(_ptr(arr) if arr.size else None, arr.size, seed.tri, seed.verts)), arr
+
+
+def greedy_pp_host(n: int, core: np.ndarray, inc_ptr: np.ndarray, inc: np.ndarray, passes: int) -> DsgResult:
+    """Host stage of Greedy / Greedy++ on caller-made incidence lists (ga_greedy_pp_host)."""
+    r, setbuf, per = _DsgRes(), np.zeros(max(n, 1), np.uint32), np.zeros(2 * max(passes, 1), np.uint64)
+    core = np.ascontiguousarray(core, np.uint32)
+    ip, ie = np.ascontiguousarray(inc_ptr, np.uint64), np.ascontiguousarray(inc, np.uint32)
+    _check(lib().ga_greedy_pp_host(n, _ptr(core) if n else None, _ptr(ip), _ptr(ie) if ie.size else None, passes,
+                                   C.byref(r), _ptr(setbuf), _ptr(per)))
+    return _dsg_result(r, setbuf, per[: 2 * passes])
+
+
+def core_exact_host(g: Graph, tris: np.ndarray, core: np.ndarray, use_pruning12: bool = True,
+                    seed: DsgResult | None = None) -> DsgResult:
+    """Host stage of CoreExact on caller-listed triangles (lowest, middle, highest) (ga_core_exact_host)."""
+    r, setbuf = _DsgRes(), np.zeros(max(g.n, 1), np.uint32)
+    t = np.ascontiguousarray(tris, np.uint32).reshape(-1)
+    core = np.ascontiguousarray(core, np.uint32)
+    sp, keep = _seed(seed)
+    _check(lib().ga_core_exact_host(g.n, _ptr(np.ascontiguousarray(g.rowptr, np.uint32)),
+                                    _ptr(np.ascontiguousarray(g.col, np.uint32)) if g.m else None, t.size // 3,
+                                    _ptr(t) if t.size else None, _ptr(core) if g.n else None, int(use_pruning12), sp,
+                                    C.byref(r), _ptr(setbuf)))
+    del keep
+    return _dsg_result(r, setbuf)
+
+
+def exact_densest_host(n: int, tris: np.ndarray) -> DsgResult:
+    r, setbuf = _DsgRes(), np.zeros(max(n, 1), np.uint32)
+    t = np.ascontiguousarray(tris, np.uint32).reshape(-1)
+    _check(lib().ga_exact_densest_host(n, t.size // 3, _ptr(t) if t.size else None, C.byref(r), _ptr(setbuf)))
+    return _dsg_result(r, setbuf)
+
+
+def prune_to_core(g: Graph, core: np.ndarray, k: int) -> tuple[Graph, np.ndarray, np.ndarray]:
+    """prune_to_core (dsg.h:638-645): (subgraph of {core >= k}, old ids, restricted core numbers)."""
+    out = C.POINTER(_HostGraph)()
+    old, cout = np.zeros(max(g.n, 1), np.uint32), np.zeros(max(g.n, 1), np.uint32)
+    core = np.ascontiguousarray(core, np.uint32)
+    _check(lib().ga_prune_to_core(_ptr(np.ascontiguousarray(g.rowptr, np.uint32)),
+                                  _ptr(np.ascontiguousarray(g.col, np.uint32)) if g.m else None, g.n, g.m,
+                                  _ptr(core) if g.n else None, k, C.byref(out), _ptr(old), _ptr(cout)))
+    gp = _from_host_graph(out)
+    return gp, old[: gp.n].copy(), cout[: gp.n].copy()
+
+
+@dataclass
 class CoreResult:
     """Core numbers plus the CoreLoopResult fields (dsg.h:687-691)."""
 
@@ -492,6 +582,30 @@ class DeviceGraph:
         core = np.zeros(max(self.n, 1), np.uint32) if want_core else None
         _check(lib().ga_core_decomposition(self._h, _ptr(core), C.byref(r)))
         return CoreResult(core[: self.n] if core is not None else np.zeros(0, np.uint32), r.kmax, r.rounds)
+
+
+    def greedy_pp(self, passes: int = 1) -> DsgResult:
+        """Greedy (passes = 1) / Greedy++ (dsg.h:189-250): core numbers and triangle lists on the device."""
+        r, setbuf = _DsgRes(), np.zeros(max(self.n, 1), np.uint32)
+        per = np.zeros(2 * max(passes, 1), np.uint64)
+        _check(lib().ga_greedy_pp(self._h, passes, C.byref(r), _ptr(setbuf), _ptr(per)))
+        return _dsg_result(r, setbuf, per[: 2 * passes])
+
+    def core_exact(self, core: np.ndarray | None = None, use_pruning12: bool = True,
+                   seed: DsgResult | None = None) -> DsgResult:
+        """CoreExact (dsg.h:463-627); core numbers from the device when `core` is None."""
+        r, setbuf = _DsgRes(), np.zeros(max(self.n, 1), np.uint32)
+        c = np.ascontiguousarray(core, np.uint32) if core is not None and self.n else None
+        sp, keep = _seed(seed)
+        _check(lib().ga_core_exact(self._h, _ptr(c), int(use_pruning12), sp, C.byref(r), _ptr(setbuf)))
+        del keep
+        return _dsg_result(r, setbuf)
+
+    def exact_densest(self) -> DsgResult:
+        """Exact (dsg.h:405-428)."""
+        r, setbuf = _DsgRes(), np.zeros(max(self.n, 1), np.uint32)
+        _check(lib().ga_exact_densest(self._h, C.byref(r), _ptr(setbuf)))
+        return _dsg_result(r, setbuf)
 
 
 # one-shot helpers with the reference driver's semantics (upload, run, download)

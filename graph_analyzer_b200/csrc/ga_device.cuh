@@ -185,6 +185,13 @@ ga_status scan_u64(ga_graph* g, unsigned long long* data, uint64_t n);
 // Frees the loop state and its device buffers (the next loop call rebuilds them).
 void reset_loops(ga_graph* g);
 
+// The core numbers of g (device, n entries, valid until the next loop call) from one run of the core loop.
+ga_status core_numbers(ga_graph* g, const uint32_t** d_core, uint32_t* kmax);
+// The triangle incidence lists of g (device): for every vertex v the other two corners of each triangle through v
+// in inc[inc_ptr[v] .. inc_ptr[v+1]), (middle, highest) in the list of a triangle's lowest corner. Built when
+// missing, whatever GA_OPT_UPDATE_MODE says; *T = triangles.
+ga_status incidence_lists(ga_graph* g, const uint2** inc, const unsigned long long** inc_ptr, uint64_t* T);
+
 // Batches: g is the disjoint union of `count` graphs, graph s owning vertices [d_off[s], d_off[s+1]) (device array
 // of count + 1 offsets that outlives g's use of it). set_segments installs the per-graph loop state once;
 // count_segments gives every graph's triangle count; peel_segments peels all graphs in one loop, each exactly as if

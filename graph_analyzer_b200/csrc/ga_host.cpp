@@ -24,12 +24,6 @@
 
 #include "ga_internal.h"
 
-#define GA_TRY_HOST(call)            \
-    do {                             \
-        const ga_status s_ = (call); \
-        if (s_ != GA_OK) return s_;  \
-    } while (0)
-
 namespace ga {
 
 static thread_local std::string t_err;
@@ -251,6 +245,48 @@ ga_status ga_host_graph_from_edges(uint32_t n, const uint32_t* pairs, uint64_t n
         ga_host_graph* g = new_host_graph(n, (uint32_t)m);
         if (!g) return fail(GA_ERR_OUT_OF_MEMORY, "host allocation failed");
         ga_status s = build_csr(n, p, (uint32_t)m, g->rowptr, g->col, g->src, &g->max_out_degree);
+        if (s != GA_OK) { ga_host_graph_free(g); return s; }
+        *out = g;
+    } catch (const std::bad_alloc&) {
+        return fail(GA_ERR_OUT_OF_MEMORY, "host allocation failed");
+    }
+    return GA_OK;
+}
+
+// prune_to_core (dsg.h:638-645): keep {v : core[v] >= k}, renumber in increasing id order, and build the kept edges
+// as a fresh graph (induced_subgraph, dsg.h:103-114), so the orientation follows the degrees inside the subgraph.
+ga_status ga_prune_to_core(const uint32_t* rowptr, const uint32_t* col, uint32_t n, uint32_t m, const uint32_t* core,
+                           uint64_t k, ga_host_graph** out, uint32_t* old_id, uint32_t* core_out) {
+    if (!rowptr || (!col && m) || !out || (n && (!core || !old_id || !core_out)))
+        return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    try {
+        if (rowptr[0] != 0 || rowptr[n] != m) return fail(GA_ERR_INVALID_GRAPH, "rowptr does not span [0, m]");
+        std::vector<uint32_t> new_id(n, UINT32_MAX);
+        uint32_t kept = 0;
+        for (uint32_t v = 0; v < n; v++) {
+            if (core[v] < k) continue;
+            new_id[v] = kept;
+            old_id[kept] = v;
+            core_out[kept] = core[v];
+            kept++;
+        }
+        std::vector<uint32_t> pairs;
+        for (uint32_t u = 0; u < n; u++) {
+            if (rowptr[u] > rowptr[u + 1]) return fail(GA_ERR_INVALID_GRAPH, "rowptr not monotone at %u", u);
+            for (uint32_t e = rowptr[u]; e < rowptr[u + 1]; e++) {
+                const uint32_t v = col[e];
+                if (v >= n) return fail(GA_ERR_INVALID_GRAPH, "endpoint %u >= n=%u", v, n);
+                if (new_id[u] != UINT32_MAX && new_id[v] != UINT32_MAX) {
+                    pairs.push_back(new_id[u]);
+                    pairs.push_back(new_id[v]);
+                }
+            }
+        }
+        const uint32_t m2 = (uint32_t)(pairs.size() / 2);
+        ga_host_graph* g = new_host_graph(kept, m2);
+        if (!g) return fail(GA_ERR_OUT_OF_MEMORY, "host allocation failed");
+        ga_status s = build_csr(kept, pairs.data(), m2, g->rowptr, g->col, g->src, &g->max_out_degree);
         if (s != GA_OK) { ga_host_graph_free(g); return s; }
         *out = g;
     } catch (const std::bad_alloc&) {

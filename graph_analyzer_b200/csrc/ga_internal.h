@@ -9,6 +9,13 @@
 
 namespace ga {
 
+// Returns from the calling function when a host-side step fails (its message is already recorded).
+#define GA_TRY_HOST(expr)                    \
+    do {                                     \
+        const ga_status st_ = (expr);        \
+        if (st_ != GA_OK) return st_;        \
+    } while (0)
+
 // Records the message returned by ga_last_error() for this thread and returns `s`.
 ga_status fail(ga_status s, const char* fmt, ...);
 void clear_error();

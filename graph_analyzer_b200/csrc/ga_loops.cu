@@ -871,6 +871,56 @@ static ga_status run_loop(ga_graph* g, uint64_t num, uint64_t den, LoopScalars* 
     return GA_OK;
 }
 
+ga_status core_numbers(ga_graph* g, const uint32_t** d_core, uint32_t* kmax) {
+    LoopScalars s;
+    GA_TRY(run_loop<LOOP_CORE>(g, 0, 1, &s));
+    *d_core = g->loops->out;
+    *kmax = s.kcur;
+    return GA_OK;
+}
+
+ga_status incidence_lists(ga_graph* g, const uint2** inc, const unsigned long long** inc_ptr, uint64_t* T) {
+    GA_TRY(ready(g));
+    GA_TRY(ensure_loops(g));
+    ga_loops* L = g->loops;
+    cudaStream_t st = g->stream;
+    if (!L->inc && g->n) {
+        // per-vertex counts size the lists (the list build's input)
+        TcArgs<unsigned int> a{};
+        a.total = g->d_scalars;
+        a.vsup = L->tri;
+        GA_TRY((run_tc<TC_VSUP, false, unsigned int>(g, a, true)));
+        GA_CUDA(cudaMemcpyAsync(g->h_scalars, g->d_scalars, 8, cudaMemcpyDeviceToHost, st));
+        GA_CUDA(cudaStreamSynchronize(st));
+        const uint64_t T0 = g->h_scalars[0];
+        if (T0 >= (1ull << 32))
+            return fail(GA_ERR_ARITH, "triangle count %llu >= 2^32: uint32 tri[] counters could overflow",
+                        (unsigned long long)T0);
+        // build them even where the loops were told to enumerate; the loops keep the update they had chosen
+        const int prev = L->lists;
+        const int64_t mode = g->opt_update_mode;
+        L->lists = -1;
+        g->opt_update_mode = 2;
+        const ga_status s = build_lists(g, T0);
+        g->opt_update_mode = mode;
+        if (s != GA_OK) {
+            L->lists = prev;
+            return s;
+        }
+        if (prev == 0) L->lists = 0;
+        else if (mode == 1) L->lists = -1;
+    }
+    *inc = L->inc;
+    *inc_ptr = L->inc_ptr;
+    *T = 0;
+    if (g->n) {
+        GA_CUDA(cudaMemcpyAsync(g->h_scalars, L->inc_ptr + g->n, 8, cudaMemcpyDeviceToHost, st));
+        GA_CUDA(cudaStreamSynchronize(st));
+        *T = g->h_scalars[0] / 3;
+    }
+    return GA_OK;
+}
+
 ga_status set_segments(ga_graph* g, const unsigned long long* d_off, uint32_t count) {
     reset_loops(g);
     g->seg_off = d_off;

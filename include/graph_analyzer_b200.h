@@ -275,6 +275,67 @@ typedef struct ga_core_result {
  * Refuses T >= 2^32 with GA_ERR_ARITH (dsg.h:727). */
 ga_status ga_core_decomposition(ga_graph* g, uint32_t* core, ga_core_result* res);
 
+/* ---- densest subgraph by triangle density: the paper algorithms of dsg.h (Greedy / Greedy++ dsg.h:179-250,
+ *      Exact dsg.h:399-428, CoreExact dsg.h:431-627, prune_to_core dsg.h:630-645) and the greedy peel of densest.h
+ *      (cpu_greedy_peel, densest.h:200-252). Density of a vertex set S = triangles(S) / |S|, compared exactly.
+ *      The device lists the triangles (the incidence lists of the core loop) and computes the core numbers; the
+ *      sequential parts (heap-ordered removals, max-flow) run on the host. Results are the reference functions'
+ *      results on the same graph: the same triangle and vertex counts, the same vertex set, the same number of
+ *      max-flow calls. The reference runs all of these on the CPU only (gpu_dsg.cu:318-369). ---- */
+typedef struct ga_dsg_result {
+    uint64_t tri;                  /* triangles of the returned vertex set (DsgResult::tri)                     */
+    uint64_t verts;                /* its vertices (DsgResult::verts); 0 with tri 0: the graph has no triangle  */
+    uint32_t flow_calls;           /* max-flow computations (Exact, CoreExact)                                   */
+    uint32_t components_searched;  /* CoreExact: components that entered the binary search                       */
+    uint32_t shrinks;              /* CoreExact: network rebuilds on a higher core (Alg 4 line 17)               */
+    uint32_t reserved;
+} ga_dsg_result;
+
+/* A lower bound for CoreExact (the `seed` of core_exact, dsg.h:457-462,545-555): a vertex set of the same graph with its
+ * claimed triangle count; it is verified before use. */
+typedef struct ga_dsg_seed {
+    const uint32_t* set;           /* host, set_len vertex ids                                                    */
+    uint64_t set_len;
+    uint64_t tri;                  /* claimed triangles of the set                                                */
+    uint64_t verts;                /* claimed size (must equal set_len); 0 = no seed                              */
+} ga_dsg_seed;
+
+/* Greedy (passes = 1: Charikar's peel, greedy() dsg.h:250, the same best density as cpu_greedy_peel) and
+ * Greedy++ (passes > 1, greedy_pp dsg.h:189-249): remove the vertex with the smallest load + triangle degree (ties:
+ * smaller id), record the best residual subgraph. set: host, n entries or NULL: the best subgraph, ascending
+ * (res->verts ids written). per_pass: host, 2 * passes entries or NULL: (tri, verts) of the best after each pass.
+ * The first pass runs as one removal sequence per core level (the device's core numbers split Charikar's order into
+ * independent pieces), on all host threads. GA_ERR_ARITH for T >= 2^32 (the core loop's counters). */
+ga_status ga_greedy_pp(ga_graph* g, uint32_t passes, ga_dsg_result* res, uint32_t* set, uint64_t* per_pass);
+
+/* CoreExact (DSD Alg 4, core_exact dsg.h:463-627). core: host core numbers of the graph (n entries) or NULL (then
+ * computed on the device). use_pruning12 = 0 is the reference's test hook (start from one triangle instead of
+ * Pruning1/2). seed: NULL or a lower bound (GA_ERR_INVALID_ARGUMENT if it is not a subgraph with the claimed
+ * count). set: host, n entries or NULL. GA_ERR_ARITH when a flow network's capacities could reach 2^59. */
+ga_status ga_core_exact(ga_graph* g, const uint32_t* core, int use_pruning12, const ga_dsg_seed* seed,
+                        ga_dsg_result* res, uint32_t* set);
+
+/* Exact (DSD Alg 1, exact_densest dsg.h:405-428): binary search on the density with a max-flow per step. */
+ga_status ga_exact_densest(ga_graph* g, ga_dsg_result* res, uint32_t* set);
+
+/* Host stages of the three functions above on caller-provided data (what they run after the device work), for
+ * callers that already hold the triangle lists. inc_ptr (n + 1) and inc (2 ids per entry): for every vertex v the
+ * other two corners of each triangle through v in inc[2*inc_ptr[v] .. 2*inc_ptr[v+1]). tris: 3 ids per triangle,
+ * (lowest, middle, highest) in the (degree, id) orientation, i.e. u -> v -> w oriented edges. core: the graph's core
+ * numbers (ga_core_decomposition). rowptr / col: the oriented CSR. */
+ga_status ga_greedy_pp_host(uint32_t n, const uint32_t* core, const uint64_t* inc_ptr, const uint32_t* inc,
+                            uint32_t passes, ga_dsg_result* res, uint32_t* set, uint64_t* per_pass);
+ga_status ga_core_exact_host(uint32_t n, const uint32_t* rowptr, const uint32_t* col, uint64_t ntri,
+                             const uint32_t* tris, const uint32_t* core, int use_pruning12, const ga_dsg_seed* seed,
+                             ga_dsg_result* res, uint32_t* set);
+ga_status ga_exact_densest_host(uint32_t n, uint64_t ntri, const uint32_t* tris, ga_dsg_result* res, uint32_t* set);
+
+/* prune_to_core (dsg.h:638-645, induced_subgraph dsg.h:103-114): the subgraph induced by {v : core[v] >= k}, ids
+ * renumbered in increasing order, oriented by (degree, id) inside the subgraph. old_id and core_out: host, n
+ * entries each (the first (*out)->n written: the old id and the core number of each kept vertex). Host only. */
+ga_status ga_prune_to_core(const uint32_t* rowptr, const uint32_t* col, uint32_t n, uint32_t m, const uint32_t* core,
+                           uint64_t k, ga_host_graph** out, uint32_t* old_id, uint32_t* core_out);
+
 /* ---- serving: a request loop with continuous batching (no counterpart in the reference) ----
  * Requests (triangle count, batch peeling, (k,triangle)-cores) on registered graphs are admitted while device memory
  * under the HBM budget and a free slot allow: each slot is a host worker with its own CUDA stream, so admitted

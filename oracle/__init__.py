@@ -44,6 +44,18 @@ class PeelOut:
     removed_round: np.ndarray
 
 
+@dataclass
+class DsgOut:
+    """DsgResult of dsg.h: the returned vertex set (ascending ids) with its triangle count."""
+    tri: int
+    verts: int
+    set: np.ndarray
+    flow_calls: int = 0
+    components_searched: int = 0
+    shrinks: int = 0
+    per_pass: list | None = None
+
+
 class _Base:
     lib: C.CDLL
 
@@ -240,6 +252,20 @@ class Reference(_Base):
         L.ref_core_level_density.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, _u32p, _u32p, C.c_uint32,
                                              C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
 
+        _g = [C.c_uint32, C.c_uint32, _u32p, _u32p, _u32p]
+        L.ref_greedy_pp.restype = C.c_int
+        L.ref_greedy_pp.argtypes = _g + [C.c_uint32, _u64p, _u32p, _u64p, C.c_char_p, C.c_int]
+        L.ref_cpu_greedy_peel.restype = C.c_int
+        L.ref_cpu_greedy_peel.argtypes = _g + [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        L.ref_core_exact.restype = C.c_int
+        L.ref_core_exact.argtypes = _g + [_u32p, C.c_int, C.c_int, _u32p, C.c_uint64, C.c_uint64, C.c_uint64, _u64p,
+                                          _u32p, C.c_char_p, C.c_int]
+        L.ref_exact_densest.restype = C.c_int
+        L.ref_exact_densest.argtypes = _g + [_u64p, _u32p, C.c_char_p, C.c_int]
+        L.ref_prune_to_core.restype = None
+        L.ref_prune_to_core.argtypes = _g + [_u32p, C.c_uint64, _u32p, _u32p, _u32p, _u32p, _u32p,
+                                             C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+
     def resident(self, g: CSR) -> "RefGraph":
         """A copy of g held in the reference's own Graph, for timing its counter without the copy-in."""
         return RefGraph(self, g)
@@ -331,6 +357,55 @@ class Reference(_Base):
         self.lib.ref_core_level_density(*self._args2(g), c, k, C.byref(a), C.byref(b))
         return int(a.value), int(b.value)
 
+
+    # ---- densest subgraph (dsg.h) ----
+    def _dsg(self, ok, out, setbuf, err, what) -> DsgOut:
+        if not ok:
+            raise RuntimeError(f"{what}: {err.value.decode()}")
+        return DsgOut(int(out[0]), int(out[1]), setbuf[: int(out[5])].copy(), int(out[2]), int(out[3]), int(out[4]))
+
+    def greedy_pp(self, g: CSR, passes: int) -> DsgOut:
+        out, setbuf = np.zeros(6, np.uint64), np.zeros(max(g.n, 1), np.uint32)
+        per = np.zeros(2 * max(passes, 1), np.uint64)
+        err = C.create_string_buffer(256)
+        r = self._dsg(self.lib.ref_greedy_pp(*self._args2(g), passes, out, setbuf, per, err, 256), out, setbuf, err,
+                      "greedy_pp")
+        r.per_pass = [(int(per[2 * i]), int(per[2 * i + 1])) for i in range(passes)]
+        return r
+
+    def cpu_greedy_peel(self, g: CSR) -> tuple[int, int]:
+        a, b = C.c_uint64(0), C.c_uint64(0)
+        if not self.lib.ref_cpu_greedy_peel(*self._args2(g), C.byref(a), C.byref(b)):
+            raise RuntimeError("cpu_greedy_peel failed")
+        return int(a.value), int(b.value)
+
+    def core_exact(self, g: CSR, core: np.ndarray, use_pruning12: bool = True, seed: "DsgOut | None" = None) -> DsgOut:
+        out, setbuf = np.zeros(6, np.uint64), np.zeros(max(g.n, 1), np.uint32)
+        err = C.create_string_buffer(256)
+        c = np.ascontiguousarray(core, np.uint32) if g.n else np.zeros(1, np.uint32)
+        sset = np.ascontiguousarray(seed.set, np.uint32) if seed is not None and len(seed.set) else np.zeros(1, np.uint32)
+        slen = len(seed.set) if seed is not None else 0
+        ok = self.lib.ref_core_exact(*self._args2(g), c, int(use_pruning12), int(seed is not None), sset, slen,
+                                     seed.tri if seed else 0, seed.verts if seed else 0, out, setbuf, err, 256)
+        return self._dsg(ok, out, setbuf, err, "core_exact")
+
+    def exact_densest(self, g: CSR) -> DsgOut:
+        out, setbuf = np.zeros(6, np.uint64), np.zeros(max(g.n, 1), np.uint32)
+        err = C.create_string_buffer(256)
+        return self._dsg(self.lib.ref_exact_densest(*self._args2(g), out, setbuf, err, 256), out, setbuf, err,
+                         "exact_densest")
+
+    def prune_to_core(self, g: CSR, core: np.ndarray, k: int) -> tuple[CSR, np.ndarray, np.ndarray]:
+        rowptr = np.zeros(g.n + 1, np.uint32)
+        col, src = np.zeros(max(g.m, 1), np.uint32), np.zeros(max(g.m, 1), np.uint32)
+        old, cout = np.zeros(max(g.n, 1), np.uint32), np.zeros(max(g.n, 1), np.uint32)
+        c = np.ascontiguousarray(core, np.uint32) if g.n else np.zeros(1, np.uint32)
+        n2, m2, mx = C.c_uint32(0), C.c_uint32(0), C.c_uint32(0)
+        self.lib.ref_prune_to_core(*self._args2(g), c, k, rowptr, col, src, old, cout, C.byref(n2), C.byref(m2),
+                                   C.byref(mx))
+        n2, m2 = int(n2.value), int(m2.value)
+        return (CSR(n2, m2, rowptr[: n2 + 1].copy(), col[:m2].copy(), src[:m2].copy(), int(mx.value)),
+                old[:n2].copy(), cout[:n2].copy())
 
 def _col(g: CSR) -> np.ndarray:
     return g.col if g.m else np.zeros(1, np.uint32)

@@ -5,6 +5,7 @@
 // Each wrapper copies plain arrays into the reference's Graph and calls the reference function named in its comment
 // (one, ref_graph_triangles_omp_rows, runs cpu_triangles_omp's loop over a row range). Used to pin oracle/ga_oracle.c
 // and as the timed reference CPU baseline.
+#include <cstdio>
 #include <cstring>
 
 #include "dsg.h"
@@ -208,6 +209,80 @@ void ref_core_level_density(uint32_t n, uint32_t m, const uint32_t* rowptr, cons
     const Dens d = core_level_density(make_graph(n, m, rowptr, col, src), c, k);
     *num = d.num;
     *den = d.den;
+}
+
+// ---- densest subgraph (dsg.h): Greedy / Greedy++, CoreExact, Exact, prune_to_core ----
+static int dsg_out(const DsgResult& r, uint64_t* out, uint32_t* set, char* err, int errlen) {
+    if (!r.ok) {
+        if (err && errlen > 0) std::snprintf(err, (size_t)errlen, "%s", r.error.c_str());
+        return 0;
+    }
+    out[0] = r.tri;
+    out[1] = r.verts;
+    out[2] = r.flow_calls;
+    out[3] = r.components_searched;
+    out[4] = r.shrinks;
+    out[5] = r.set.size();
+    if (set && !r.set.empty()) std::memcpy(set, r.set.data(), r.set.size() * sizeof(uint32_t));
+    return 1;
+}
+
+// greedy_pp (dsg.h:189; passes = 1 is greedy()). out6 = {tri, verts, flow_calls, components_searched, shrinks,
+// set size}; set: n entries; per_pass: 2 * passes entries (num, den after each pass). Returns 1 if ok.
+int ref_greedy_pp(uint32_t n, uint32_t m, const uint32_t* rowptr, const uint32_t* col, const uint32_t* src,
+                  uint32_t passes, uint64_t* out, uint32_t* set, uint64_t* per_pass, char* err, int errlen) {
+    const DsgResult r = greedy_pp(make_graph(n, m, rowptr, col, src), passes);
+    for (size_t i = 0; i < r.per_pass.size() && per_pass; i++) {
+        per_pass[2 * i] = r.per_pass[i].num;
+        per_pass[2 * i + 1] = r.per_pass[i].den;
+    }
+    return dsg_out(r, out, set, err, errlen);
+}
+
+// cpu_greedy_peel (densest.h:209). Returns 1 if ok.
+int ref_cpu_greedy_peel(uint32_t n, uint32_t m, const uint32_t* rowptr, const uint32_t* col, const uint32_t* src,
+                        uint64_t* best_num, uint64_t* best_den) {
+    const GreedyResult r = cpu_greedy_peel(make_graph(n, m, rowptr, col, src));
+    *best_num = r.best_num;
+    *best_den = r.best_den;
+    return r.ok ? 1 : 0;
+}
+
+// core_exact (dsg.h:449) with the given core numbers; the seed (has_seed != 0) is a DsgResult holding seed_set,
+// seed_tri, seed_verts. Returns 1 if ok.
+int ref_core_exact(uint32_t n, uint32_t m, const uint32_t* rowptr, const uint32_t* col, const uint32_t* src,
+                   const uint32_t* core, int use_pruning12, int has_seed, const uint32_t* seed_set, uint64_t seed_len,
+                   uint64_t seed_tri, uint64_t seed_verts, uint64_t* out, uint32_t* set, char* err, int errlen) {
+    std::vector<uint32_t> c(core, core + n);
+    DsgResult seed;
+    seed.tri = seed_tri;
+    seed.verts = seed_verts;
+    if (seed_len) seed.set.assign(seed_set, seed_set + seed_len);
+    const DsgResult r = core_exact(make_graph(n, m, rowptr, col, src), c, use_pruning12 != 0, has_seed ? &seed : nullptr);
+    return dsg_out(r, out, set, err, errlen);
+}
+
+// exact_densest (dsg.h:404). Returns 1 if ok.
+int ref_exact_densest(uint32_t n, uint32_t m, const uint32_t* rowptr, const uint32_t* col, const uint32_t* src,
+                      uint64_t* out, uint32_t* set, char* err, int errlen) {
+    return dsg_out(exact_densest(make_graph(n, m, rowptr, col, src)), out, set, err, errlen);
+}
+
+// prune_to_core (dsg.h:637) into caller arrays sized for the whole graph (n+1, m, m, n, n); *out_n / *out_m / *maxdeg
+// give the pruned sizes.
+void ref_prune_to_core(uint32_t n, uint32_t m, const uint32_t* rowptr, const uint32_t* col, const uint32_t* src,
+                       const uint32_t* core, uint64_t k, uint32_t* rowptr_out, uint32_t* col_out, uint32_t* src_out,
+                       uint32_t* old_id, uint32_t* core_out, uint32_t* out_n, uint32_t* out_m, uint32_t* maxdeg) {
+    std::vector<uint32_t> c(core, core + n), ids, cores;
+    Graph out;
+    prune_to_core(make_graph(n, m, rowptr, col, src), c, k, out, ids, cores);
+    copy_out(out, rowptr_out, col_out, src_out, maxdeg);
+    if (!ids.empty()) {
+        std::memcpy(old_id, ids.data(), ids.size() * sizeof(uint32_t));
+        std::memcpy(core_out, cores.data(), cores.size() * sizeof(uint32_t));
+    }
+    *out_n = out.n;
+    *out_m = out.m;
 }
 
 }  // extern "C"
