@@ -684,8 +684,10 @@ def run_reference_gpu(args):
     """The reference's own GPU drivers (baseline/_ref/bin, built from its sources for sm_100a by
     baseline/build_reference_gpu.py) against this library's drivers, on the same text files and the same GPU:
     gpu_tc vs ga_tc on R-MAT 22 (kernels v1-v9), gpu_densest vs ga_densest (eps 1/10) on the Holme-Kim n 1.70M graph,
-    gpu_dsg vs ga_dsg (core decomposition) on the Holme-Kim n 8,298 graph. Every program verifies its own results
-    (the reference's against its CPU code); the triangle counts, peel results and core rows must agree."""
+    gpu_dsg vs ga_dsg (core decomposition) on the Holme-Kim n 8,298 graph, and gpu_dsg vs ga_dsg's whole densest-
+    subgraph pipeline on the Holme-Kim n 8,298 and n 1.70M graphs. Every program verifies its own results (the
+    reference's against its CPU code); the triangle counts, peel results, core rows and pipeline subgraphs must
+    agree."""
     import tempfile
     import graph_analyzer_b200 as ga
     ref_bin = os.path.join(ROOT, "baseline", "_ref", "bin")
@@ -702,6 +704,11 @@ def run_reference_gpu(args):
          ["gpu_densest", "ga_densest"], lambda p: [p, "1", "10", "--repeats", "3", "--no-greedy"]),
         ("cores_hk8298", lambda: ga.graph_from_pairs(8298, ga.gen_holme_kim(8298, 12, 12, 0.0, 0.5, seed=SEED)),
          ["gpu_dsg", "ga_dsg"], lambda p: [p, "--repeats", "3", "--no-exact", "--no-greedy", "--no-greedypp"]),
+        # the whole densest-subgraph pipeline: cores, greedy lower bound, prune, Greedy++ (10 passes), seeded CoreExact
+        ("dsg_hk8298", lambda: ga.graph_from_pairs(8298, ga.gen_holme_kim(8298, 12, 12, 0.0, 0.5, seed=SEED)),
+         ["gpu_dsg", "ga_dsg"], lambda p: [p, "--repeats", "3"]),
+        ("dsg_hk1.7M", lambda: ga.graph_from_pairs(1_700_000, ga.gen_holme_kim(1_700_000, 6, 7, 0.54, 0.3, seed=SEED)),
+         ["gpu_dsg", "ga_dsg"], lambda p: [p, "--repeats", "3"]),
     ]
     ok = True
     for name, make, (ref_prog, our_prog), argv in runs:
@@ -732,6 +739,27 @@ def run_reference_gpu(args):
                           "speedup": float(ref_best[5]) / float(our_best[5]),
                           "same_triangles": len({r[4] for r in tc["reference"] + tc["ours"]}) == 1}
         ok &= out["tc_best"]["same_triangles"]
+    # densest-subgraph pipeline: stage times side by side (the reference's CPU stages vs this library's) and the
+    # results, which must be the same subgraphs
+    stages = [("gpu_core_decomp", "gpu_core_decomp"), ("cpu_greedy", "greedy"), ("prune_kcore", "prune_kcore"),
+              ("cpu_greedy_pp_pruned", "greedy_pp_pruned"),
+              ("cpu_core_exact_pruned_seeded", "core_exact_pruned_seeded"), ("pipeline_gpu_core", "pipeline_gpu_core")]
+    for name in ("dsg_hk8298", "dsg_hk1.7M"):
+        d = out.get(name, {})
+        if not (d.get("reference") and d.get("ours")):
+            continue
+        ref_rows = {r[0]: r for r in d["reference"]}
+        our_rows = {r[0]: r for r in d["ours"]}
+        summ = {}
+        for rn, on in stages:
+            if rn in ref_rows and on in our_rows:
+                a, b = ref_rows[rn], our_rows[on]
+                summ[on] = {"reference_ms": float(a[7]), "ours_ms": float(b[7]), "same_result": a[2:6] == b[2:6]}
+                ok &= summ[on]["same_result"]
+        if "pipeline_gpu_core" in summ:
+            p = summ["pipeline_gpu_core"]
+            p["speedup"] = p["reference_ms"] / max(p["ours_ms"], 1e-9)
+        out[name + "_stages"] = summ
     out["all_verified"] = bool(ok)
     print(json.dumps(out), flush=True)
     return 0 if ok else 1

@@ -1,12 +1,15 @@
 // ga_densest - triangle-density batch peeling driver over the C ABI; replaces the reference's gpu_densest.cu.
 // usage: ga_densest graph.txt [eps_num eps_den] [--pinned] [--no-burnin] [--repeats N] [--no-greedy] [--verbose]
 //   eps = eps_num/eps_den (default 1/10): a vertex is peeled when its triangle participation is at most (1+eps) times
-//   the average (densest.h:138-160). --no-greedy is accepted for command-line compatibility (the CPU greedy peel is
-//   not part of this library, so there is never a greedy row).
+//   the average (densest.h:138-160). --no-greedy: no greedy row and no density ratio.
 // Rows (stdout, CSV, the reference's columns, printed only if everything verified):
 //   impl,graph,n,m,best_triangles,best_vertices,density,rounds,time_ms,h2d_ms,total_ms
 //   gpu_batch_peel       the device-resident loop, rounds in a CUDA graph with a conditional node (default)
 //   gpu_batch_peel_host  the same rounds driven from the host, one small read per round (the reference's structure)
+//   greedy_peel          Charikar's greedy peel, the quality baseline (the reference's cpu_greedy_peel,
+//                        densest.h:193-252): device core numbers and triangle lists, one removal sequence per core
+//                        level on the host threads; rounds = n removals, one timed call, h2d_ms = 0. The density
+//                        ratio batch peel / greedy goes to stderr, as in the reference.
 // (suffix "_pinned" with --pinned). time_ms = best of N (default 5) calls of ga_batch_peel after one untimed verified
 // call, host wall clock around the synchronous call: the round-0 count, every round, the final read of the result;
 // EXCLUDES the upload (h2d_ms), the one-time build of the triangle incidence lists (first call) and removed_round's
@@ -38,13 +41,13 @@ bool same(const Run& a, const Run& b) {
 }  // namespace
 
 int main(int argc, char** argv) {
-    bool pinned = false, burnin = true, verbose = false;
+    bool pinned = false, burnin = true, verbose = false, greedy = true;
     int repeats = 5;
     std::vector<const char*> pos;
     for (int i = 1; i < argc; i++) {
         if (std::strcmp(argv[i], "--pinned") == 0) pinned = true;
         else if (std::strcmp(argv[i], "--no-burnin") == 0) burnin = false;
-        else if (std::strcmp(argv[i], "--no-greedy") == 0) {}
+        else if (std::strcmp(argv[i], "--no-greedy") == 0) greedy = false;
         else if (std::strcmp(argv[i], "--verbose") == 0) verbose = true;
         else if (std::strcmp(argv[i], "--repeats") == 0 && i + 1 < argc) repeats = std::max(1, std::atoi(argv[++i]));
         else pos.push_back(argv[i]);
@@ -111,6 +114,21 @@ int main(int argc, char** argv) {
         if (!ok) {
             std::fprintf(stderr, "VERIFICATION FAILED - no timing rows printed\n");
             return 1;
+        }
+        if (greedy) {
+            ga_dsg_result gr{};
+            const double t0 = cli::now_ms();
+            ga::check(ga_greedy_pp(up.g, 1, &gr, nullptr, nullptr));
+            const double ms = cli::now_ms() - t0;
+            const uint64_t gden = gr.verts ? gr.verts : g.n;   // no triangle: the whole graph, 0 / n
+            char buf[1024];
+            std::snprintf(buf, sizeof buf, "greedy_peel,%s,%u,%u,%llu,%llu,%.6f,%u,%.3f,%.3f,%.3f", path, g.n, g.m,
+                          (unsigned long long)gr.tri, (unsigned long long)gden, ga::density_value(gr.tri, gden), g.n,
+                          ms, 0.0, ms);
+            rows.push_back(buf);
+            const double dg = ga::density_value(first.r.best_num, first.r.best_den), dr = ga::density_value(gr.tri, gden);
+            std::fprintf(stderr, "density ratio gpu/greedy = %.6f (gpu %.6f, greedy %.6f)\n", dr > 0 ? dg / dr : 0.0,
+                         dg, dr);
         }
         for (auto& r : rows) std::puts(r.c_str());
         std::fflush(stdout);

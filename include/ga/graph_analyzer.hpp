@@ -13,6 +13,10 @@
 //                                                        cpu_triangle_participation (densest.h:81)
 //   batch_peel_loop(n, T_full, num, den, DeviceGraph&)   batch_peel_loop (densest.h:279-303) + GpuBackend
 //   core_decomp_loop_inc(n, T_full, DeviceGraph&, core)  core_decomp_loop_inc (dsg.h:724-751) + GpuCoreBackendInc
+//   Dens, dens_cmp, dens_gt, dens_ceil, DsgResult        dsg.h:33-59
+//   greedy, greedy_pp, core_exact, exact_densest         dsg.h:189-250, 463-627, 405-428 (device triangle lists)
+//   prune_to_core                                        dsg.h:638-645
+//   GreedyResult, greedy_peel                            cpu_greedy_peel, densest.h:193-252 (the same greedy)
 //
 // Everything lives in namespace ga; define GA_B200_GLOBAL_NAMES before including to also get the reference's
 // unqualified names. Errors follow the reference: functions that returned bool return false (load_graph), results
@@ -229,12 +233,147 @@ inline CoreLoopResult core_decomp_loop_inc(uint32_t n, uint64_t T_full, DeviceGr
     return r;
 }
 
+// ---- densest subgraph by triangle density (dsg.h) -----------------------------------------------------------------
+struct Dens {
+    uint64_t num = 0, den = 0;   // triangles / vertices; den == 0 means "no subgraph", density 0
+};
+inline int dens_cmp(Dens a, Dens b) {
+    if (a.den == 0) a = Dens{0, 1};
+    if (b.den == 0) b = Dens{0, 1};
+    const unsigned __int128 l = (unsigned __int128)a.num * b.den, r = (unsigned __int128)b.num * a.den;
+    return l < r ? -1 : (l > r ? 1 : 0);
+}
+inline bool dens_gt(Dens a, Dens b) { return dens_cmp(a, b) > 0; }
+inline uint64_t dens_ceil(Dens d) { return d.den == 0 ? 0 : (d.num + d.den - 1) / d.den; }
+inline double dens_value(Dens d) { return density_value(d.num, d.den); }
+
+struct DsgResult {
+    uint64_t tri = 0, verts = 0;          // best subgraph: triangles / vertices (0/0 = graph without triangles)
+    std::vector<uint32_t> set;            // its vertices, ascending
+    std::vector<Dens> per_pass;           // greedy_pp only: best density after pass 1, 2, ...
+    uint32_t flow_calls = 0, components_searched = 0, shrinks = 0;
+    bool ok = true;
+    std::string error;
+    Dens dens() const { return Dens{tri, verts}; }
+};
+
+namespace detail {
+inline DsgResult dsg_result(ga_status s, const ga_dsg_result& res, std::vector<uint32_t>& set) {
+    DsgResult r;
+    if (s != GA_OK) { r.ok = false; r.error = ga_last_error(); return r; }
+    r.tri = res.tri;
+    r.verts = res.verts;
+    r.flow_calls = res.flow_calls;
+    r.components_searched = res.components_searched;
+    r.shrinks = res.shrinks;
+    set.resize(res.verts);
+    r.set = std::move(set);
+    return r;
+}
+}  // namespace detail
+
+// greedy_pp (dsg.h:189-249) / greedy (dsg.h:250) on a device-resident graph.
+inline DsgResult greedy_pp(DeviceGraph& d, uint32_t passes) {
+    ga_dsg_result res{};
+    std::vector<uint32_t> set(d.n());
+    std::vector<uint64_t> per(2ull * (passes ? passes : 1));
+    DsgResult r = detail::dsg_result(ga_greedy_pp(d.handle(), passes, &res, set.data(), per.data()), res, set);
+    if (r.ok)
+        for (uint32_t i = 0; i < passes; i++) r.per_pass.push_back(Dens{per[2 * i], per[2 * i + 1]});
+    return r;
+}
+inline DsgResult greedy_pp(const Graph& g, uint32_t passes) {
+    DeviceGraph d(g);
+    return greedy_pp(d, passes);
+}
+inline DsgResult greedy(const Graph& g) { return greedy_pp(g, 1); }
+
+// core_exact (dsg.h:463-627): core = the graph's core numbers (empty: computed on the device); seed as in the
+// reference (a verified lower bound, e.g. a Greedy++ result).
+inline DsgResult core_exact(DeviceGraph& d, const std::vector<uint32_t>& core, bool use_pruning12 = true,
+                            const DsgResult* seed = nullptr) {
+    if (!core.empty() && core.size() != d.n()) {
+        DsgResult r;
+        r.ok = false;
+        r.error = "core[] has the wrong size";
+        return r;
+    }
+    ga_dsg_seed sd{};
+    if (seed && seed->ok) sd = ga_dsg_seed{seed->set.data(), seed->set.size(), seed->tri, seed->verts};
+    ga_dsg_result res{};
+    std::vector<uint32_t> set(d.n());
+    return detail::dsg_result(ga_core_exact(d.handle(), core.empty() ? nullptr : core.data(), use_pruning12 ? 1 : 0,
+                                            seed ? &sd : nullptr, &res, set.data()), res, set);
+}
+inline DsgResult core_exact(const Graph& g, const std::vector<uint32_t>& core, bool use_pruning12 = true,
+                            const DsgResult* seed = nullptr) {
+    DeviceGraph d(g);
+    return core_exact(d, core, use_pruning12, seed);
+}
+
+// exact_densest (dsg.h:405-428).
+inline DsgResult exact_densest(DeviceGraph& d) {
+    ga_dsg_result res{};
+    std::vector<uint32_t> set(d.n());
+    return detail::dsg_result(ga_exact_densest(d.handle(), &res, set.data()), res, set);
+}
+inline DsgResult exact_densest(const Graph& g) {
+    DeviceGraph d(g);
+    return exact_densest(d);
+}
+
+// prune_to_core (dsg.h:638-645): the subgraph of {v : core[v] >= k}, its old ids and restricted core numbers.
+inline void prune_to_core(const Graph& g, const std::vector<uint32_t>& core, uint64_t k, Graph& out,
+                          std::vector<uint32_t>& old_id, std::vector<uint32_t>& core_out) {
+    if (core.size() != g.n) throw Error(GA_ERR_INVALID_ARGUMENT, "core[] has the wrong size");
+    old_id.assign(g.n, 0);
+    core_out.assign(g.n, 0);
+    ga_host_graph* h = nullptr;
+    check(ga_prune_to_core(g.rowptr.data(), g.m ? g.col.data() : nullptr, g.n, g.m, core.data(), k, &h,
+                           old_id.data(), core_out.data()));
+    out.n = h->n;
+    out.m = h->m;
+    out.max_out_degree = h->max_out_degree;
+    out.rowptr.assign(h->rowptr, h->rowptr + h->n + 1);
+    out.col.assign(h->col, h->col + h->m);
+    out.src.assign(h->src, h->src + h->m);
+    ga_host_graph_free(h);
+    old_id.resize(out.n);
+    core_out.resize(out.n);
+}
+
+// cpu_greedy_peel (densest.h:193-252): the best density of Charikar's peel. Same numbers as greedy(); with no
+// triangle at all the reference records the whole graph (0 / n).
+struct GreedyResult {
+    uint64_t best_num = 0, best_den = 0;
+    bool ok = true;
+    std::string error;
+};
+inline GreedyResult greedy_peel(DeviceGraph& d) {
+    GreedyResult r;
+    const DsgResult g = greedy_pp(d, 1);
+    if (!g.ok) { r.ok = false; r.error = g.error; return r; }
+    r.best_num = g.tri;
+    r.best_den = g.verts ? g.verts : d.n();
+    return r;
+}
+
 }  // namespace ga
 
 #ifdef GA_B200_GLOBAL_NAMES
 using ga::batch_peel_loop;
 using ga::build_graph_from_edges;
 using ga::core_decomp_loop_inc;
+using ga::core_exact;
+using ga::Dens;
+using ga::dens_ceil;
+using ga::dens_cmp;
+using ga::dens_gt;
+using ga::DsgResult;
+using ga::exact_densest;
+using ga::greedy;
+using ga::greedy_pp;
+using ga::prune_to_core;
 using ga::CoreLoopResult;
 using ga::density_value;
 using ga::Graph;

@@ -106,6 +106,9 @@ class Oracle(_Base):
         L.or_core_level_density.restype = None
         L.or_core_level_density.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, _u32p, _u32p, C.c_uint32,
                                             C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        L.or_greedy_pp.restype = C.c_int
+        L.or_greedy_pp.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, _u32p, C.c_uint32, C.POINTER(C.c_uint64),
+                                   C.POINTER(C.c_uint64), _u32p, _u64p]
 
     # graph.h
     def canonical_edges(self, pairs: np.ndarray) -> np.ndarray:
@@ -199,6 +202,14 @@ class Oracle(_Base):
         c = np.ascontiguousarray(core, np.uint32) if g.n else np.zeros(1, np.uint32)
         self.lib.or_core_level_density(g.n, g.m, g.rowptr, _col(g), _src(g), c, k, C.byref(a), C.byref(b))
         return int(a.value), int(b.value)
+
+    def greedy_pp(self, g: CSR, passes: int) -> DsgOut:
+        a, b = C.c_uint64(0), C.c_uint64(0)
+        setbuf, per = np.zeros(max(g.n, 1), np.uint32), np.zeros(2 * max(passes, 1), np.uint64)
+        if self.lib.or_greedy_pp(g.n, g.m, g.rowptr, _col(g), _src(g), passes, C.byref(a), C.byref(b), setbuf, per):
+            raise RuntimeError("greedy_pp: triangle bookkeeping inconsistent")
+        return DsgOut(int(a.value), int(b.value), setbuf[: int(b.value)].copy(),
+                      per_pass=[(int(per[2 * i]), int(per[2 * i + 1])) for i in range(passes)])
 
 
 class Reference(_Base):

@@ -451,3 +451,99 @@ void or_core_level_density(uint32_t n, uint32_t m, const uint32_t* rowptr, const
     *den = cnt;
     free(in);
 }
+
+/* Common neighbours w > a of v and a (for_common_above, densest.h:176-191, merge form): writes them to out. */
+static size_t common_above(const uint32_t* nv, uint32_t dv, const uint32_t* na, uint32_t da, uint32_t a,
+                           uint32_t* out) {
+    const uint32_t *ap = upper_u32(nv, nv + dv, a), *ae = nv + dv;
+    const uint32_t *bp = upper_u32(na, na + da, a), *be = na + da;
+    size_t c = 0;
+    while (ap < ae && bp < be) {
+        if (*ap < *bp) ++ap;
+        else if (*ap > *bp) ++bp;
+        else { out[c++] = *ap; ++ap; ++bp; }
+    }
+    return c;
+}
+
+static int dens_gt_u(uint64_t an, uint64_t ad, uint64_t bn, uint64_t bd) {
+    if (ad == 0) { an = 0; ad = 1; }
+    if (bd == 0) { bn = 0; bd = 1; }
+    return (unsigned __int128)an * bd > (unsigned __int128)bn * ad;
+}
+
+/* greedy_pp (dsg.h:189-249): `passes` passes of removing the alive vertex with the smallest load + triangle degree
+ * (ties: smaller id), loads += the degree at removal; the best (strictly denser, dsg.h:212) residual over all passes.
+ * out: best_num, best_den; set: n entries (the best residual, ascending); per_pass: 2 * passes. Returns 0, or -1 if
+ * the triangle bookkeeping disagrees (dsg.h:232). */
+int or_greedy_pp(uint32_t n, uint32_t m, const uint32_t* rowptr, const uint32_t* col, const uint32_t* src,
+                 uint32_t passes, uint64_t* best_num, uint64_t* best_den, uint32_t* set, uint64_t* per_pass) {
+    const size_t N = n ? n : 1;
+    uint32_t* urow = (uint32_t*)malloc((size_t)(n + 1) * sizeof(uint32_t));
+    uint32_t* ucol = (uint32_t*)malloc((size_t)(2ull * m ? 2ull * m : 1) * sizeof(uint32_t));
+    or_undirected_csr(n, m, col, src, urow, ucol);
+    uint64_t* tri0 = (uint64_t*)malloc(N * sizeof(uint64_t));
+    const uint64_t T0 = or_triangle_degrees(n, m, rowptr, col, src, tri0);
+    uint64_t* load = (uint64_t*)calloc(N, sizeof(uint64_t));
+    uint64_t* next_load = (uint64_t*)calloc(N, sizeof(uint64_t));
+    uint64_t* cur = (uint64_t*)malloc(N * sizeof(uint64_t));
+    uint8_t* alive = (uint8_t*)malloc(N);
+    uint8_t* flag = (uint8_t*)calloc(N, 1);
+    uint32_t *order = (uint32_t*)malloc(N * sizeof(uint32_t)), *best_order = (uint32_t*)malloc(N * sizeof(uint32_t));
+    uint32_t *touched = (uint32_t*)malloc(N * sizeof(uint32_t)), *buf = (uint32_t*)malloc(N * sizeof(uint32_t));
+    uint64_t bn = 0, bd = 0, best_cut = 0;
+    int rc = 0;
+    heap_t h = {0, 0, 0};
+    for (uint32_t pass = 1; pass <= passes && rc == 0; pass++) {
+        memcpy(cur, tri0, (size_t)n * sizeof(uint64_t));
+        memset(alive, 1, n);
+        uint64_t t = T0, nalive = n, norder = 0, cut = 0;
+        int improved = 0;
+        h.n = 0;
+        for (uint32_t v = 0; v < n; v++) h_push(&h, load[v] + cur[v], v);
+        while (nalive > 0 && rc == 0) {
+            if (dens_gt_u(t, nalive, bn, bd)) { bn = t; bd = nalive; improved = 1; cut = norder; }
+            const hentry top = h_pop(&h);
+            const uint32_t v = top.v;
+            if (!alive[v] || load[v] + cur[v] != top.key) continue;
+            uint64_t found = 0;
+            size_t nt = 0;
+            const uint32_t* nv = ucol + urow[v];
+            const uint32_t dv = urow[v + 1] - urow[v];
+            for (uint32_t k = 0; k < dv && rc == 0; k++) {
+                const uint32_t a = nv[k];
+                if (!alive[a]) continue;
+                const size_t c = common_above(nv, dv, ucol + urow[a], urow[a + 1] - urow[a], a, buf);
+                for (size_t i = 0; i < c; i++) {
+                    const uint32_t w = buf[i];
+                    if (!alive[w]) continue;
+                    found++;
+                    if (cur[a] == 0 || cur[w] == 0) { rc = -1; break; }
+                    cur[a]--;
+                    cur[w]--;
+                    if (!flag[a]) { flag[a] = 1; touched[nt++] = a; }
+                    if (!flag[w]) { flag[w] = 1; touched[nt++] = w; }
+                }
+            }
+            if (rc == 0 && found != cur[v]) rc = -1;
+            next_load[v] = load[v] + cur[v];
+            alive[v] = 0;
+            order[norder++] = v;
+            t -= cur[v];
+            nalive--;
+            for (size_t i = 0; i < nt; i++) { flag[touched[i]] = 0; h_push(&h, load[touched[i]] + cur[touched[i]], touched[i]); }
+        }
+        if (improved) { memcpy(best_order, order, (size_t)n * sizeof(uint32_t)); best_cut = cut; }
+        memcpy(load, next_load, (size_t)n * sizeof(uint64_t));
+        if (per_pass) { per_pass[2 * (pass - 1)] = bn; per_pass[2 * (pass - 1) + 1] = bd; }
+    }
+    *best_num = bn;
+    *best_den = bd;
+    if (set && bd) {
+        memcpy(set, best_order + best_cut, (size_t)(n - best_cut) * sizeof(uint32_t));
+        qsort(set, (size_t)(n - best_cut), sizeof(uint32_t), cmp_u32);
+    }
+    free(h.a); free(buf); free(touched); free(best_order); free(order); free(flag); free(alive); free(cur);
+    free(next_load); free(load); free(tri0); free(ucol); free(urow);
+    return rc;
+}

@@ -88,6 +88,12 @@ uint64_t or_triangles_omp(uint32_t n, const uint32_t* rowptr, const uint32_t* co
 /* Number of OpenMP threads or_triangles_omp uses (1 without OpenMP). */
 int or_num_threads(void);
 
+/* greedy_pp (dsg.h:189-249; passes = 1 is greedy(), dsg.h:250): the best residual subgraph over `passes` passes of
+ * removing the vertex with the smallest load + triangle degree. set: n entries (best_den ascending ids written);
+ * per_pass: 2 * passes or NULL. Returns 0, or -1 if the triangle bookkeeping disagrees. */
+int or_greedy_pp(uint32_t n, uint32_t m, const uint32_t* rowptr, const uint32_t* col, const uint32_t* src,
+                 uint32_t passes, uint64_t* best_num, uint64_t* best_den, uint32_t* set, uint64_t* per_pass);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,6 +1,6 @@
 // api_check.cpp - the reference-names C++ surface (include/ga/graph_analyzer.hpp) used the way the reference's own
 // drivers use graph.h / densest.h / dsg.h: load_graph, a device graph, batch_peel_loop with the CPU count as T_full,
-// core_decomp_loop_inc, and the support helpers. Prints one line per result for the test to compare with the golden
+// core_decomp_loop_inc, the support helpers and the densest-subgraph pipeline of gpu_dsg. Prints one line per result for the test to compare with the golden
 // outputs. usage: api_check graph.txt eps_num eps_den T_full
 #define GA_B200_GLOBAL_NAMES
 #include "ga/graph_analyzer.hpp"
@@ -32,6 +32,24 @@ int main(int argc, char** argv) {
         std::vector<uint64_t> deg;
         std::printf("supports %llu %llu\n", (unsigned long long)d.edge_support(sup),
                     (unsigned long long)d.triangle_degrees(deg));
+        // the gpu_dsg pipeline (gpu_dsg.cu:318-369) with the dsg.h names: lower bound, prune, Greedy++, CoreExact
+        std::vector<uint8_t> in(g.n);
+        uint64_t kverts = 0;
+        for (uint32_t v = 0; v < g.n; v++) kverts += in[v] = core[v] >= c.kmax;
+        std::vector<uint32_t> tri;
+        Dens lb{d.triangle_participation(in, tri), kverts};
+        DsgResult gr = greedy(g);
+        if (!gr.ok) { std::fprintf(stderr, "greedy: %s\n", gr.error.c_str()); return 1; }
+        if (dens_gt(gr.dens(), lb)) lb = gr.dens();
+        Graph gp;
+        std::vector<uint32_t> old_id, core_p;
+        prune_to_core(g, core, dens_ceil(lb), gp, old_id, core_p);
+        DsgResult gpp = greedy_pp(gp, 10);
+        DsgResult ex = core_exact(gp, core_p, true, &gpp);
+        if (!gpp.ok || !ex.ok) { std::fprintf(stderr, "dsg: %s%s\n", gpp.error.c_str(), ex.error.c_str()); return 1; }
+        std::printf("dsg %llu %llu %u %u %llu %llu %llu %llu %u\n", (unsigned long long)gr.tri,
+                    (unsigned long long)gr.verts, gp.n, gp.m, (unsigned long long)gpp.tri, (unsigned long long)gpp.verts,
+                    (unsigned long long)ex.tri, (unsigned long long)ex.verts, ex.flow_calls);
         // the refusals of batch_peel_loop (densest.h:65-78, 283-287): wrong T_full, eps out of range
         PeelResult bad = batch_peel_loop(g.n, T_full + 1, num, den, d);
         PeelResult bad_eps = batch_peel_loop(g.n, T_full, 1, 0, d);

@@ -3,6 +3,7 @@ gpu_dsg: built against the C ABI, same usage and CSV columns; on a GPU their row
 golden fixtures."""
 from __future__ import annotations
 
+import json
 import os
 import subprocess
 
@@ -89,24 +90,59 @@ def test_ga_densest_rows(ga, oracle, cuda_ok, fx, eps):
     r = _run("ga_densest", fixture_path(fx), str(eps[0]), str(eps[1]), "--no-burnin", "--repeats", "2")
     assert r.returncode == 0, r.stderr
     rows = _rows("ga_densest", r.stdout)
-    assert [x["impl"] for x in rows] == ["gpu_batch_peel", "gpu_batch_peel_host"]
-    o = oracle.batch_peel(ga.load_graph(fixture_path(fx)), *eps)
-    for x in rows:
+    assert [x["impl"] for x in rows] == ["gpu_batch_peel", "gpu_batch_peel_host", "greedy_peel"]
+    g = ga.load_graph(fixture_path(fx))
+    o = oracle.batch_peel(g, *eps)
+    for x in rows[:2]:
         assert (int(x["best_triangles"]), int(x["best_vertices"]), int(x["rounds"])) == (o.best_num, o.best_den,
                                                                                          o.rounds)
+    w = oracle.greedy_pp(g, 1)                                   # cpu_greedy_peel's best (densest.h:209-252)
+    assert (int(rows[2]["best_triangles"]), int(rows[2]["best_vertices"]), int(rows[2]["rounds"])) == (
+        w.tri, w.verts, g.n)
+    assert "density ratio gpu/greedy" in r.stderr
+    r = _run("ga_densest", fixture_path(fx), str(eps[0]), str(eps[1]), "--no-burnin", "--repeats", "1", "--no-greedy")
+    assert [x["impl"] for x in _rows("ga_densest", r.stdout)] == ["gpu_batch_peel", "gpu_batch_peel_host"]
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("fx", FIXTURES)
 def test_ga_dsg_rows(ga, oracle, cuda_ok, fx):
-    r = _run("ga_dsg", fixture_path(fx), "--no-burnin", "--repeats", "2", "--no-exact", "--T", "5")
+    """Core rows against the oracle; the pipeline rows (greedy, prune, Greedy++, seeded CoreExact, the full-graph
+    check) against the reference's outputs for the same stages (tests/golden/dsg.json)."""
+    r = _run("ga_dsg", fixture_path(fx), "--no-burnin", "--repeats", "2", "--verify-full")
     assert r.returncode == 0, r.stderr
-    rows = _rows("ga_dsg", r.stdout)
-    assert [x["impl"] for x in rows] == ["gpu_core_decomp", "gpu_core_decomp_host"]
+    rows = {x["impl"]: x for x in _rows("ga_dsg", r.stdout)}
+    assert list(rows) == ["gpu_core_decomp", "gpu_core_decomp_host", "greedy", "prune_kcore", "greedy_pp_pruned",
+                          "core_exact_pruned_seeded", "pipeline_gpu_core", "core_exact_full"]
     g = ga.load_graph(fixture_path(fx))
     core, kmax, rounds = oracle.core_levels(g)
     tri, verts = oracle.core_level_density(g, core, kmax)
-    for x in rows:
+    for name in ("gpu_core_decomp", "gpu_core_decomp_host"):
+        x = rows[name]
         assert (int(x["kmax"]), int(x["rounds"])) == (kmax, rounds)
         assert (int(x["triangles"]), int(x["vertices"])) == (tri, verts)
         assert np.isclose(float(x["density"]), tri / verts if verts else 0.0, rtol=1e-6)
+    with open(os.path.join(ROOT, "tests", "golden", "dsg.json")) as f:
+        rec = {x["name"]: x for x in json.load(f)["graphs"]}[fx]
+    p = rec["pipeline"]
+
+    def tv(x):
+        return int(x["triangles"]), int(x["vertices"])
+
+    assert tv(rows["greedy"]) == (rec["greedy"]["tri"], rec["greedy"]["verts"])
+    x = rows["prune_kcore"]
+    assert (int(x["n"]), int(x["m"]), int(x["triangles"]), int(x["rounds"])) == (
+        p["pruned_n"], p["pruned_m"], p["pruned_triangles"], p["k"])
+    assert tv(rows["greedy_pp_pruned"]) == (p["greedy_pp"]["tri"], p["greedy_pp"]["verts"])
+    ex = p["core_exact_seeded"]
+    assert tv(rows["core_exact_pruned_seeded"]) + (int(rows["core_exact_pruned_seeded"]["rounds"]),) == (
+        ex["tri"], ex["verts"], ex["flow_calls"])
+    assert tv(rows["pipeline_gpu_core"]) == (ex["tri"], ex["verts"])
+    full = rec["core_exact"]
+    assert tv(rows["core_exact_full"]) + (int(rows["core_exact_full"]["rounds"]),) == (
+        full["tri"], full["verts"], full["flow_calls"])
+    # --no-exact stops after the pruning and Greedy++ (gpu_dsg.cu's flags)
+    r = _run("ga_dsg", fixture_path(fx), "--no-burnin", "--repeats", "1", "--no-exact", "--T", "5")
+    assert r.returncode == 0, r.stderr
+    assert [x["impl"] for x in _rows("ga_dsg", r.stdout)] == ["gpu_core_decomp", "gpu_core_decomp_host", "greedy",
+                                                              "prune_kcore", "greedy_pp_pruned"]

@@ -1,15 +1,16 @@
 """The reference-names C++ surface (include/ga/graph_analyzer.hpp: Graph, load_graph, PeelResult, batch_peel_loop,
-core_decomp_loop_inc) compiled into a small program as a maintainer of the reference would, linked against the
+core_decomp_loop_inc, greedy / greedy_pp / prune_to_core / core_exact) compiled into a small program as a maintainer of the reference would, linked against the
 library; on a GPU its results must equal the golden outputs of the reference's own code."""
 from __future__ import annotations
 
+import json
 import os
 import subprocess
 
 import numpy as np
 import pytest
 
-from conftest import FIXTURES, ROOT, fixture_path, golden_arrays
+from conftest import FIXTURES, GOLDEN, ROOT, fixture_path, golden_arrays
 
 LIB_DIR = os.path.join(ROOT, "graph_analyzer_b200", "_lib")
 
@@ -49,3 +50,10 @@ def test_reference_names_match_golden(api_check, golden, cuda_ok, name):
     assert out["cores"].split() == [str(w["kmax"]), str(w["core_rounds"]), _hash(a["core"])]
     assert out["supports"].split() == [str(w["triangles"])] * 2
     assert out["refusals"].split() == ["0", "0"]
+    with open(os.path.join(GOLDEN, "dsg.json")) as f:
+        rec = {x["name"]: x for x in json.load(f)["graphs"]}[name]
+    p = rec["pipeline"]
+    assert out["dsg"].split() == [str(x) for x in (
+        rec["greedy"]["tri"], rec["greedy"]["verts"], p["pruned_n"], p["pruned_m"], p["greedy_pp"]["tri"],
+        p["greedy_pp"]["verts"], p["core_exact_seeded"]["tri"], p["core_exact_seeded"]["verts"],
+        p["core_exact_seeded"]["flow_calls"])]

@@ -170,3 +170,15 @@ def test_host_refusals(ga, prepared):
         ga.exact_densest_host(3, np.array([[0, 1, 3]], np.uint32))
     with pytest.raises(ga.GAError):
         ga.exact_densest_host(3, np.array([[0, 1, 1]], np.uint32))
+
+
+@pytest.mark.parametrize("name", list(BY_NAME))
+def test_oracle_greedy_pinned(oracle, ga, name):
+    """The oracle's C restatement of greedy_pp (the checker of the larger GPU cases) against the golden vectors."""
+    rec = BY_NAME[name]
+    g = dsg_graph(ga, rec)
+    check(oracle.greedy_pp(g, 1), rec["greedy"])
+    for T, want in rec["greedy_pp"].items():
+        r = oracle.greedy_pp(g, int(T))
+        check(r, want)
+        assert [list(p) for p in r.per_pass] == want["per_pass"]
