@@ -12,11 +12,12 @@ namespace ga {
 
 // Count (WRITE = false: fptr[v] = count, fptr[n] = 0, for an exclusive scan) or write (WRITE = true: at fptr[v])
 // the entries of v's incidence list whose triangle lies in v's core level: both other corners have core >= core[v].
-// One warp per vertex; a ballot keeps the entries in list order.
+// Written entries name a corner of v's level by its level-local id (local[]) and a corner of a higher level as
+// UINT32_MAX, the form the host's per-level removals read. One warp per vertex; a ballot keeps the list order.
 template <bool WRITE>
 __global__ void k_level_entries(const uint2* __restrict__ inc, const unsigned long long* __restrict__ inc_ptr,
-                                const uint32_t* __restrict__ core, uint32_t n, unsigned long long* __restrict__ fptr,
-                                uint2* __restrict__ fent) {
+                                const uint32_t* __restrict__ core, const uint32_t* __restrict__ local, uint32_t n,
+                                unsigned long long* __restrict__ fptr, uint2* __restrict__ fent) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t v = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
@@ -32,7 +33,9 @@ __global__ void k_level_entries(const uint2* __restrict__ inc, const unsigned lo
                 keep = core[t.x] >= k && core[t.y] >= k;
             }
             const uint32_t mask = __ballot_sync(GA_FULL_MASK, keep);
-            if (WRITE && keep) fent[out + __popc(mask & ((1u << lane) - 1u))] = t;
+            if (WRITE && keep)
+                fent[out + __popc(mask & ((1u << lane) - 1u))] =
+                    make_uint2(core[t.x] == k ? local[t.x] : GA_EMPTY, core[t.y] == k ? local[t.y] : GA_EMPTY);
             out += __popc(mask);
         }
         if (!WRITE && lane == 0) fptr[v] = out;
@@ -167,26 +170,33 @@ ga_status ga_greedy_pp(ga_graph* g, uint32_t passes, ga_dsg_result* res, uint32_
     uint64_t T;
     GA_TRY(incidence_lists(g, &inc, &inc_ptr, &T));
     cudaStream_t st = g->stream;
-    std::vector<uint32_t> core(n), lent, fent;
+    std::vector<uint32_t> core(n), local(n), lent, fent;
     std::vector<uint64_t> lptr((size_t)n + 1), fptr;
     {
-        Scratch s_ptr(st), s_ent(st);
+        // level-local ids from the core numbers (host), so the device writes the levels' lists in the form the
+        // host's removals read
+        GA_TRY(download(core.data(), d_core, (size_t)n * 4, st));
+        GA_CUDA(cudaStreamSynchronize(st));
+        dsg::level_ranks(n, core.data(), local.data());
+        Scratch s_ptr(st), s_ent(st), s_local(st);
         unsigned long long* d_lptr;
         uint2* d_lent;
+        uint32_t* d_local;
+        GA_TRY(s_local.alloc(&d_local, n));
+        GA_CUDA(cudaMemcpyAsync(d_local, local.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st));
         GA_TRY(s_ptr.alloc(&d_lptr, (size_t)n + 1));
         const unsigned grid = grid_for((uint64_t)n * 32, 256);
-        k_level_entries<false><<<grid, 256, 0, st>>>(inc, inc_ptr, d_core, n, d_lptr, nullptr);
+        k_level_entries<false><<<grid, 256, 0, st>>>(inc, inc_ptr, d_core, nullptr, n, d_lptr, nullptr);
         GA_CUDA(cudaGetLastError());
         GA_TRY(scan_u64(g, d_lptr, (uint64_t)n + 1));
         GA_TRY(download(lptr.data(), d_lptr, ((size_t)n + 1) * 8, st));
         GA_CUDA(cudaStreamSynchronize(st));
         const uint64_t E = lptr[n];
         GA_TRY(s_ent.alloc(&d_lent, E));
-        k_level_entries<true><<<grid, 256, 0, st>>>(inc, inc_ptr, d_core, n, d_lptr, d_lent);
+        k_level_entries<true><<<grid, 256, 0, st>>>(inc, inc_ptr, d_core, d_local, n, d_lptr, d_lent);
         GA_CUDA(cudaGetLastError());
         lent.resize(2 * E);
         GA_TRY(download(lent.data(), d_lent, E * 8, st));
-        GA_TRY(download(core.data(), d_core, (size_t)n * 4, st));
         if (passes > 1) {
             fptr.resize((size_t)n + 1);
             fent.resize(6 * T);
@@ -195,7 +205,7 @@ ga_status ga_greedy_pp(ga_graph* g, uint32_t passes, ga_dsg_result* res, uint32_
         }
         GA_CUDA(cudaStreamSynchronize(st));
     }
-    const dsg::Incidence first{lptr.data(), lent.data()}, full{fptr.data(), fent.data()};
+    const dsg::Incidence first{lptr.data(), lent.data(), true}, full{fptr.data(), fent.data(), false};
     GA_TRY(dsg::greedy_pp(n, T, core.data(), first, passes > 1 ? &full : nullptr, passes, &r));
     dsg::write_result(r, res, set, per_pass);
     return GA_OK;

@@ -21,10 +21,16 @@ inline uint64_t dens_ceil(Dens d) { return d.den ? (d.num + d.den - 1) / d.den :
 
 // Triangle incidence: for vertex v the other two corners of a triangle through v are ent[2i], ent[2i+1] for every
 // i in [ptr[v], ptr[v+1]).
+// With `level_local`, the lists hold exactly the triangles of each vertex's own core level, their corners given as
+// level-local ids (level_ranks) or UINT32_MAX for a corner of a higher core.
 struct Incidence {
     const uint64_t* ptr = nullptr;
     const uint32_t* ent = nullptr;
+    bool level_local = false;
 };
+
+// local[v] = the rank of v among the vertices of its core level, by id (the ids a level's removals run on).
+void level_ranks(uint32_t n, const uint32_t* core, uint32_t* local);
 
 struct Result {
     Dens best;

@@ -95,68 +95,186 @@ void group_by_core(uint32_t n, const uint32_t* core, std::vector<uint32_t>* memb
     }
 }
 
-// Charikar's removals inside one core level (see the file comment): pops the core-k vertices in (key, id) order,
-// key = triangles of the current residual graph through the vertex; writes the removal order to seq[b, e) and the
-// key at removal (= the triangles the removal destroys) to rkey[b, e).
-int run_level(const Level& L, const uint32_t* core, const Incidence& first, const std::vector<uint32_t>& member,
-              std::vector<uint64_t>& key, std::vector<uint8_t>& removed, std::vector<uint8_t>& mark,
-              std::vector<uint32_t>& seq, std::vector<uint64_t>& rkey) {
-    const uint32_t k = L.k;
-    // a triangle of v's list belongs to this level's graph when its other corners are in the k-core; a corner of a
-    // higher core stays alive for the whole level (only this level's vertices are read and written here)
-    auto in_level = [&](uint32_t a, uint32_t c) { return core[a] >= k && core[c] >= k; };
-    auto alive = [&](uint32_t x) { return core[x] != k || !removed[x]; };
-    std::vector<Entry> heap;
-    heap.reserve(L.e - L.b);
-    for (uint64_t i = L.b; i < L.e; i++) {
-        const uint32_t v = member[i];
-        uint64_t c = 0;
-        for (uint64_t j = first.ptr[v]; j < first.ptr[v + 1]; j++)
-            c += in_level(first.ent[2 * j], first.ent[2 * j + 1]);
-        if (c < k) return LEVEL_CORES;   // a vertex of the k-core lies in >= k of its triangles
-        key[v] = c;
-        heap.emplace_back(c, v);
+// The vertices of a level that may be removed next: those with key <= k, ordered by (key, level-local id).
+// KeyBuckets (k < 64): one bitset per key over the local ids with two levels of summary words, so the smallest
+// (key, id) is a mask lookup and three count-trailing-zeros away, and a move between keys is a few bit operations.
+class KeyBuckets {
+public:
+    KeyBuckets(uint32_t keys, uint32_t size)
+        : w0_(((uint64_t)size + 63) / 64), w1_((w0_ + 63) / 64), w2_((w1_ + 63) / 64),
+          l0_(keys * w0_, 0), l1_(keys * w1_, 0), l2_(keys * w2_, 0), count_(keys, 0) {}
+    bool empty() const { return nonempty_ == 0; }
+    void insert(uint32_t key, uint32_t i) {
+        l0_[key * w0_ + (i >> 6)] |= 1ull << (i & 63);
+        l1_[key * w1_ + (i >> 12)] |= 1ull << ((i >> 6) & 63);
+        l2_[key * w2_ + (i >> 18)] |= 1ull << ((i >> 12) & 63);
+        if (count_[key]++ == 0) nonempty_ |= 1ull << key;
     }
-    std::make_heap(heap.begin(), heap.end(), std::greater<Entry>());
-    std::vector<uint32_t> touched;
-    uint64_t pos = L.b, top_key = 0;
-    while (pos < L.e) {
-        if (heap.empty()) return LEVEL_BOOKKEEPING;
-        std::pop_heap(heap.begin(), heap.end(), std::greater<Entry>());
-        const Entry top = heap.back();
-        heap.pop_back();
+    void erase(uint32_t key, uint32_t i) {
+        uint64_t& a = l0_[key * w0_ + (i >> 6)];
+        a &= ~(1ull << (i & 63));
+        if (!a) {
+            uint64_t& b = l1_[key * w1_ + (i >> 12)];
+            b &= ~(1ull << ((i >> 6) & 63));
+            if (!b) l2_[key * w2_ + (i >> 18)] &= ~(1ull << ((i >> 12) & 63));
+        }
+        if (--count_[key] == 0) nonempty_ &= ~(1ull << key);
+    }
+    // Removes and returns the smallest (key, id); the queue must not be empty.
+    std::pair<uint32_t, uint32_t> pop() {
+        const uint32_t key = (uint32_t)__builtin_ctzll(nonempty_);
+        const uint64_t* c = &l2_[key * w2_];
+        uint64_t j = 0;
+        while (!c[j]) j++;
+        const uint64_t i2 = j * 64 + __builtin_ctzll(c[j]);
+        const uint64_t i1 = i2 * 64 + __builtin_ctzll(l1_[key * w1_ + i2]);
+        const uint32_t i = (uint32_t)(i1 * 64 + __builtin_ctzll(l0_[key * w0_ + i1]));
+        erase(key, i);
+        return {key, i};
+    }
+    void update(uint32_t old_key, uint32_t new_key, uint32_t i, uint32_t k) {
+        if (old_key <= k) erase(old_key, i);
+        if (new_key <= k) insert(new_key, i);
+    }
+
+private:
+    uint64_t w0_, w1_, w2_;
+    std::vector<uint64_t> l0_, l1_, l2_;
+    std::vector<uint32_t> count_;
+    uint64_t nonempty_ = 0;
+};
+
+// KeyHeap (any k): a lazy binary heap of key << 32 | id; an entry is stale once its vertex left (its key is then
+// kGone) or its key fell.
+class KeyHeap {
+public:
+    explicit KeyHeap(const std::vector<uint32_t>& key) : key_(key) {}
+    bool empty() {
+        drop_stale();
+        return heap_.empty();
+    }
+    void insert(uint32_t key, uint32_t i) {
+        heap_.push_back((uint64_t)key << 32 | i);
+        std::push_heap(heap_.begin(), heap_.end(), std::greater<uint64_t>());
+    }
+    std::pair<uint32_t, uint32_t> pop() {
+        drop_stale();
+        std::pop_heap(heap_.begin(), heap_.end(), std::greater<uint64_t>());
+        const uint64_t top = heap_.back();
+        heap_.pop_back();
+        return {(uint32_t)(top >> 32), (uint32_t)top};
+    }
+    void update(uint32_t, uint32_t new_key, uint32_t i, uint32_t k) {
+        if (new_key <= k) insert(new_key, i);
+    }
+
+private:
+    void drop_stale() {
+        while (!heap_.empty()) {
+            const uint64_t top = heap_.front();
+            const uint32_t i = (uint32_t)top;
+            if (key_[i] == top >> 32) return;
+            std::pop_heap(heap_.begin(), heap_.end(), std::greater<uint64_t>());
+            heap_.pop_back();
+        }
+    }
+    const std::vector<uint32_t>& key_;
+    std::vector<uint64_t> heap_;
+};
+
+constexpr uint32_t kOutside = UINT32_MAX;   // a corner of a higher core: alive for the whole level
+constexpr uint32_t kGone = UINT32_MAX;      // the key of a vertex already removed (one array answers both)
+
+// The removals of one level on its own triangle list (level-local ids; lptr / lent as built by run_level).
+template <class Queue>
+int simulate_level(const Level& L, const std::vector<uint32_t>& member, const std::vector<uint64_t>& lptr,
+                   const std::vector<uint32_t>& lent, std::vector<uint32_t>& key, Queue& q,
+                   std::vector<uint32_t>& seq, std::vector<uint64_t>& rkey) {
+    const uint32_t k = L.k;
+    const uint32_t size = (uint32_t)(L.e - L.b);
+    for (uint32_t i = 0; i < size; i++)
+        if (key[i] <= k) q.insert(key[i], i);
+    std::vector<uint8_t> mark(size, 0);
+    std::vector<std::pair<uint32_t, uint32_t>> touched;   // (local id, key before this removal)
+    auto alive = [&](uint32_t x) { return x == kOutside || key[x] != kGone; };
+    uint32_t top_key = 0;
+    for (uint32_t pos = 0; pos < size; pos++) {
+        if (q.empty()) return LEVEL_CORES;   // no vertex of key <= k left: the core numbers were not the graph's
+        const std::pair<uint32_t, uint32_t> top = q.pop();
         const uint32_t v = top.second;
-        if (removed[v] || key[v] != top.first) continue;   // stale entry
-        uint64_t found = 0;
+        uint32_t found = 0;
         touched.clear();
-        for (uint64_t j = first.ptr[v]; j < first.ptr[v + 1]; j++) {
-            const uint32_t a = first.ent[2 * j], c = first.ent[2 * j + 1];
-            if (!in_level(a, c) || !alive(a) || !alive(c)) continue;
+        for (uint64_t j = lptr[v]; j < lptr[v + 1]; j++) {
+            const uint32_t a = lent[2 * j], c = lent[2 * j + 1];
+            if (!alive(a) || !alive(c)) continue;
             found++;
             for (const uint32_t x : {a, c}) {
-                if (core[x] != k) continue;
+                if (x == kOutside) continue;
                 if (key[x] == 0) return LEVEL_BOOKKEEPING;
+                if (!mark[x]) { mark[x] = 1; touched.emplace_back(x, key[x]); }
                 key[x]--;
-                if (!mark[x]) { mark[x] = 1; touched.push_back(x); }
             }
         }
         if (found != key[v]) return LEVEL_BOOKKEEPING;
-        if (key[v] > k) return LEVEL_CORES;      // the running maximum of the keys is the core number
-        top_key = std::max(top_key, key[v]);
-        removed[v] = 1;
-        seq[pos] = v;
-        rkey[pos] = key[v];
-        pos++;
-        for (const uint32_t x : touched) {
-            mark[x] = 0;
-            heap.emplace_back(key[x], x);
-            std::push_heap(heap.begin(), heap.end(), std::greater<Entry>());
+        top_key = std::max(top_key, key[v]);   // <= k: only such keys are queued
+        seq[L.b + pos] = member[L.b + v];
+        rkey[L.b + pos] = key[v];
+        key[v] = kGone;
+        for (const auto& t : touched) {
+            mark[t.first] = 0;
+            q.update(t.second, key[t.first], t.first, k);
         }
     }
     return top_key == k ? LEVEL_OK : LEVEL_CORES;
 }
 
+// Charikar's removals inside one core level (see the file comment): the core-k vertices leave in (key, id) order,
+// key = triangles of the current residual graph through the vertex; writes the removal order to seq[b, e) and the
+// key at removal (= the triangles the removal destroys) to rkey[b, e). The level first copies its triangles into a
+// list of its own with level-local ids (ascending with the ids; a corner of a higher core becomes kOutside), so the
+// removals touch only arrays of the level's size. Only vertices with key <= k can be the minimum (a core-k vertex
+// with key <= k exists while any is left, and every vertex enters the level with key >= k), so only those are
+// queued: a vertex joins when its key falls to k or below.
+int run_level(const Level& L, const uint32_t* core, const Incidence& first, const std::vector<uint32_t>& member,
+              const std::vector<uint32_t>& local, std::vector<uint32_t>& seq, std::vector<uint64_t>& rkey) {
+    const uint32_t k = L.k;
+    const uint32_t size = (uint32_t)(L.e - L.b);
+    std::vector<uint64_t> lptr((size_t)size + 1, 0);
+    std::vector<uint32_t> lent, key(size);
+    for (uint32_t i = 0; i < size; i++) {
+        const uint32_t v = member[L.b + i];
+        if (first.level_local) {   // already the level's triangles in local ids (made on the device)
+            lent.insert(lent.end(), first.ent + 2 * first.ptr[v], first.ent + 2 * first.ptr[v + 1]);
+        } else {
+            for (uint64_t j = first.ptr[v]; j < first.ptr[v + 1]; j++) {
+                const uint32_t a = first.ent[2 * j], c = first.ent[2 * j + 1];
+                if (core[a] < k || core[c] < k) continue;   // a corner left in an earlier level
+                lent.push_back(core[a] == k ? local[a] : kOutside);
+                lent.push_back(core[c] == k ? local[c] : kOutside);
+            }
+        }
+        lptr[i + 1] = lent.size() / 2;
+        if (lptr[i + 1] - lptr[i] >= kGone) return LEVEL_BOOKKEEPING;
+        key[i] = (uint32_t)(lptr[i + 1] - lptr[i]);
+        if (key[i] < k) return LEVEL_CORES;   // a vertex of the k-core lies in >= k of its triangles
+    }
+    if (k < 64) {
+        KeyBuckets q(k + 1, size);
+        return simulate_level(L, member, lptr, lent, key, q, seq, rkey);
+    }
+    KeyHeap q(key);
+    return simulate_level(L, member, lptr, lent, key, q, seq, rkey);
+}
+
 }  // namespace
+
+void level_ranks(uint32_t n, const uint32_t* core, uint32_t* local) {
+    std::vector<uint32_t> member;
+    std::vector<Level> levels;
+    group_by_core(n, core, &member, &levels);
+    for (const Level& L : levels)
+        for (uint64_t i = L.b; i < L.e; i++) local[member[i]] = (uint32_t)(i - L.b);
+}
 
 // greedy_pp (dsg.h:189-249): the first pass per core level, later passes with loads on the whole graph.
 ga_status greedy_pp(uint32_t n, uint64_t T, const uint32_t* core, const Incidence& first, const Incidence* full,
@@ -168,9 +286,11 @@ ga_status greedy_pp(uint32_t n, uint64_t T, const uint32_t* core, const Incidenc
         std::vector<uint32_t> member;
         std::vector<Level> levels;
         group_by_core(n, core, &member, &levels);
-        std::vector<uint64_t> key(n, 0), rkey(n, 0);
-        std::vector<uint8_t> removed(n, 0), mark(n, 0);
-        std::vector<uint32_t> seq(n);
+        std::vector<uint64_t> rkey(n, 0);
+        std::vector<uint8_t> mark(n, 0);
+        std::vector<uint32_t> seq(n), local(n);
+        for (const Level& L : levels)
+            for (uint64_t i = L.b; i < L.e; i++) local[member[i]] = (uint32_t)(i - L.b);
         // largest levels first, so the long sequential ones start early
         std::vector<uint32_t> order(levels.size());
         for (uint32_t i = 0; i < order.size(); i++) order[i] = i;
@@ -181,7 +301,7 @@ ga_status greedy_pp(uint32_t n, uint64_t T, const uint32_t* core, const Incidenc
 #pragma omp parallel for schedule(dynamic, 1)
         for (int64_t i = 0; i < (int64_t)order.size(); i++) {
             if (err.load(std::memory_order_relaxed) != LEVEL_OK) continue;
-            const int s = run_level(levels[order[i]], core, first, member, key, removed, mark, seq, rkey);
+            const int s = run_level(levels[order[i]], core, first, member, local, seq, rkey);
             if (s != LEVEL_OK) err.store(s);
         }
         if (err.load() == LEVEL_CORES)

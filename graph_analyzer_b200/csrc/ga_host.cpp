@@ -271,19 +271,38 @@ ga_status ga_prune_to_core(const uint32_t* rowptr, const uint32_t* col, uint32_t
             core_out[kept] = core[v];
             kept++;
         }
-        std::vector<uint32_t> pairs;
-        for (uint32_t u = 0; u < n; u++) {
-            if (rowptr[u] > rowptr[u + 1]) return fail(GA_ERR_INVALID_GRAPH, "rowptr not monotone at %u", u);
+        // kept edges per row (in parallel), then their (new id, new id) pairs in CSR order
+        std::vector<uint64_t> start((size_t)n + 1, 0);
+        bool bad_row = false, bad_end = false;
+#pragma omp parallel for schedule(dynamic, 4096) reduction(|| : bad_row, bad_end)
+        for (int64_t u = 0; u < (int64_t)n; u++) {
+            if (rowptr[u] > rowptr[u + 1]) { bad_row = true; continue; }
+            uint64_t c = 0;
             for (uint32_t e = rowptr[u]; e < rowptr[u + 1]; e++) {
                 const uint32_t v = col[e];
-                if (v >= n) return fail(GA_ERR_INVALID_GRAPH, "endpoint %u >= n=%u", v, n);
-                if (new_id[u] != UINT32_MAX && new_id[v] != UINT32_MAX) {
-                    pairs.push_back(new_id[u]);
-                    pairs.push_back(new_id[v]);
-                }
+                if (v >= n) { bad_end = true; break; }
+                c += new_id[u] != UINT32_MAX && new_id[v] != UINT32_MAX;
+            }
+            start[u + 1] = c;
+        }
+        if (bad_row) return fail(GA_ERR_INVALID_GRAPH, "rowptr not monotone");
+        if (bad_end) return fail(GA_ERR_INVALID_GRAPH, "an endpoint is >= n=%u", n);
+        for (uint32_t u = 0; u < n; u++) start[u + 1] += start[u];
+        std::vector<uint32_t> pairs(2 * start[n]);
+#pragma omp parallel for schedule(dynamic, 4096)
+        for (int64_t u = 0; u < (int64_t)n; u++) {
+            if (new_id[u] == UINT32_MAX) continue;
+            uint64_t w = start[u];
+            for (uint32_t e = rowptr[u]; e < rowptr[u + 1]; e++) {
+                const uint32_t v = col[e];
+                if (new_id[v] == UINT32_MAX) continue;
+                pairs[2 * w] = new_id[u];
+                pairs[2 * w + 1] = new_id[v];
+                w++;
             }
         }
-        const uint32_t m2 = (uint32_t)(pairs.size() / 2);
+        if (start[n] > UINT32_MAX - 1) return fail(GA_ERR_INVALID_GRAPH, "more than 2^32-2 edges");
+        const uint32_t m2 = (uint32_t)start[n];
         ga_host_graph* g = new_host_graph(kept, m2);
         if (!g) return fail(GA_ERR_OUT_OF_MEMORY, "host allocation failed");
         ga_status s = build_csr(kept, pairs.data(), m2, g->rowptr, g->col, g->src, &g->max_out_degree);

@@ -182,3 +182,24 @@ def test_oracle_greedy_pinned(oracle, ga, name):
         r = oracle.greedy_pp(g, int(T))
         check(r, want)
         assert [list(p) for p in r.per_pass] == want["per_pass"]
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_host_greedy_high_levels_vs_oracle(ga, oracle, seed):
+    """Graphs whose core levels reach past 64 (the levels' queue switches from key buckets to a heap there), with
+    sparse low levels beside them; the host stage against the oracle's pinned greedy_pp."""
+    from conftest import random_pairs
+    rng = np.random.default_rng(seed)
+    n_dense, n_sparse = 30 + 5 * seed, 200
+    dense = random_pairs(rng, n_dense, 0.85)
+    sparse = random_pairs(rng, n_sparse, 0.03) + n_dense
+    bridge = np.stack([rng.integers(0, n_dense, 40), rng.integers(n_dense, n_dense + n_sparse, 40)], 1)
+    g = ga.graph_from_pairs(n_dense + n_sparse, np.concatenate([dense, sparse, bridge]).astype(np.uint32))
+    core, kmax, _ = oracle.core_levels(g)
+    assert kmax >= 64
+    tris = triangles_of(g)
+    ip, ie = incidence_of(g.n, tris)
+    for passes in (1, 2):
+        got, want = ga.greedy_pp_host(g.n, core, ip, ie, passes), oracle.greedy_pp(g, passes)
+        assert (got.tri, got.verts, got.set.tolist(), got.per_pass) == (want.tri, want.verts, want.set.tolist(),
+                                                                        want.per_pass)
