@@ -59,7 +59,6 @@ void write_result(const Result& r, ga_dsg_result* res, uint32_t* set, uint64_t* 
 
 namespace {
 
-typedef std::pair<uint64_t, uint32_t> Entry;   // (key, vertex): the heap order of greedy_pp, dsg.h:186-188
 
 struct Level {
     uint32_t k;
@@ -266,6 +265,106 @@ int run_level(const Level& L, const uint32_t* core, const Incidence& first, cons
     return simulate_level(L, member, lptr, lent, key, q, seq, rkey);
 }
 
+// A 4-ary min-heap of packed (key, id) values (fewer levels and cache lines per sift than a binary heap).
+template <class K>
+class QuadHeap {
+public:
+    void clear() { a_.clear(); }
+    bool empty() const { return a_.empty(); }
+    void build(std::vector<K>&& items) {
+        a_ = std::move(items);
+        for (size_t i = a_.size() / 4 + 1; i-- > 0;) sift_down(i);
+    }
+    void push(K x) {
+        size_t i = a_.size();
+        a_.push_back(x);
+        while (i > 0) {
+            const size_t p = (i - 1) / 4;
+            if (!(x < a_[p])) break;
+            a_[i] = a_[p];
+            i = p;
+        }
+        a_[i] = x;
+    }
+    K pop() {
+        const K top = a_[0];
+        a_[0] = a_.back();
+        a_.pop_back();
+        if (!a_.empty()) sift_down(0);
+        return top;
+    }
+
+private:
+    void sift_down(size_t i) {
+        const size_t n = a_.size();
+        const K x = a_[i];
+        for (;;) {
+            const size_t c0 = 4 * i + 1;
+            if (c0 >= n) break;
+            size_t m = c0;
+            const size_t ce = std::min(c0 + 4, n);
+            for (size_t c = c0 + 1; c < ce; c++)
+                if (a_[c] < a_[m]) m = c;
+            if (!(a_[m] < x)) break;
+            a_[i] = a_[m];
+            i = m;
+        }
+        a_[i] = x;
+    }
+    std::vector<K> a_;
+};
+
+// One Greedy++ pass after the first (dsg.h:199-244): remove the vertex with the smallest load + triangle degree
+// (ties: smaller id), load += its degree at removal; records the best residual into `best` (strictly denser wins).
+// K holds (load + degree) << 32 | id: uint64_t when every load + degree fits 32 bits, else a 128-bit value.
+// cur[v] = triangles through v in the residual graph, kGone once v is removed.
+template <class K>
+ga_status later_pass(uint32_t n, uint64_t T, const Incidence& full, const std::vector<uint32_t>& tri0,
+                     const std::vector<uint64_t>& load, std::vector<uint64_t>& next_load, std::vector<uint32_t>& cur,
+                     std::vector<uint8_t>& mark, std::vector<uint32_t>& pass_seq, Dens& best, bool* improved,
+                     uint64_t* pcut) {
+    auto packed = [&](uint32_t v) { return (K)(load[v] + cur[v]) << 32 | v; };
+    cur = tri0;
+    std::vector<K> items(n);
+    for (uint32_t v = 0; v < n; v++) items[v] = packed(v);
+    QuadHeap<K> heap;
+    heap.build(std::move(items));
+    std::vector<uint32_t> touched;
+    pass_seq.clear();
+    uint64_t t = T, alive = n;
+    *improved = false;
+    while (alive > 0) {
+        if (dens_gt(Dens{t, alive}, best)) { best = Dens{t, alive}; *improved = true; *pcut = pass_seq.size(); }
+        if (heap.empty()) return fail(GA_ERR_DEVICE_CHECK, "greedy_pp: heap ran empty");
+        const K top = heap.pop();
+        const uint32_t v = (uint32_t)top;
+        if (cur[v] == kGone || packed(v) != top) continue;   // stale entry
+        uint64_t found = 0;
+        touched.clear();
+        for (uint64_t j = full.ptr[v]; j < full.ptr[v + 1]; j++) {
+            const uint32_t a = full.ent[2 * j], c = full.ent[2 * j + 1];
+            if (cur[a] == kGone || cur[c] == kGone) continue;
+            found++;
+            if (cur[a] == 0 || cur[c] == 0) return fail(GA_ERR_DEVICE_CHECK, "greedy_pp: triangle bookkeeping inconsistent");
+            cur[a]--;
+            cur[c]--;
+            for (const uint32_t x : {a, c})
+                if (!mark[x]) { mark[x] = 1; touched.push_back(x); }
+        }
+        if (found != cur[v]) return fail(GA_ERR_DEVICE_CHECK, "greedy_pp: triangle bookkeeping inconsistent");
+        next_load[v] = load[v] + cur[v];
+        pass_seq.push_back(v);
+        t -= cur[v];
+        alive--;
+        cur[v] = kGone;
+        for (const uint32_t x : touched) {
+            mark[x] = 0;
+            heap.push(packed(x));
+        }
+    }
+    return GA_OK;
+}
+
 }  // namespace
 
 void level_ranks(uint32_t n, const uint32_t* core, uint32_t* local) {
@@ -282,6 +381,7 @@ ga_status greedy_pp(uint32_t n, uint64_t T, const uint32_t* core, const Incidenc
     *out = Result{};
     if (passes == 0) return fail(GA_ERR_INVALID_ARGUMENT, "passes must be >= 1");
     if (passes > 1 && !full) return fail(GA_ERR_INVALID_ARGUMENT, "Greedy++ needs the full triangle lists");
+    if (T >= kGone) return fail(GA_ERR_ARITH, "triangle count %llu >= 2^32 - 1", (unsigned long long)T);
     try {
         std::vector<uint32_t> member;
         std::vector<Level> levels;
@@ -335,55 +435,22 @@ ga_status greedy_pp(uint32_t n, uint64_t T, const uint32_t* core, const Incidenc
         out->per_pass.push_back(best);
         if (passes > 1) {
             // Greedy++ passes 2..: load[v] += triangles through v when it was removed (Alg 2 line 7)
-            std::vector<uint64_t> load(n), next_load(n), tri0(n), cur(n);
+            std::vector<uint64_t> load(n), next_load(n);
+            std::vector<uint32_t> tri0(n), cur(n), pass_seq;
             for (uint32_t i = 0; i < n; i++) load[seq[i]] = rkey[i];
-            for (uint32_t v = 0; v < n; v++) tri0[v] = full->ptr[v + 1] - full->ptr[v];
-            std::vector<uint8_t> live(n);
-            std::vector<uint32_t> pass_seq, touched;
+            for (uint32_t v = 0; v < n; v++) tri0[v] = (uint32_t)(full->ptr[v + 1] - full->ptr[v]);
             pass_seq.reserve(n);
-            std::vector<Entry> heap;
             for (uint32_t pass = 2; pass <= passes; pass++) {
-                cur = tri0;
-                std::fill(live.begin(), live.end(), 1);
-                uint64_t t = T, alive = n, pcut = 0;
+                uint64_t top = 0;
+                for (uint32_t v = 0; v < n; v++) top = std::max(top, load[v] + tri0[v]);
                 bool improved = false;
-                heap.clear();
-                for (uint32_t v = 0; v < n; v++) heap.emplace_back(load[v] + cur[v], v);
-                std::make_heap(heap.begin(), heap.end(), std::greater<Entry>());
-                pass_seq.clear();
-                while (alive > 0) {
-                    if (dens_gt(Dens{t, alive}, best)) { best = Dens{t, alive}; improved = true; pcut = pass_seq.size(); }
-                    if (heap.empty()) return fail(GA_ERR_DEVICE_CHECK, "greedy_pp: heap ran empty");
-                    std::pop_heap(heap.begin(), heap.end(), std::greater<Entry>());
-                    const Entry top = heap.back();
-                    heap.pop_back();
-                    const uint32_t v = top.second;
-                    if (!live[v] || load[v] + cur[v] != top.first) continue;
-                    uint64_t found = 0;
-                    touched.clear();
-                    for (uint64_t j = full->ptr[v]; j < full->ptr[v + 1]; j++) {
-                        const uint32_t a = full->ent[2 * j], c = full->ent[2 * j + 1];
-                        if (!live[a] || !live[c]) continue;
-                        found++;
-                        if (cur[a] == 0 || cur[c] == 0)
-                            return fail(GA_ERR_DEVICE_CHECK, "greedy_pp: triangle bookkeeping inconsistent");
-                        cur[a]--;
-                        cur[c]--;
-                        for (const uint32_t x : {a, c})
-                            if (!mark[x]) { mark[x] = 1; touched.push_back(x); }
-                    }
-                    if (found != cur[v]) return fail(GA_ERR_DEVICE_CHECK, "greedy_pp: triangle bookkeeping inconsistent");
-                    next_load[v] = load[v] + cur[v];
-                    live[v] = 0;
-                    pass_seq.push_back(v);
-                    t -= cur[v];
-                    alive--;
-                    for (const uint32_t x : touched) {
-                        mark[x] = 0;
-                        heap.emplace_back(load[x] + cur[x], x);
-                        std::push_heap(heap.begin(), heap.end(), std::greater<Entry>());
-                    }
-                }
+                uint64_t pcut = 0;
+                if (top < (1ull << 32))
+                    GA_TRY_HOST(later_pass<uint64_t>(n, T, *full, tri0, load, next_load, cur, mark, pass_seq, best,
+                                                     &improved, &pcut));
+                else
+                    GA_TRY_HOST(later_pass<u128>(n, T, *full, tri0, load, next_load, cur, mark, pass_seq, best,
+                                                 &improved, &pcut));
                 if (improved) { best_seq = pass_seq; best_cut = pcut; }
                 load.swap(next_load);
                 out->per_pass.push_back(best);
