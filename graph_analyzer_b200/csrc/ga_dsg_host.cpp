@@ -546,20 +546,35 @@ public:
             if (sink_slot[v] != UINT64_MAX) sink_arc_[v] = fwd[sink_slot[v]];
         level_.assign(N_, -1);
         it_.assign(N_, 0);
+        kept_alpha_ = -1;
         return GA_OK;
     }
 
     uint64_t triangles() const { return tris_.size() / 3; }
 
     // Vertices (local ids, ascending) on the minimal source side of a minimum cut for alpha = a / Q.
+    // The binary searches only ever ask for an alpha above the last one that had an answer, so that answer's
+    // maximum flow stays feasible (only the v -> t capacities grew) and the next flow starts from it: its residual
+    // capacities are kept, the v -> t arcs get 3 (a - a_kept) more, and augmenting goes on from there. The minimal
+    // source side does not depend on which maximum flow is found.
     void solve(int64_t a, std::vector<uint32_t>* S) {
-        cap_ = cap0_;
-        for (uint32_t v = 0; v < h_; v++)
-            if (sink_arc_[v] != UINT32_MAX) cap_[sink_arc_[v]] = 3 * a;
+        if (kept_alpha_ >= 0 && a >= kept_alpha_) {
+            cap_ = kept_;
+            for (uint32_t v = 0; v < h_; v++)
+                if (sink_arc_[v] != UINT32_MAX) cap_[sink_arc_[v]] += 3 * (a - kept_alpha_);
+        } else {
+            cap_ = cap0_;
+            for (uint32_t v = 0; v < h_; v++)
+                if (sink_arc_[v] != UINT32_MAX) cap_[sink_arc_[v]] = 3 * a;
+        }
         while (bfs()) blocking_flow();
         S->clear();
         for (uint32_t v = 0; v < h_; v++)
             if (deg_[v] && level_[2 + v] >= 0) S->push_back(v);   // level_ = reachability after the last BFS
+        if (!S->empty()) {
+            kept_ = cap_;
+            kept_alpha_ = a;
+        }
     }
 
     // Triangles of the network's graph with all three corners in S.
@@ -631,7 +646,8 @@ private:
     std::vector<uint32_t> tris_;
     std::vector<uint64_t> deg_;
     std::vector<uint32_t> start_, to_, rev_, sink_arc_, it_, queue_, path_;
-    std::vector<int64_t> cap0_, cap_;
+    std::vector<int64_t> cap0_, cap_, kept_;   // capacities at alpha 0, current residuals, kept residuals
+    int64_t kept_alpha_ = -1;                  // alpha of the kept residuals (-1: none)
     std::vector<int32_t> level_;
     std::vector<uint8_t> in_;
 };
