@@ -3,7 +3,8 @@ kind the reference's own mutation list targets (scripts/mutation_check.py: kerne
 flip, ...), compiled on the side. The golden vectors of the reference's fixtures must expose every mutant, and the
 unmutated copy must match them: this is what makes the oracle a pinned checker rather than a second opinion. The
 golden vectors are the four generated fixtures plus ties.json (graphs whose peeling meets one density twice, outputs
-from the reference's own code)."""
+from the reference's own code). The greedy_pp restatement has its own mutants, exposed by dsg.json (the reference's
+greedy / greedy_pp outputs on 49 graphs)."""
 from __future__ import annotations
 
 import os
@@ -26,6 +27,39 @@ MUTANTS = {
     "dedup_dropped": ("if (i > 0 && key[i] == key[i - 1]) continue;", ""),
     "intersect_skips": ("else { c++; i++; j++; }", "else { c++; i += 2; j++; }"),
 }
+
+# Mutants of the oracle's greedy_pp restatement (dsg.h:189-249), checked against the densest-subgraph golden vectors
+# (tests/golden/dsg.json, the reference's own greedy / greedy_pp outputs).
+DSG_MUTANTS = {
+    "greedy_improve_not_strict": ("if (dens_gt_u(t, nalive, bn, bd)) { bn = t;",
+                                  "if (!dens_gt_u(bn, bd, t, nalive)) { bn = t;"),
+    "greedy_load_not_accumulated": ("next_load[v] = load[v] + cur[v];", "next_load[v] = cur[v];"),
+    "greedy_cut_off_by_one": ("improved = 1; cut = norder; }", "improved = 1; cut = norder + (norder < n - 1); }"),
+    "greedy_best_order_kept": ("if (improved) { memcpy(best_order", "if (!improved) { memcpy(best_order"),
+}
+
+DSG_CHECK = r"""
+import json, sys
+import numpy as np
+sys.path.insert(0, {root!r})
+from oracle import Oracle
+from conftest import GOLDEN, FIXTURES, fixture_path
+o = Oracle({lib!r})
+diff = []
+for rec in json.load(open(GOLDEN + "/dsg.json"))["graphs"]:
+    if rec["name"] == "hk8298":
+        continue
+    if rec["name"] in FIXTURES:
+        g = o.load_graph(fixture_path(rec["name"]))
+    else:
+        g = o.build_graph_from_edges(rec["n"], np.array(rec["pairs"], np.uint32).reshape(-1, 2))
+    for T, want in [("1", rec["greedy"])] + list(rec["greedy_pp"].items()):
+        r = o.greedy_pp(g, int(T))
+        if (r.tri, r.verts, r.set.tolist()) != (want["tri"], want["verts"], want["set"]):
+            diff.append((rec["name"], T))
+print(diff)
+sys.exit(3 if diff else 0)
+"""
 
 # Compares one compiled oracle with the golden vectors; exit 0 = all equal, 3 = a difference was found.
 CHECK = r"""
@@ -78,10 +112,10 @@ def _compile(tmp_path, name, text):
     return str(lib)
 
 
-def _check(lib, timeout=15):
+def _check(lib, timeout=15, script=CHECK):
     """Exit status of the golden comparison; a mutant that never finishes (a loop that stops making progress) is
     stopped after `timeout` seconds and counts as exposed (status -1)."""
-    code = CHECK.format(root=ROOT, lib=lib)
+    code = script.format(root=ROOT, lib=lib)
     env = dict(os.environ, PYTHONPATH=os.path.join(ROOT, "tests"))
     try:
         return subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=timeout, env=env)
@@ -90,7 +124,10 @@ def _check(lib, timeout=15):
 
 
 def test_unmutated_copy_matches_golden(tmp_path):
-    r = _check(_compile(tmp_path, "clean", open(ORACLE_C).read()), timeout=300)
+    lib = _compile(tmp_path, "clean", open(ORACLE_C).read())
+    r = _check(lib, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    r = _check(lib, timeout=300, script=DSG_CHECK)
     assert r.returncode == 0, r.stdout + r.stderr
 
 
@@ -101,4 +138,13 @@ def test_golden_vectors_kill_mutant(tmp_path, mutant):
     assert text.count(old) == 1, f"mutation site of {mutant} not found exactly once"
     r = _check(_compile(tmp_path, mutant, text.replace(old, new)))
     # killed: a golden mismatch (exit 3) or the mutant failing outright (crash, exception)
+    assert r.returncode != 0, f"mutant {mutant} survived the golden vectors"
+
+
+@pytest.mark.parametrize("mutant", list(DSG_MUTANTS))
+def test_dsg_golden_vectors_kill_mutant(tmp_path, mutant):
+    old, new = DSG_MUTANTS[mutant]
+    text = open(ORACLE_C).read()
+    assert text.count(old) == 1, f"mutation site of {mutant} not found exactly once"
+    r = _check(_compile(tmp_path, mutant, text.replace(old, new)), script=DSG_CHECK)
     assert r.returncode != 0, f"mutant {mutant} survived the golden vectors"
