@@ -119,17 +119,20 @@ public:
         }
         if (--count_[key] == 0) nonempty_ &= ~(1ull << key);
     }
-    // Removes and returns the smallest (key, id); the queue must not be empty.
-    std::pair<uint32_t, uint32_t> pop() {
+    // The smallest (key, id); the queue must not be empty.
+    std::pair<uint32_t, uint32_t> peek() const {
         const uint32_t key = (uint32_t)__builtin_ctzll(nonempty_);
         const uint64_t* c = &l2_[key * w2_];
         uint64_t j = 0;
         while (!c[j]) j++;
         const uint64_t i2 = j * 64 + __builtin_ctzll(c[j]);
         const uint64_t i1 = i2 * 64 + __builtin_ctzll(l1_[key * w1_ + i2]);
-        const uint32_t i = (uint32_t)(i1 * 64 + __builtin_ctzll(l0_[key * w0_ + i1]));
-        erase(key, i);
-        return {key, i};
+        return {key, (uint32_t)(i1 * 64 + __builtin_ctzll(l0_[key * w0_ + i1]))};
+    }
+    std::pair<uint32_t, uint32_t> pop() {
+        const std::pair<uint32_t, uint32_t> top = peek();
+        erase(top.first, top.second);
+        return top;
     }
     void update(uint32_t old_key, uint32_t new_key, uint32_t i, uint32_t k) {
         if (old_key <= k) erase(old_key, i);
@@ -273,7 +276,8 @@ public:
     bool empty() const { return a_.empty(); }
     void build(std::vector<K>&& items) {
         a_ = std::move(items);
-        for (size_t i = a_.size() / 4 + 1; i-- > 0;) sift_down(i);
+        if (a_.size() > 1)
+            for (size_t i = (a_.size() - 2) / 4 + 1; i-- > 0;) sift_down(i);   // every node with a child
     }
     void push(K x) {
         size_t i = a_.size();
@@ -286,6 +290,7 @@ public:
         }
         a_[i] = x;
     }
+    K top() const { return a_[0]; }
     K pop() {
         const K top = a_[0];
         a_[0] = a_.back();
@@ -316,29 +321,45 @@ private:
 
 // One Greedy++ pass after the first (dsg.h:199-244): remove the vertex with the smallest load + triangle degree
 // (ties: smaller id), load += its degree at removal; records the best residual into `best` (strictly denser wins).
-// K holds (load + degree) << 32 | id: uint64_t when every load + degree fits 32 bits, else a 128-bit value.
-// cur[v] = triangles through v in the residual graph, kGone once v is removed.
+// Keys below 64 (most vertices of sparse graphs) sit in `low`, one bitset per key over the ids; larger keys in a lazy
+// 4-ary heap of (load + degree) << 32 | id values (K = uint64_t when every load + degree fits 32 bits, else 128-bit).
+// Keys only fall during a pass, so a vertex moves from the heap into `low`, never back; the next vertex is the smaller
+// of the two fronts. cur[v] = triangles through v in the residual graph, kGone once v is removed. `low` is empty on
+// entry and on a successful return.
 template <class K>
 ga_status later_pass(uint32_t n, uint64_t T, const Incidence& full, const std::vector<uint32_t>& tri0,
                      const std::vector<uint64_t>& load, std::vector<uint64_t>& next_load, std::vector<uint32_t>& cur,
-                     std::vector<uint8_t>& mark, std::vector<uint32_t>& pass_seq, Dens& best, bool* improved,
-                     uint64_t* pcut) {
+                     std::vector<uint8_t>& mark, KeyBuckets& low, std::vector<uint32_t>& pass_seq, Dens& best,
+                     bool* improved, uint64_t* pcut) {
+    constexpr uint64_t kLow = 64;
     auto packed = [&](uint32_t v) { return (K)(load[v] + cur[v]) << 32 | v; };
     cur = tri0;
-    std::vector<K> items(n);
-    for (uint32_t v = 0; v < n; v++) items[v] = packed(v);
+    std::vector<K> items;
+    for (uint32_t v = 0; v < n; v++) {
+        const uint64_t key = load[v] + cur[v];
+        if (key < kLow) low.insert((uint32_t)key, v);
+        else items.push_back(packed(v));
+    }
     QuadHeap<K> heap;
     heap.build(std::move(items));
-    std::vector<uint32_t> touched;
+    std::vector<std::pair<uint32_t, uint64_t>> touched;   // (vertex, key before this removal)
     pass_seq.clear();
     uint64_t t = T, alive = n;
     *improved = false;
     while (alive > 0) {
         if (dens_gt(Dens{t, alive}, best)) { best = Dens{t, alive}; *improved = true; *pcut = pass_seq.size(); }
-        if (heap.empty()) return fail(GA_ERR_DEVICE_CHECK, "greedy_pp: heap ran empty");
-        const K top = heap.pop();
-        const uint32_t v = (uint32_t)top;
-        if (cur[v] == kGone || packed(v) != top) continue;   // stale entry
+        while (!heap.empty()) {   // drop stale heap entries (vertex gone, or its key fell)
+            const K top = heap.top();
+            const uint32_t v = (uint32_t)top;
+            if (cur[v] != kGone && packed(v) == top) break;
+            heap.pop();
+        }
+        uint32_t v;
+        if (low.empty() && heap.empty()) return fail(GA_ERR_DEVICE_CHECK, "greedy_pp: queue ran empty");
+        if (!low.empty() && (heap.empty() || ((K)low.peek().first << 32 | low.peek().second) < heap.top()))
+            v = low.pop().second;
+        else
+            v = (uint32_t)heap.pop();
         uint64_t found = 0;
         touched.clear();
         for (uint64_t j = full.ptr[v]; j < full.ptr[v + 1]; j++) {
@@ -346,10 +367,10 @@ ga_status later_pass(uint32_t n, uint64_t T, const Incidence& full, const std::v
             if (cur[a] == kGone || cur[c] == kGone) continue;
             found++;
             if (cur[a] == 0 || cur[c] == 0) return fail(GA_ERR_DEVICE_CHECK, "greedy_pp: triangle bookkeeping inconsistent");
+            for (const uint32_t x : {a, c})
+                if (!mark[x]) { mark[x] = 1; touched.emplace_back(x, load[x] + cur[x]); }
             cur[a]--;
             cur[c]--;
-            for (const uint32_t x : {a, c})
-                if (!mark[x]) { mark[x] = 1; touched.push_back(x); }
         }
         if (found != cur[v]) return fail(GA_ERR_DEVICE_CHECK, "greedy_pp: triangle bookkeeping inconsistent");
         next_load[v] = load[v] + cur[v];
@@ -357,9 +378,12 @@ ga_status later_pass(uint32_t n, uint64_t T, const Incidence& full, const std::v
         t -= cur[v];
         alive--;
         cur[v] = kGone;
-        for (const uint32_t x : touched) {
-            mark[x] = 0;
-            heap.push(packed(x));
+        for (const auto& x : touched) {
+            mark[x.first] = 0;
+            const uint64_t key = load[x.first] + cur[x.first];
+            if (x.second < kLow) low.erase((uint32_t)x.second, x.first);
+            if (key < kLow) low.insert((uint32_t)key, x.first);
+            else heap.push(packed(x.first));
         }
     }
     return GA_OK;
@@ -440,16 +464,17 @@ ga_status greedy_pp(uint32_t n, uint64_t T, const uint32_t* core, const Incidenc
             for (uint32_t i = 0; i < n; i++) load[seq[i]] = rkey[i];
             for (uint32_t v = 0; v < n; v++) tri0[v] = (uint32_t)(full->ptr[v + 1] - full->ptr[v]);
             pass_seq.reserve(n);
+            KeyBuckets low(64, n);
             for (uint32_t pass = 2; pass <= passes; pass++) {
                 uint64_t top = 0;
                 for (uint32_t v = 0; v < n; v++) top = std::max(top, load[v] + tri0[v]);
                 bool improved = false;
                 uint64_t pcut = 0;
                 if (top < (1ull << 32))
-                    GA_TRY_HOST(later_pass<uint64_t>(n, T, *full, tri0, load, next_load, cur, mark, pass_seq, best,
-                                                     &improved, &pcut));
+                    GA_TRY_HOST(later_pass<uint64_t>(n, T, *full, tri0, load, next_load, cur, mark, low, pass_seq,
+                                                     best, &improved, &pcut));
                 else
-                    GA_TRY_HOST(later_pass<u128>(n, T, *full, tri0, load, next_load, cur, mark, pass_seq, best,
+                    GA_TRY_HOST(later_pass<u128>(n, T, *full, tri0, load, next_load, cur, mark, low, pass_seq, best,
                                                  &improved, &pcut));
                 if (improved) { best_seq = pass_seq; best_cut = pcut; }
                 load.swap(next_load);
