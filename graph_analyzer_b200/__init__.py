@@ -595,6 +595,8 @@ class DeviceGraph:
                    seed: DsgResult | None = None) -> DsgResult:
         """CoreExact (dsg.h:463-627); core numbers from the device when `core` is None."""
         r, setbuf = _DsgRes(), np.zeros(max(self.n, 1), np.uint32)
+        if core is not None and len(core) != self.n:
+            raise ValueError("core must have n entries")
         c = np.ascontiguousarray(core, np.uint32) if core is not None and self.n else None
         sp, keep = _seed(seed)
         _check(lib().ga_core_exact(self._h, _ptr(c), int(use_pruning12), sp, C.byref(r), _ptr(setbuf)))

@@ -101,3 +101,30 @@ def test_gpu_greedy_larger_vs_oracle(ga, oracle, cuda_ok, case):
             assert (got.tri, got.verts) == (want.tri, want.verts)
             assert np.array_equal(got.set, want.set)
             assert got.per_pass == want.per_pass
+
+
+def test_gpu_dsg_refusals(ga, cuda_ok):
+    """Refusals through the device entry points: no passes, a seed that is not a subgraph with the claimed count, core
+    numbers of the wrong length; the graph stays usable after each."""
+    rec = BY_NAME["t_pl400"]
+    g = dsg_graph(ga, rec)
+    w = rec["greedy_pp"]["10"]
+    with ga.DeviceGraph(g) as d:
+        with pytest.raises(ga.GAError) as e:
+            d.greedy_pp(0)
+        assert e.value.name == "GA_ERR_INVALID_ARGUMENT"
+        bad = ga.DsgResult(w["tri"] + 1, w["verts"], np.array(w["set"], np.uint32))
+        with pytest.raises(ga.GAError) as e:
+            d.core_exact(seed=bad)
+        assert e.value.name == "GA_ERR_INVALID_ARGUMENT"
+        with pytest.raises(ValueError):
+            d.core_exact(np.zeros(g.n - 1, np.uint32))
+        check(d.greedy_pp(10), w)
+        check(d.core_exact(), rec["core_exact"], flows=True)
+    # an empty graph and a graph without triangles
+    with ga.DeviceGraph(ga.build_graph_from_edges(0, np.zeros((0, 2), np.uint32))) as d:
+        assert (d.greedy_pp(3).verts, d.core_exact().verts, d.exact_densest().verts) == (0, 0, 0)
+    with ga.DeviceGraph(ga.build_graph_from_edges(4, np.array([[0, 1], [1, 2], [2, 3]], np.uint32))) as d:
+        r = d.greedy_pp(2)
+        assert (r.tri, r.verts, r.per_pass) == (0, 0, [(0, 0), (0, 0)])
+        assert (d.core_exact().tri, d.exact_densest().tri) == (0, 0)
