@@ -15,7 +15,6 @@ from conftest import FIXTURES, GOLDEN, fixture_path
 with open(os.path.join(GOLDEN, "dsg.json")) as _f:
     DSG = json.load(_f)["graphs"]
 BY_NAME = {g["name"]: g for g in DSG}
-SMALL = [g["name"] for g in DSG if g["name"] != "hk8298"]
 
 
 def dsg_graph(ga, rec):
