@@ -683,9 +683,9 @@ def _csv_rows(text):
 def run_reference_gpu(args):
     """The reference's own GPU drivers (baseline/_ref/bin, built from its sources for sm_100a by
     baseline/build_reference_gpu.py) against this library's drivers, on the same text files and the same GPU:
-    gpu_tc vs ga_tc on R-MAT 22 (kernels v1-v9), gpu_densest vs ga_densest (eps 1/10) on the Holme-Kim n 1.70M graph,
-    gpu_dsg vs ga_dsg (core decomposition) on the Holme-Kim n 8,298 graph, and gpu_dsg vs ga_dsg's whole densest-
-    subgraph pipeline on the Holme-Kim n 8,298 and n 1.70M graphs. Every program verifies its own results (the
+    gpu_tc vs ga_tc on R-MAT 22 (kernels v1-v9), gpu_densest vs ga_densest (eps 1/10, with the greedy peel rows) on
+    the Holme-Kim n 1.70M graph, gpu_dsg vs ga_dsg (core decomposition) on the Holme-Kim n 8,298 graph, and gpu_dsg
+    vs ga_dsg's whole densest-subgraph pipeline on the Holme-Kim n 8,298 and n 1.70M graphs. Every program verifies its own results (the
     reference's against its CPU code); the triangle counts, peel results, core rows and pipeline subgraphs must
     agree."""
     import tempfile
@@ -701,7 +701,7 @@ def run_reference_gpu(args):
     runs = [
         ("tc_rmat22", lambda: make_graph(ga), ["gpu_tc", "ga_tc"], lambda p: [p, str(max(3, args.steps // 2))]),
         ("peel_hk1.7M", lambda: ga.graph_from_pairs(1_700_000, ga.gen_holme_kim(1_700_000, 6, 7, 0.54, 0.3, seed=SEED)),
-         ["gpu_densest", "ga_densest"], lambda p: [p, "1", "10", "--repeats", "3", "--no-greedy"]),
+         ["gpu_densest", "ga_densest"], lambda p: [p, "1", "10", "--repeats", "3"]),
         ("cores_hk8298", lambda: ga.graph_from_pairs(8298, ga.gen_holme_kim(8298, 12, 12, 0.0, 0.5, seed=SEED)),
          ["gpu_dsg", "ga_dsg"], lambda p: [p, "--repeats", "3", "--no-exact", "--no-greedy", "--no-greedypp"]),
         # the whole densest-subgraph pipeline: cores, greedy lower bound, prune, Greedy++ (10 passes), seeded CoreExact
@@ -739,6 +739,15 @@ def run_reference_gpu(args):
                           "speedup": float(ref_best[5]) / float(our_best[5]),
                           "same_triangles": len({r[4] for r in tc["reference"] + tc["ours"]}) == 1}
         ok &= out["tc_best"]["same_triangles"]
+    # the greedy peel beside the batch peel (the quality baseline of gpu_densest): same best density, both times
+    pk = out.get("peel_hk1.7M", {})
+    if pk.get("reference") and pk.get("ours"):
+        a = {r[0]: r for r in pk["reference"]}.get("cpu_greedy_peel")
+        b = {r[0]: r for r in pk["ours"]}.get("greedy_peel")
+        if a and b:
+            out["greedy_peel_hk1.7M"] = {"reference_ms": float(a[8]), "ours_ms": float(b[8]),
+                                         "same_result": a[2:6] == b[2:6]}
+            ok &= out["greedy_peel_hk1.7M"]["same_result"]
     # densest-subgraph pipeline: stage times side by side (the reference's CPU stages vs this library's) and the
     # results, which must be the same subgraphs
     stages = [("gpu_core_decomp", "gpu_core_decomp"), ("cpu_greedy", "greedy"), ("prune_kcore", "prune_kcore"),

@@ -202,3 +202,22 @@ def test_host_greedy_high_levels_vs_oracle(ga, oracle, seed):
         got, want = ga.greedy_pp_host(g.n, core, ip, ie, passes), oracle.greedy_pp(g, passes)
         assert (got.tri, got.verts, got.set.tolist(), got.per_pass) == (want.tri, want.verts, want.set.tolist(),
                                                                         want.per_pass)
+
+
+def test_prune_to_core_refusals(ga):
+    g = ga.build_graph_from_edges(4, np.array([[0, 1], [1, 2], [0, 2], [2, 3]], np.uint32))
+    core = np.array([1, 1, 1, 0], np.uint32)
+    gp, old, cp = ga.prune_to_core(g, core, 1)
+    assert (gp.n, gp.m, old.tolist(), cp.tolist()) == (3, 3, [0, 1, 2], [1, 1, 1])
+    gp, old, _ = ga.prune_to_core(g, core, 2)                     # nothing kept
+    assert (gp.n, gp.m, old.size) == (0, 0, 0)
+    bad = ga.Graph(g.n, g.m, g.rowptr.copy(), g.col.copy(), g.src, g.max_out_degree)
+    bad.col[0] = 9                                                # endpoint >= n
+    with pytest.raises(ga.GAError) as e:
+        ga.prune_to_core(bad, core, 1)
+    assert e.value.name == "GA_ERR_INVALID_GRAPH"
+    bad = ga.Graph(g.n, g.m, g.rowptr.copy(), g.col.copy(), g.src, g.max_out_degree)
+    bad.rowptr[-1] = g.m - 1                                      # rowptr does not span the edges
+    with pytest.raises(ga.GAError) as e:
+        ga.prune_to_core(bad, core, 1)
+    assert e.value.name == "GA_ERR_INVALID_GRAPH"
