@@ -185,7 +185,8 @@ ga_status scan_u64(ga_graph* g, unsigned long long* data, uint64_t n);
 // Frees the loop state and its device buffers (the next loop call rebuilds them).
 void reset_loops(ga_graph* g);
 
-// The core numbers of g (device, n entries, valid until the next loop call) from one run of the core loop.
+// The core numbers of g (device, n entries, valid until the next loop call): those of the last core loop when no
+// other loop has run since, else from a new run of the core loop.
 ga_status core_numbers(ga_graph* g, const uint32_t** d_core, uint32_t* kmax);
 // The triangle incidence lists of g (device): for every vertex v the other two corners of each triangle through v
 // in inc[inc_ptr[v] .. inc_ptr[v+1]), (middle, highest) in the list of a triangle's lowest corner. Built when

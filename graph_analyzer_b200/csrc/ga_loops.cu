@@ -102,6 +102,8 @@ struct ga_loops {
     // triangle incidence lists (built once per graph when memory allows): for every vertex v the other two corners
     // of each triangle through v, in inc[inc_ptr[v] .. inc_ptr[v+1])
     int lists = -1;                    // -1 undecided, 0 enumeration update, 1 incidence-list update
+    bool cores_in_out = false;         // out[] holds the core numbers of a finished core loop (kmax in cores_kmax)
+    uint32_t cores_kmax = 0;
     uint2* inc = nullptr;
     unsigned long long* inc_ptr = nullptr;   // n+1
     ga::Segs segs;                     // per-graph state of a batch (count 0 for a single graph)
@@ -803,6 +805,7 @@ static ga_status run_loop(ga_graph* g, uint64_t num, uint64_t den, LoopScalars* 
     GA_TRY(ensure_loops(g));
     ga_loops* L = g->loops;
     cudaStream_t st = g->stream;
+    L->cores_in_out = false;   // out[] is rewritten below
     const uint32_t n = g->n;
     // tri[] = triangles per vertex on the whole graph (uint32 counters; T < 2^32 is checked below): the list lengths
     // when the incidence lists exist, else one per-vertex triangle pass
@@ -872,10 +875,14 @@ static ga_status run_loop(ga_graph* g, uint64_t num, uint64_t den, LoopScalars* 
 }
 
 ga_status core_numbers(ga_graph* g, const uint32_t** d_core, uint32_t* kmax) {
-    LoopScalars s;
-    GA_TRY(run_loop<LOOP_CORE>(g, 0, 1, &s));
+    if (!g->loops || !g->loops->cores_in_out) {
+        LoopScalars s;
+        GA_TRY(run_loop<LOOP_CORE>(g, 0, 1, &s));
+        g->loops->cores_in_out = true;
+        g->loops->cores_kmax = s.kcur;
+    }
     *d_core = g->loops->out;
-    *kmax = s.kcur;
+    *kmax = g->loops->cores_kmax;
     return GA_OK;
 }
 
@@ -1007,6 +1014,8 @@ ga_status ga_core_decomposition(ga_graph* g, uint32_t* core, ga_core_result* res
     GA_TRY(use_device(g));
     LoopScalars s;
     GA_TRY(run_loop<LOOP_CORE>(g, 0, 1, &s));
+    g->loops->cores_in_out = true;   // the densest-subgraph stages start from these core numbers
+    g->loops->cores_kmax = s.kcur;
     res->kmax = s.kcur;
     res->rounds = s.round;
     if (core && g->n) {

@@ -128,3 +128,20 @@ def test_gpu_dsg_refusals(ga, cuda_ok):
         r = d.greedy_pp(2)
         assert (r.tri, r.verts, r.per_pass) == (0, 0, [(0, 0), (0, 0)])
         assert (d.core_exact().tri, d.exact_densest().tri) == (0, 0)
+
+
+def test_gpu_core_numbers_reused_only_while_valid(ga, oracle, cuda_ok):
+    """The densest stages start from the last core loop's numbers when nothing ran since, and recompute them after a
+    peeling loop (which rewrites the same device array)."""
+    rec = BY_NAME["t_er800"]
+    g = dsg_graph(ga, rec)
+    core, _, _ = oracle.core_levels(g)
+    with ga.DeviceGraph(g) as d:
+        assert np.array_equal(d.core_decomposition().core, core)
+        check(d.greedy_pp(1), rec["greedy"])                        # reuses the loop's numbers
+        d.batch_peel(1, 10)                                         # out[] now holds removed_round
+        check(d.greedy_pp(3), rec["greedy_pp"]["3"])
+        check(d.core_exact(), rec["core_exact"], flows=True)
+        d.batch_peel(1, 2)
+        check(d.core_exact(), rec["core_exact"], flows=True)
+        assert np.array_equal(d.core_decomposition().core, core)
