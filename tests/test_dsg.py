@@ -221,3 +221,25 @@ def test_prune_to_core_refusals(ga):
     with pytest.raises(ga.GAError) as e:
         ga.prune_to_core(bad, core, 1)
     assert e.value.name == "GA_ERR_INVALID_GRAPH"
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_host_exact_is_the_brute_force_optimum(ga, oracle, seed):
+    """Independent of any implementation: on tiny graphs Exact and CoreExact (with and without Pruning1/2, seeded
+    with Greedy++) reach the optimum density over all vertex subsets, Greedy++ stays at or below it and Greedy reaches
+    at least a third of it (densest.h:11-14's guarantee for the triangle peel)."""
+    from test_tiny_bruteforce import _brute_force, _tiny_graphs
+    for n, pairs in _tiny_graphs(25, 300 + seed):
+        g = ga.build_graph_from_edges(n, ga.canonical_edges(pairs))
+        (bn, bd), _ = _brute_force(n, pairs)
+        tris = triangles_of(g)
+        ip, ie = incidence_of(g.n, tris)
+        core, _, _ = oracle.core_levels(g)
+        gpp = ga.greedy_pp_host(g.n, core, ip, ie, 5)
+        gr = ga.greedy_pp_host(g.n, core, ip, ie, 1)
+        for r in (ga.exact_densest_host(g.n, tris), ga.core_exact_host(g, tris, core),
+                  ga.core_exact_host(g, tris, core, use_pruning12=False), ga.core_exact_host(g, tris, core, seed=gpp)):
+            assert r.tri * (bd or 1) == bn * (r.verts or 1) and (r.verts == 0) == (bn == 0)
+            assert len(r.set) == r.verts
+        assert gpp.tri * (bd or 1) <= bn * (gpp.verts or 1)
+        assert 3 * gr.tri * (bd or 1) >= bn * (gr.verts or 1)

@@ -145,3 +145,19 @@ def test_gpu_core_numbers_reused_only_while_valid(ga, oracle, cuda_ok):
         d.batch_peel(1, 2)
         check(d.core_exact(), rec["core_exact"], flows=True)
         assert np.array_equal(d.core_decomposition().core, core)
+
+
+@pytest.mark.parametrize("seed", range(2))
+def test_gpu_exact_is_the_brute_force_optimum(ga, cuda_ok, seed):
+    """On tiny graphs the device entry points reach the optimum over all vertex subsets (Exact, CoreExact), Greedy++
+    stays at or below it and Greedy reaches at least a third of it."""
+    from test_tiny_bruteforce import _brute_force, _tiny_graphs
+    for n, pairs in _tiny_graphs(20, 400 + seed):
+        g = ga.build_graph_from_edges(n, ga.canonical_edges(pairs))
+        (bn, bd), _ = _brute_force(n, pairs)
+        with ga.DeviceGraph(g) as d:
+            gpp, gr = d.greedy_pp(5), d.greedy_pp(1)
+            for r in (d.exact_densest(), d.core_exact(), d.core_exact(use_pruning12=False), d.core_exact(seed=gpp)):
+                assert r.tri * (bd or 1) == bn * (r.verts or 1) and (r.verts == 0) == (bn == 0)
+        assert gpp.tri * (bd or 1) <= bn * (gpp.verts or 1)
+        assert 3 * gr.tri * (bd or 1) >= bn * (gr.verts or 1)
