@@ -243,3 +243,25 @@ def test_host_exact_is_the_brute_force_optimum(ga, oracle, seed):
             assert len(r.set) == r.verts
         assert gpp.tri * (bd or 1) <= bn * (gpp.verts or 1)
         assert 3 * gr.tri * (bd or 1) >= bn * (gr.verts or 1)
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_host_mid_graphs_against_reference(ga, oracle, reference, seed):
+    """The reference's --mid check (Exact as the oracle of CoreExact) on seeded mid-size graphs, with the reference's
+    own functions run beside (skipped where the reference is not built): same sets, same flow-call counts."""
+    from conftest import random_pairs
+    rng = np.random.default_rng(500 + seed)
+    for n, p in ((40, 0.35), (80, 0.2), (120, 0.12)):
+        pairs = random_pairs(rng, n, p)
+        g = ga.build_graph_from_edges(n, ga.canonical_edges(pairs))
+        rg = reference.build_graph_from_edges(n, ga.canonical_edges(pairs))
+        tris = triangles_of(g)
+        core, _, _ = oracle.core_levels(g)
+        ex, ce = ga.exact_densest_host(g.n, tris), ga.core_exact_host(g, tris, core)
+        assert ex.tri * ce.verts == ce.tri * ex.verts
+        for ours, theirs in ((ex, reference.exact_densest(rg)), (ce, reference.core_exact(rg, core))):
+            assert (ours.tri, ours.verts, ours.set.tolist(), ours.flow_calls) == (
+                theirs.tri, theirs.verts, theirs.set.tolist(), theirs.flow_calls)
+        ip, ie = incidence_of(g.n, tris)
+        ours, theirs = ga.greedy_pp_host(g.n, core, ip, ie, 4), reference.greedy_pp(rg, 4)
+        assert (ours.tri, ours.verts, ours.set.tolist()) == (theirs.tri, theirs.verts, theirs.set.tolist())
