@@ -200,3 +200,15 @@ def test_density_ties_in_one_batch(ga, cuda_ok):
                 assert (got.best_num, got.best_den, got.best_round, got.rounds) == (
                     want["best_num"], want["best_den"], want["best_round"], want["rounds"]), (i, key)
                 assert got.removed_round.tolist() == want["removed_round"]
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+@pytest.mark.parametrize("eps", [(1, 10), (0, 1), (3, 7)])
+def test_gpu_best_round_recomputed_from_removed_round(ga, cuda_ok, name, eps):
+    """The device loop's PeelResult against what its removed_round array alone implies (the reference's emulator
+    check, emu_densest.cpp:44-54,153-166)."""
+    from peel_check import best_from_removed_round
+    g = ga.load_graph(fixture_path(name))
+    with ga.DeviceGraph(g) as d:
+        r = d.batch_peel(*eps)
+    assert (r.best_num, r.best_den, r.best_round, r.rounds) == best_from_removed_round(g, r.removed_round)

@@ -188,3 +188,13 @@ def test_oracle_matches_reference_on_density_ties(oracle, i):
         assert r.removed_round.tolist() == want["removed_round"]
     core, kmax, rounds = oracle.core_levels(g)
     assert (kmax, rounds, core.tolist()) == (t["kmax"], t["core_rounds"], t["core"])
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+@pytest.mark.parametrize("eps", [(1, 10), (0, 1), (3, 7)])
+def test_best_round_recomputed_from_removed_round(oracle, name, eps):
+    """The oracle's PeelResult against what its own removed_round array implies (the reference's emulator check)."""
+    from peel_check import best_from_removed_round
+    g = oracle.load_graph(fixture_path(name))
+    r = oracle.batch_peel(g, *eps)
+    assert (r.best_num, r.best_den, r.best_round, r.rounds) == best_from_removed_round(g, r.removed_round)
