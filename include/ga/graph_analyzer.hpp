@@ -17,6 +17,7 @@
 //   greedy, greedy_pp, core_exact, exact_densest         dsg.h:189-250, 463-627, 405-428 (device triangle lists)
 //   prune_to_core                                        dsg.h:638-645
 //   GreedyResult, greedy_peel                            cpu_greedy_peel, densest.h:193-252 (the same greedy)
+//   DeviceBatch, Server                                  batches and the request loop (no counterpart)
 //
 // Everything lives in namespace ga; define GA_B200_GLOBAL_NAMES before including to also get the reference's
 // unqualified names. Errors follow the reference: functions that returned bool return false (load_graph), results
@@ -232,6 +233,101 @@ inline CoreLoopResult core_decomp_loop_inc(uint32_t n, uint64_t T_full, DeviceGr
     r.kmax = res.kmax;
     return r;
 }
+
+// ---- many graphs at once, and serving (no counterpart in the reference) ----------------------------------------
+// A batch of host graphs resident on one device: one count launch and one peeling loop for all of them.
+class DeviceBatch {
+  public:
+    explicit DeviceBatch(const std::vector<const Graph*>& graphs, int device = 0, void* stream = nullptr) {
+        const uint32_t G = (uint32_t)graphs.size();
+        std::vector<uint64_t> vtx(G + 1, 0), edge(G + 1, 0);
+        for (uint32_t i = 0; i < G; i++) {
+            vtx[i + 1] = vtx[i] + graphs[i]->n;
+            edge[i + 1] = edge[i] + graphs[i]->m;
+        }
+        std::vector<uint32_t> rowptr, col;
+        rowptr.reserve(vtx[G] + G);
+        col.reserve(edge[G]);
+        for (const Graph* g : graphs) {   // local offsets and local ids, graph after graph
+            rowptr.insert(rowptr.end(), g->rowptr.begin(), g->rowptr.end());
+            col.insert(col.end(), g->col.begin(), g->col.end());
+        }
+        check(ga_batch_create(G, vtx.data(), edge.data(), rowptr.data(), col.empty() ? nullptr : col.data(), device,
+                              stream, &h_));
+        count_ = G;
+        vtx_ = std::move(vtx);
+    }
+    ~DeviceBatch() { if (h_) ga_batch_destroy(h_); }
+    DeviceBatch(const DeviceBatch&) = delete;
+    DeviceBatch& operator=(const DeviceBatch&) = delete;
+
+    ga_batch* handle() const { return h_; }
+    std::vector<uint64_t> triangles() {
+        std::vector<uint64_t> t(count_);
+        check(ga_batch_tc(h_, t.data()));
+        return t;
+    }
+    // Every graph counted and peeled (eps = num/den) as if alone: its PeelResult with its own removed_round
+    // (ok = false with the reason when peel_arith_ok refused that graph); its triangle count into *triangles.
+    std::vector<PeelResult> tc_peel(uint64_t num, uint64_t den, std::vector<uint64_t>* triangles = nullptr) {
+        std::vector<uint64_t> t(count_);
+        std::vector<ga_peel_result> res(count_);
+        std::vector<uint32_t> status(count_), removed(vtx_[count_]);
+        check(ga_batch_tc_peel(h_, num, den, t.data(), res.data(), status.data(),
+                               removed.empty() ? nullptr : removed.data()));
+        std::vector<PeelResult> out(count_);
+        for (uint32_t i = 0; i < count_; i++) {
+            PeelResult& r = out[i];
+            r.best_num = res[i].best_num;
+            r.best_den = res[i].best_den;
+            r.best_round = res[i].best_round;
+            r.rounds = res[i].rounds;
+            r.removed_round.assign(removed.begin() + (ptrdiff_t)vtx_[i], removed.begin() + (ptrdiff_t)vtx_[i + 1]);
+            if (status[i] != GA_OK) {
+                r.ok = false;
+                r.error = ga_status_string((ga_status)status[i]);
+            }
+        }
+        if (triangles) *triangles = t;
+        return out;
+    }
+
+  private:
+    ga_batch* h_ = nullptr;
+    uint32_t count_ = 0;
+    std::vector<uint64_t> vtx_;   // vertex offsets of the graphs in batch order
+};
+
+// The request loop of ga_server_*: register graphs, submit counts / peels / core decompositions, wait for results.
+class Server {
+  public:
+    explicit Server(const ga_server_config* cfg = nullptr) {
+        ga_server_config c{};
+        check(ga_server_create(cfg ? cfg : &c, &h_));
+    }
+    ~Server() { if (h_) ga_server_destroy(h_); }
+    Server(const Server&) = delete;
+    Server& operator=(const Server&) = delete;
+
+    uint64_t add_graph(const Graph& g) {
+        uint64_t id = 0;
+        check(ga_server_add_graph(h_, g.rowptr.data(), g.m ? g.col.data() : nullptr, g.n, g.m, &id));
+        return id;
+    }
+    uint64_t submit(uint64_t graph_id, ga_request_kind kind, uint64_t num = 1, uint64_t den = 10) {
+        uint64_t t = 0;
+        check(ga_server_submit(h_, graph_id, kind, num, den, &t));
+        return t;
+    }
+    ga_request_result wait(uint64_t ticket) {
+        ga_request_result r{};
+        check(ga_server_wait(h_, ticket, &r));
+        return r;
+    }
+
+  private:
+    ga_server* h_ = nullptr;
+};
 
 // ---- densest subgraph by triangle density (dsg.h) -----------------------------------------------------------------
 struct Dens {

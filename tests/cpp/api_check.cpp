@@ -50,6 +50,24 @@ int main(int argc, char** argv) {
         std::printf("dsg %llu %llu %u %u %llu %llu %llu %llu %u\n", (unsigned long long)gr.tri,
                     (unsigned long long)gr.verts, gp.n, gp.m, (unsigned long long)gpp.tri, (unsigned long long)gpp.verts,
                     (unsigned long long)ex.tri, (unsigned long long)ex.verts, ex.flow_calls);
+        // the same graph twice in one batch, and through the request loop: each result equals the single-graph one
+        {
+            ga::DeviceBatch b({&g, &g});
+            std::vector<uint64_t> bt;
+            std::vector<PeelResult> bp = b.tc_peel(num, den, &bt);
+            const bool same = bp.size() == 2 && bp[0] == r && bp[1] == r && bt[0] == T_full && bt[1] == T_full &&
+                              b.triangles() == bt;
+            ga::Server srv;
+            const uint64_t id = srv.add_graph(g);
+            const uint64_t t_tc = srv.submit(id, GA_REQ_TC), t_peel = srv.submit(id, GA_REQ_PEEL, num, den),
+                           t_core = srv.submit(id, GA_REQ_CORE);
+            const ga_request_result a = srv.wait(t_tc), p = srv.wait(t_peel), q = srv.wait(t_core);
+            const bool served = a.status == GA_OK && a.triangles == T_full && p.status == GA_OK &&
+                                p.peel.best_num == r.best_num && p.peel.best_den == r.best_den &&
+                                p.peel.best_round == r.best_round && p.peel.rounds == r.rounds &&
+                                q.status == GA_OK && q.core.kmax == c.kmax && q.core.rounds == c.rounds;
+            std::printf("batch_serve %d %d\n", same ? 1 : 0, served ? 1 : 0);
+        }
         // the refusals of batch_peel_loop (densest.h:65-78, 283-287): wrong T_full, eps out of range
         PeelResult bad = batch_peel_loop(g.n, T_full + 1, num, den, d);
         PeelResult bad_eps = batch_peel_loop(g.n, T_full, 1, 0, d);

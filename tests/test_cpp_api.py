@@ -50,6 +50,7 @@ def test_reference_names_match_golden(api_check, golden, cuda_ok, name):
     assert out["cores"].split() == [str(w["kmax"]), str(w["core_rounds"]), _hash(a["core"])]
     assert out["supports"].split() == [str(w["triangles"])] * 2
     assert out["refusals"].split() == ["0", "0"]
+    assert out["batch_serve"].split() == ["1", "1"]      # DeviceBatch and Server give the single-graph results
     with open(os.path.join(GOLDEN, "dsg.json")) as f:
         rec = {x["name"]: x for x in json.load(f)["graphs"]}[name]
     p = rec["pipeline"]
