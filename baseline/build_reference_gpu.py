@@ -2,7 +2,7 @@
 of its Makefile (-O3 -std=c++17 -Xcompiler -fopenmp), into baseline/_ref/bin/. They are run only as a comparison
 (`bench.py --workload reference-gpu`): the reference's kernels v1-v9 on the same graph and the same GPU.
 
-Usage: python baseline/build_reference_gpu.py [reference_root]   (default: /root/reference)
+Usage: python baseline/build_reference_gpu.py [reference_root]   (default: $GA_REFERENCE_ROOT, else /root/reference)
 """
 from __future__ import annotations
 
@@ -14,9 +14,10 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref", "bin")
 PROGRAMS = ["gpu_tc", "gpu_densest", "gpu_dsg"]
+REF_ROOT = os.environ.get("GA_REFERENCE_ROOT", "/root/reference")
 
 
-def build(ref_root: str = "/root/reference") -> list[str]:
+def build(ref_root: str = REF_ROOT) -> list[str]:
     src = os.path.join(ref_root, "src")
     if not os.path.isdir(src):
         raise FileNotFoundError(f"{src} not found")
@@ -34,4 +35,4 @@ def build(ref_root: str = "/root/reference") -> list[str]:
 
 
 if __name__ == "__main__":
-    print("\n".join(build(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")))
+    print("\n".join(build(sys.argv[1] if len(sys.argv) > 1 else REF_ROOT)))

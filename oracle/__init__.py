@@ -86,6 +86,8 @@ class Oracle(_Base):
         L.or_participation.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, _u32p, _u8p, _u32p]
         L.or_edge_support.restype = C.c_uint64
         L.or_edge_support.argtypes = [C.c_uint32, _u32p, _u32p, _u32p, _u32p]
+        L.or_edge_support_omp.restype = C.c_uint64
+        L.or_edge_support_omp.argtypes = [C.c_uint32, _u32p, _u32p, _u32p, _u32p]
         L.or_triangle_degrees.restype = C.c_uint64
         L.or_triangle_degrees.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, _u32p, _u64p]
         L.or_peel_arith_ok.restype = C.c_int
@@ -103,6 +105,9 @@ class Oracle(_Base):
         L.or_core_levels.restype = C.c_int
         L.or_core_levels.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, _u32p, _u32p, C.POINTER(C.c_uint32),
                                      C.POINTER(C.c_uint32)]
+        L.or_core_levels_inc.restype = C.c_int
+        L.or_core_levels_inc.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, _u32p, _u32p, C.POINTER(C.c_uint32),
+                                         C.POINTER(C.c_uint32)]
         L.or_core_level_density.restype = None
         L.or_core_level_density.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, _u32p, _u32p, C.c_uint32,
                                             C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
@@ -152,9 +157,10 @@ class Oracle(_Base):
         T = self.lib.or_participation(g.n, g.m, g.rowptr, _col(g), _src(g), _alive(alive, g.n), tri)
         return int(T), tri[: g.n]
 
-    def edge_support(self, g: CSR) -> tuple[int, np.ndarray]:
+    def edge_support(self, g: CSR, use_omp: bool = False) -> tuple[int, np.ndarray]:
         sup = np.zeros(max(g.m, 1), np.uint32)
-        T = self.lib.or_edge_support(g.m, g.rowptr, _col(g), _src(g), sup)
+        f = self.lib.or_edge_support_omp if use_omp else self.lib.or_edge_support
+        T = f(g.m, g.rowptr, _col(g), _src(g), sup)
         return int(T), sup[: g.m]
 
     def triangle_degrees(self, g: CSR) -> tuple[int, np.ndarray]:
@@ -195,6 +201,17 @@ class Oracle(_Base):
         k, r = C.c_uint32(0), C.c_uint32(0)
         if self.lib.or_core_levels(g.n, g.m, g.rowptr, _col(g), _src(g), core, C.byref(k), C.byref(r)) != 0:
             raise OverflowError("triangle count >= 2^32")
+        return core[: g.n], int(k.value), int(r.value)
+
+    def core_levels_inc(self, g: CSR) -> tuple[np.ndarray, int, int]:
+        """Same as core_levels (core[], kmax, level rounds) by the incremental frontier loop: O(T) updates."""
+        core = np.zeros(max(g.n, 1), np.uint32)
+        k, r = C.c_uint32(0), C.c_uint32(0)
+        rc = self.lib.or_core_levels_inc(g.n, g.m, g.rowptr, _col(g), _src(g), core, C.byref(k), C.byref(r))
+        if rc == -1:
+            raise OverflowError("triangle count >= 2^32")
+        if rc != 0:
+            raise MemoryError("or_core_levels_inc: out of host memory")
         return core[: g.n], int(k.value), int(r.value)
 
     def core_level_density(self, g: CSR, core: np.ndarray, k: int) -> tuple[int, int]:
@@ -238,6 +255,8 @@ class Reference(_Base):
         L.ref_graph_triangles_omp.argtypes = [C.c_void_p]
         L.ref_graph_triangles_omp_rows.restype = C.c_uint64
         L.ref_graph_triangles_omp_rows.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
+        L.ref_graph_triangles_serial_rows.restype = C.c_uint64
+        L.ref_graph_triangles_serial_rows.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
         L.ref_participation.restype = C.c_uint64
         L.ref_participation.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, _u32p, _u8p, _u32p, C.c_int]
         L.ref_edge_support.restype = C.c_uint64
@@ -444,6 +463,9 @@ class RefGraph:
 
     def triangles_omp_rows(self, u0: int, u1: int) -> int:
         return int(self.ref.lib.ref_graph_triangles_omp_rows(self.h, u0, u1))
+
+    def triangles_serial_rows(self, u0: int, u1: int) -> int:
+        return int(self.ref.lib.ref_graph_triangles_serial_rows(self.h, u0, u1))
 
     def close(self) -> None:
         if self.h:

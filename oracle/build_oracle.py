@@ -15,7 +15,9 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = "/root/reference/src"
+# root of the reference's source tree (read only); GA_REFERENCE_ROOT overrides the default location
+REF_ROOT = os.environ.get("GA_REFERENCE_ROOT", "/root/reference")
+REF_SRC = os.path.join(REF_ROOT, "src")
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libga_ref.so")
 

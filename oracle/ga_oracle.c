@@ -208,6 +208,36 @@ uint64_t or_edge_support(uint32_t m, const uint32_t* rowptr, const uint32_t* col
     return T;
 }
 
+/* The same sum over edges with OpenMP threads (edges in dynamic chunks; the three increments of a triangle are
+ * atomic, so the result is or_edge_support's exactly). For graphs whose serial pass takes minutes. */
+uint64_t or_edge_support_omp(uint32_t m, const uint32_t* rowptr, const uint32_t* col, const uint32_t* src,
+                             uint32_t* sup) {
+    memset(sup, 0, (size_t)m * sizeof(uint32_t));
+    uint64_t T = 0;
+#pragma omp parallel for schedule(dynamic, 4096) reduction(+ : T)
+    for (int64_t e = 0; e < (int64_t)m; e++) {
+        const uint32_t u = src[e], v = col[e];
+        uint32_t i = rowptr[u], iend = rowptr[u + 1], j = rowptr[v], jend = rowptr[v + 1];
+        while (i < iend && j < jend) {
+            const uint32_t a = col[i], b = col[j];
+            if (a < b) i++;
+            else if (a > b) j++;
+            else {
+                T++;
+#pragma omp atomic
+                sup[e]++;
+#pragma omp atomic
+                sup[i]++;
+#pragma omp atomic
+                sup[j]++;
+                i++;
+                j++;
+            }
+        }
+    }
+    return T;
+}
+
 /* dsg.h:82-87. */
 uint64_t or_triangle_degrees(uint32_t n, uint32_t m, const uint32_t* rowptr, const uint32_t* col, const uint32_t* src,
                              uint64_t* deg) {
@@ -428,6 +458,138 @@ int or_core_levels(uint32_t n, uint32_t m, const uint32_t* rowptr, const uint32_
     free(tri);
     free(alive);
     return rc;
+}
+
+/* core_decomp_loop_inc (dsg.h:724-751) with the semantics of its kernels (kernels.cuh:484-626) restated serially:
+ * per round k = max(k, min over alive of tri), the frontier is every alive vertex with tri <= k (core = k), and every
+ * triangle with a frontier corner and no corner removed earlier takes one triangle off each of its alive
+ * non-frontier corners, once (its smallest-id frontier corner applies it). The triangles through each vertex are
+ * listed once up front (OpenMP over oriented edges), so the whole run costs O(T) updates instead of a recount per
+ * round; the frontier is taken from a lazy min-heap of (tri, v). Same core[], kmax and round count as
+ * or_core_levels. Returns 0, -1 when T >= 2^32 (dsg.h:727), or -2 when memory runs out. */
+int or_core_levels_inc(uint32_t n, uint32_t m, const uint32_t* rowptr, const uint32_t* col, const uint32_t* src,
+                       uint32_t* core, uint32_t* kmax, uint32_t* rounds) {
+    *kmax = 0;
+    *rounds = 0;
+    uint64_t* ptr = (uint64_t*)calloc((size_t)n + 1, sizeof(uint64_t));
+    uint32_t* tri = (uint32_t*)calloc(n ? n : 1, sizeof(uint32_t));
+    if (!ptr || !tri) { free(ptr); free(tri); return -2; }
+    /* pass 1: triangle degree of every vertex (the list lengths) */
+    uint64_t T = 0;
+#pragma omp parallel for schedule(dynamic, 4096) reduction(+ : T)
+    for (int64_t e = 0; e < (int64_t)m; e++) {
+        const uint32_t u = src[e], v = col[e];
+        uint32_t i = rowptr[u], iend = rowptr[u + 1], j = rowptr[v], jend = rowptr[v + 1];
+        while (i < iend && j < jend) {
+            const uint32_t a = col[i], b = col[j];
+            if (a < b) i++;
+            else if (a > b) j++;
+            else {
+                T++;
+#pragma omp atomic
+                tri[u]++;
+#pragma omp atomic
+                tri[v]++;
+#pragma omp atomic
+                tri[a]++;
+                i++;
+                j++;
+            }
+        }
+    }
+    if (T >= (1ull << 32)) { free(ptr); free(tri); return -1; }
+    for (uint32_t v = 0; v < n; v++) ptr[v + 1] = ptr[v] + tri[v];
+    uint32_t* inc = (uint32_t*)malloc((size_t)(3 * T ? 3 * T : 1) * 2 * sizeof(uint32_t));
+    uint64_t* fill = (uint64_t*)malloc((size_t)(n ? n : 1) * sizeof(uint64_t));
+    uint8_t* state = (uint8_t*)malloc(n ? n : 1);
+    uint8_t* touched_flag = (uint8_t*)calloc(n ? n : 1, 1);
+    uint32_t* frontier = (uint32_t*)malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
+    uint32_t* touched = (uint32_t*)malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
+    if (!inc || !fill || !state || !touched_flag || !frontier || !touched) {
+        free(ptr); free(tri); free(inc); free(fill); free(state); free(touched_flag); free(frontier); free(touched);
+        return -2;
+    }
+    memcpy(fill, ptr, (size_t)n * sizeof(uint64_t));
+    /* pass 2: for each corner the other two corners of each triangle through it */
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t e = 0; e < (int64_t)m; e++) {
+        const uint32_t u = src[e], v = col[e];
+        uint32_t i = rowptr[u], iend = rowptr[u + 1], j = rowptr[v], jend = rowptr[v + 1];
+        while (i < iend && j < jend) {
+            const uint32_t a = col[i], b = col[j];
+            if (a < b) i++;
+            else if (a > b) j++;
+            else {
+                const uint32_t c3[3] = {u, v, a};
+                for (int q = 0; q < 3; q++) {
+                    uint64_t p;
+#pragma omp atomic capture
+                    p = fill[c3[q]]++;
+                    inc[2 * p] = c3[(q + 1) % 3];
+                    inc[2 * p + 1] = c3[(q + 2) % 3];
+                }
+                i++;
+                j++;
+            }
+        }
+    }
+    free(fill);
+    heap_t h = {NULL, 0, 0};
+    for (uint32_t v = 0; v < n; v++) { state[v] = 1; core[v] = UINT32_MAX; h_push(&h, tri[v], v); }
+    uint64_t nalive = n, k = 0;
+    uint32_t r = 0;
+    while (nalive > 0) {
+        /* k = max(k, min over alive tri): drop stale heap entries first */
+        while (h.n && (state[h.a[0].v] != 1 || h.a[0].key != tri[h.a[0].v])) h_pop(&h);
+        if (!h.n) break;
+        if (h.a[0].key > k) k = h.a[0].key;
+        /* frontier: every alive vertex with tri <= k (all have a current entry with that key in the heap) */
+        size_t nf = 0;
+        while (h.n && h.a[0].key <= k) {
+            const hentry x = h_pop(&h);
+            if (state[x.v] != 1 || x.key != tri[x.v]) continue;
+            state[x.v] = 2;
+            core[x.v] = (uint32_t)k;
+            frontier[nf++] = x.v;
+        }
+        /* update: each destroyed triangle once, from its smallest-id frontier corner */
+        size_t nt = 0;
+#pragma omp parallel for schedule(dynamic, 64) if (nf > 256)
+        for (int64_t fi = 0; fi < (int64_t)nf; fi++) {
+            const uint32_t u = frontier[fi];
+            for (uint64_t p = ptr[u]; p < ptr[u + 1]; p++) {
+                const uint32_t a = inc[2 * p], b = inc[2 * p + 1];
+                const uint8_t sa = state[a], sb = state[b];
+                if (sa == 0 || sb == 0) continue;                          /* destroyed in an earlier round */
+                if ((sa == 2 && a < u) || (sb == 2 && b < u)) continue;    /* a smaller frontier corner applies it */
+                const uint32_t us[2] = {a, b};
+                const uint8_t ss[2] = {sa, sb};
+                for (int q = 0; q < 2; q++) {
+                    if (ss[q] != 1) continue;
+                    const uint32_t x = us[q];
+#pragma omp atomic
+                    tri[x]--;
+                    uint8_t was;
+#pragma omp atomic capture
+                    { was = touched_flag[x]; touched_flag[x] = 1; }
+                    if (!was) {
+                        size_t slot;
+#pragma omp atomic capture
+                        slot = nt++;
+                        touched[slot] = x;
+                    }
+                }
+            }
+        }
+        for (size_t i = 0; i < nt; i++) { touched_flag[touched[i]] = 0; h_push(&h, tri[touched[i]], touched[i]); }
+        for (size_t i = 0; i < nf; i++) state[frontier[i]] = 0;           /* retire */
+        nalive -= nf;
+        r++;
+    }
+    *kmax = (uint32_t)k;
+    *rounds = r;
+    free(h.a); free(ptr); free(tri); free(inc); free(state); free(touched_flag); free(frontier); free(touched);
+    return 0;
 }
 
 /* dsg.h:169-174 with count_triangles_in (dsg.h:90-94). */

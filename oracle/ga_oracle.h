@@ -45,6 +45,9 @@ uint64_t or_participation(uint32_t n, uint32_t m, const uint32_t* rowptr, const 
 /* Per-edge support through for_each_triangle (dsg.h:67-79): every triangle found at oriented edge e with witness
  * positions i, j adds one to sup[e], sup[i], sup[j]. sup has m entries (indexed like col). Returns T. */
 uint64_t or_edge_support(uint32_t m, const uint32_t* rowptr, const uint32_t* col, const uint32_t* src, uint32_t* sup);
+/* The same with OpenMP threads (atomic increments; identical result). */
+uint64_t or_edge_support_omp(uint32_t m, const uint32_t* rowptr, const uint32_t* col, const uint32_t* src,
+                             uint32_t* sup);
 
 /* triangle_degrees (dsg.h:82-87): 64-bit triangle degree per vertex. Returns T. */
 uint64_t or_triangle_degrees(uint32_t n, uint32_t m, const uint32_t* rowptr, const uint32_t* col, const uint32_t* src,
@@ -78,6 +81,12 @@ int or_core_decomposition(uint32_t n, uint32_t m, const uint32_t* rowptr, const 
  * when T >= 2^32 (dsg.h:696). */
 int or_core_levels(uint32_t n, uint32_t m, const uint32_t* rowptr, const uint32_t* col, const uint32_t* src,
                    uint32_t* core, uint32_t* kmax, uint32_t* rounds);
+
+/* core_decomp_loop_inc (dsg.h:724-751, kernels.cuh:484-626): the same level rounds as or_core_levels without a
+ * recount per round (triangles listed once per vertex, O(T) updates, frontier from a lazy heap); for graphs where
+ * thousands of rounds make the recount form too slow. Returns 0, -1 when T >= 2^32, -2 when memory runs out. */
+int or_core_levels_inc(uint32_t n, uint32_t m, const uint32_t* rowptr, const uint32_t* col, const uint32_t* src,
+                       uint32_t* core, uint32_t* kmax, uint32_t* rounds);
 
 /* core_level_density (dsg.h:169-174): triangles and vertices of {v : core[v] >= k}. */
 void or_core_level_density(uint32_t n, uint32_t m, const uint32_t* rowptr, const uint32_t* col, const uint32_t* src,

@@ -84,6 +84,22 @@ uint64_t ref_graph_triangles_omp_rows(void* h, uint32_t u0, uint32_t u1) {
     return t;
 }
 
+// cpu_triangles_serial's loop (graph.h:110-121) on the resident copy, restricted to the rows [u0, u1): the serial
+// baseline on a bounded sample (only the bounds differ from the reference's function).
+uint64_t ref_graph_triangles_serial_rows(void* h, uint32_t u0, uint32_t u1) {
+    const Graph& g = *static_cast<const Graph*>(h);
+    uint64_t t = 0;
+    for (uint32_t u = u0; u < u1; u++) {
+        const uint32_t* nu = g.col.data() + g.rowptr[u];
+        const uint32_t du = g.rowptr[u + 1] - g.rowptr[u];
+        for (uint32_t k = 0; k < du; k++) {
+            const uint32_t v = nu[k];
+            t += intersect_count(nu, du, g.col.data() + g.rowptr[v], g.rowptr[v + 1] - g.rowptr[v]);
+        }
+    }
+    return t;
+}
+
 // cpu_triangles_serial / cpu_triangles_omp (graph.h:110,123)
 uint64_t ref_triangles_serial(uint32_t n, uint32_t m, const uint32_t* rowptr, const uint32_t* col, const uint32_t* src) {
     return cpu_triangles_serial(make_graph(n, m, rowptr, col, src));

@@ -8,7 +8,8 @@
    triangle degrees, batch peeling for several eps, core numbers (Alg 3), level-round count (core_decomp_loop) and the
    kmax-core density. They are stored as ``<name>.npz``.
 
-Usage: ``python tests/golden/make_golden.py`` (needs /root/reference; the outputs are committed).
+Usage: ``python tests/golden/make_golden.py`` (needs the reference tree: $GA_REFERENCE_ROOT, else /root/reference;
+the outputs are committed).
 """
 from __future__ import annotations
 
@@ -23,8 +24,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from oracle import Reference  # noqa: E402
+from oracle.build_oracle import REF_ROOT  # noqa: E402
 
-REF_SCRIPTS = "/root/reference/scripts"
+REF_SCRIPTS = os.path.join(REF_ROOT, "scripts")
 FIXTURES = [
     ("t_er300", "gen_test_graph.py", ["300", "0.05", "1"]),
     ("t_er800", "gen_test_graph.py", ["800", "0.02", "7"]),

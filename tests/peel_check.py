@@ -11,11 +11,12 @@ NEVER = 0xFFFFFFFF
 
 
 def best_from_removed_round(g, removed_round: np.ndarray) -> tuple[int, int, int, int]:
-    """(best_num, best_den, best_round, rounds) implied by removed_round."""
+    """(best_num, best_den, best_round, rounds) implied by removed_round. Like the reference's check
+    (emu_densest.cpp:153), every vertex must have been removed in some round: a loop that stopped early fails here
+    instead of passing with never-removed vertices read as alive for ever."""
     rr = removed_round.astype(np.int64)
-    rr[rr == NEVER] = np.iinfo(np.int64).max
-    finite = rr[rr != np.iinfo(np.int64).max]
-    rounds = int(finite.max()) + 1 if finite.size else 0
+    assert not (rr == NEVER).any(), f"{int((rr == NEVER).sum())} vertices never removed"
+    rounds = int(rr.max()) + 1 if rr.size else 0
     tris = triangles_of(g)
     # a triangle lives while all its corners do: it leaves in the round its first corner leaves
     gone = np.minimum(np.minimum(rr[tris[:, 0]], rr[tris[:, 1]]), rr[tris[:, 2]]) if len(tris) else np.zeros(0)

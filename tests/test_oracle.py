@@ -198,3 +198,29 @@ def test_best_round_recomputed_from_removed_round(oracle, name, eps):
     g = oracle.load_graph(fixture_path(name))
     r = oracle.batch_peel(g, *eps)
     assert (r.best_num, r.best_den, r.best_round, r.rounds) == best_from_removed_round(g, r.removed_round)
+
+
+def test_incremental_level_loop_matches_reference(oracle, reference):
+    """or_core_levels_inc (core_decomp_loop_inc restated with listed triangles) against the reference's own level loop
+    (core_decomp_loop with a recount per round) and Alg 3, on fixtures, hubs, random, Holme-Kim and R-MAT graphs;
+    or_edge_support_omp against the reference's for_each_triangle supports."""
+    rng = np.random.default_rng(7)
+    graphs = [oracle.load_graph(fixture_path(name)) for name in FIXTURES]
+    for _ in range(4):
+        n, raw = hub_pairs(rng, int(rng.integers(1, 4)), int(rng.integers(40, 101)), int(rng.integers(8, 16)))
+        graphs.append(oracle.build_graph_from_edges(n, oracle.canonical_edges(raw)))
+    graphs.append(oracle.build_graph_from_edges(120, random_pairs(rng, 120, 0.2)))
+    graphs.append(oracle.build_graph_from_edges(1, np.zeros((0, 2), np.uint32)))
+    import graph_analyzer_b200 as ga
+    graphs.append(ga.graph_from_pairs(20000, ga.gen_holme_kim(20000, 6, 7, 0.54, 0.4, seed=9)))
+    graphs.append(ga.graph_from_pairs(1 << 11, ga.gen_rmat(11, 10 << 11, seed=2)))
+    for g in graphs:
+        r = reference.build_graph_from_edges(g.n, np.stack([g.src, g.col], 1)) if g.m else g
+        core, kmax, rounds = oracle.core_levels_inc(g)
+        cr, kr, rr = reference.core_levels(r)
+        assert (kmax, rounds) == (kr, rr) and np.array_equal(core, cr)
+        ca, ka = reference.core_decomposition(r)
+        assert ka == kmax and np.array_equal(ca, core)
+        T, sup = oracle.edge_support(g, use_omp=True)
+        Tr, supr = reference.edge_support(r)
+        assert T == Tr and np.array_equal(sup, supr)
