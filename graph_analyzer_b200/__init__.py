@@ -114,6 +114,18 @@ class _HostBatch(C.Structure):
 
 
 # (name, argtypes) of every exported entry point; the library must export all of them.
+class _Tuning(C.Structure):
+    _fields_ = [("kernel", C.c_uint32), ("light_max_deg", C.c_uint32), ("item_work", C.c_uint32),
+                ("reserved", C.c_uint32), ("signature", C.c_uint64), ("measured_ms", C.c_double),
+                ("heavy_items", C.c_uint64), ("light_items", C.c_uint64)]
+
+
+def _tuning_dict(t: _Tuning) -> dict:
+    return {"kernel": {1: "plain", 2: "hash"}.get(t.kernel, str(t.kernel)), "light_max_deg": t.light_max_deg,
+            "item_work": t.item_work, "signature": f"{t.signature:016x}", "measured_ms": t.measured_ms,
+            "heavy_items": t.heavy_items, "light_items": t.light_items}
+
+
 SIGNATURES: dict[str, list] = {
     "ga_status_string": [C.c_int],
     "ga_last_error": [],
@@ -146,6 +158,9 @@ SIGNATURES: dict[str, list] = {
     "ga_tc_support_edges_device": [_vp, _vp, C.POINTER(C.c_uint64)],
     "ga_tc_support_vertices": [_vp, _vp, C.POINTER(C.c_uint64)],
     "ga_tc_participation": [_vp, _vp, _vp, C.POINTER(C.c_uint64)],
+    "ga_core_level_density": [_vp, _vp, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
+    "ga_graph_tuning": [_vp, C.POINTER(_Tuning)],
+    "ga_batch_tuning": [_vp, C.POINTER(_Tuning)],
     "ga_batch_peel": [_vp, C.c_uint64, C.c_uint64, C.POINTER(_PeelRes), _vp],
     "ga_core_decomposition": [_vp, _vp, C.POINTER(_CoreRes)],
     "ga_greedy_pp": [_vp, C.c_uint32, C.POINTER(_DsgRes), _vp, _vp],
@@ -170,6 +185,8 @@ SIGNATURES: dict[str, list] = {
     "ga_server_destroy": [_vp],
     "ga_server_add_graph": [_vp, _u32p, _vp, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64)],
     "ga_server_submit": [_vp, C.c_uint64, C.c_int, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)],
+    "ga_server_submit_out": [_vp, C.c_uint64, C.c_int, C.c_uint64, C.c_uint64, _vp, C.c_uint64,
+                             C.POINTER(C.c_uint64)],
     "ga_server_poll": [_vp, C.c_uint64, C.POINTER(_RequestResult)],
     "ga_server_wait": [_vp, C.c_uint64, C.POINTER(_RequestResult)],
     "ga_server_stats_get": [_vp, C.POINTER(_ServerStats)],
@@ -570,6 +587,22 @@ class DeviceGraph:
                                          C.byref(t)))
         return t.value, tri[: self.n]
 
+    def tuning(self) -> dict:
+        """The count configuration (kernel, bin cutoff, item work) the autotuner chose for this graph."""
+        t = _Tuning()
+        _check(lib().ga_graph_tuning(self._h, C.byref(t)))
+        return _tuning_dict(t)
+
+    def core_level_density(self, core: np.ndarray, k: int) -> tuple[int, int]:
+        """(triangles, vertices) of {v : core[v] >= k} (core_level_density, dsg.h:169-174)."""
+        c = np.ascontiguousarray(core, np.uint32)
+        if c.size != self.n:
+            raise ValueError("core must have n entries")
+        t, v = C.c_uint64(0), C.c_uint64(0)
+        _check(lib().ga_core_level_density(self._h, _ptr(c if self.n else np.zeros(1, np.uint32)), k, C.byref(t),
+                                           C.byref(v)))
+        return t.value, v.value
+
     def batch_peel(self, num: int = 1, den: int = 10, want_removed: bool = True) -> PeelResult:
         r = _PeelRes()
         rr = np.full(max(self.n, 1), 0xFFFFFFFF, np.uint32) if want_removed else None
@@ -736,6 +769,12 @@ class DeviceBatch:
         _check(lib().ga_batch_device_bytes(self._h, C.byref(b)))
         return b.value
 
+    def tuning(self) -> dict:
+        """The count configuration of the batch's launch over the union of its graphs."""
+        t = _Tuning()
+        _check(lib().ga_batch_tuning(self._h, C.byref(t)))
+        return _tuning_dict(t)
+
     def tc(self) -> np.ndarray:
         t = np.zeros(self.G, np.uint64)
         _check(lib().ga_batch_tc(self._h, _ptr(t)))
@@ -767,12 +806,13 @@ GA_ERR_NOT_READY = 12
 class RequestResult:
     status: int
     triangles: int
-    peel: PeelResult            # REQ_PEEL (integer fields; removed_round is not returned by the server)
+    peel: PeelResult            # REQ_PEEL (removed_round filled when the request was submitted with want_array)
     core: tuple[int, int]       # REQ_CORE: (kmax, rounds)
     queue_ms: float
     run_ms: float
     folded: int                 # graphs served by the same launch (1 = alone)
     resident_hit: bool
+    core_numbers: np.ndarray | None = None   # REQ_CORE submitted with want_array: core[v] for every vertex
 
 
 def _request_result(r: _RequestResult) -> RequestResult:
@@ -790,6 +830,8 @@ class Server:
         cfg = _ServerConfig(device, hbm_budget_bytes, slots, fold_max_graphs, fold_max_edges, small_slots,
                             pin_min_edges)
         h = _vp()
+        self._n: dict[int, int] = {}                      # vertices per registered graph
+        self._arrays: dict[int, tuple] = {}               # ticket -> (kind, host array the server writes, n)
         _check(lib().ga_server_create(C.byref(cfg), C.byref(h)))
         self._h = h
 
@@ -816,12 +858,32 @@ class Server:
         rowptr = np.ascontiguousarray(g.rowptr, np.uint32)
         col = np.ascontiguousarray(g.col, np.uint32)
         _check(lib().ga_server_add_graph(self._h, rowptr, _ptr(col) if g.m else None, g.n, g.m, C.byref(gid)))
+        self._n[gid.value] = g.n
         return gid.value
 
-    def submit(self, graph_id: int, kind: int, num: int = 1, den: int = 10) -> int:
+    def submit(self, graph_id: int, kind: int, num: int = 1, den: int = 10, want_array: bool = False) -> int:
+        """Queues a request. want_array: also return the vertex array (removed_round of a peel, core numbers of a
+        core decomposition) in the result."""
         t = C.c_uint64(0)
-        _check(lib().ga_server_submit(self._h, graph_id, kind, num, den, C.byref(t)))
+        if want_array and kind != REQ_TC:
+            n = self._n[graph_id]
+            buf = np.full(max(n, 1), 0xFFFFFFFF, np.uint32)
+            _check(lib().ga_server_submit_out(self._h, graph_id, kind, num, den, _ptr(buf), buf.size, C.byref(t)))
+            self._arrays[t.value] = (kind, buf, n)     # kept alive until the result is collected
+        else:
+            _check(lib().ga_server_submit(self._h, graph_id, kind, num, den, C.byref(t)))
         return t.value
+
+    def _result(self, ticket: int, r: _RequestResult) -> RequestResult:
+        res = _request_result(r)
+        kind_buf = self._arrays.pop(ticket, None)
+        if kind_buf is not None:
+            kind, buf, n = kind_buf
+            if kind == REQ_PEEL:
+                res.peel.removed_round = buf[:n]
+            else:
+                res.core_numbers = buf[:n]
+        return res
 
     def poll(self, ticket: int) -> RequestResult | None:
         r = _RequestResult()
@@ -829,12 +891,12 @@ class Server:
         if st == GA_ERR_NOT_READY:
             return None
         _check(st)
-        return _request_result(r)
+        return self._result(ticket, r)
 
     def wait(self, ticket: int) -> RequestResult:
         r = _RequestResult()
         _check(lib().ga_server_wait(self._h, ticket, C.byref(r)))
-        return _request_result(r)
+        return self._result(ticket, r)
 
     def stats(self) -> dict:
         st = _ServerStats()

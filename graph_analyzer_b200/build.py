@@ -23,6 +23,9 @@ CLI_DIR = os.path.join(PKG, "cli")
 CLIS = ["ga_tc", "ga_densest", "ga_dsg"]
 BUILD_DIR = os.path.join(ROOT, "_build")
 LIB = os.path.join(OUT_DIR, "libga_b200.so")
+# the generators alone (no CUDA): for processes that must not load libga_b200 (bench.py's reference arm)
+GEN_LIB = os.path.join(OUT_DIR, "libga_gen.so")
+GEN_SOURCES = [os.path.join(CSRC, "ga_gen.cpp"), os.path.join(CSRC, "standalone", "ga_gen_errors.cpp")]
 INCLUDE = os.path.join(ROOT, "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -70,8 +73,18 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
         cmd = [_nvcc(), "-shared", *ARCH, "-o", LIB, *objs, "-cudart", "static", "-Xcompiler", "-fopenmp",
                "-lgomp"]
         subprocess.check_call(cmd)
+    build_gen(force)
     build_cli(force)
     return LIB
+
+
+def build_gen(force: bool = False) -> str:
+    """libga_gen.so: the seeded R-MAT sampler and id permutation of ga_gen.cpp, host C++ only."""
+    deps = GEN_SOURCES + [__file__, os.path.join(CSRC, "ga_internal.h"), os.path.join(INCLUDE, "graph_analyzer_b200.h")]
+    if force or not os.path.exists(GEN_LIB) or any(os.path.getmtime(d) > os.path.getmtime(GEN_LIB) for d in deps):
+        subprocess.check_call(["g++", "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-I", INCLUDE, "-I", CSRC,
+                               *GEN_SOURCES, "-o", GEN_LIB])
+    return GEN_LIB
 
 
 def build_cli(force: bool = False) -> list[str]:

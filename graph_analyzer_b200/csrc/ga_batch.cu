@@ -160,6 +160,11 @@ ga_status ga_batch_device_bytes(const ga_batch* b, uint64_t* bytes) {
     return ga_graph_device_bytes(b->g, bytes);
 }
 
+ga_status ga_batch_tuning(ga_batch* b, ga_tuning* out) {
+    if (!b) return fail(GA_ERR_INVALID_ARGUMENT, "null batch");
+    return ga_graph_tuning(b->g, out);
+}
+
 ga_status ga_batch_tc(ga_batch* b, uint64_t* triangles) {
     if (!b || !triangles) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
     GA_GRAPH_LOCK(b->g);

@@ -99,8 +99,16 @@ struct ga_graph {
     uint32_t* in_src = nullptr;   // m: source u of the in-edge
     uint32_t* in_eid = nullptr;   // m: index of the edge u->v in col
 
+    // the oriented CSR again with every row ordered by (degree, id) - the orientation order - instead of by id: for
+    // an in-edge u->v, only the out-neighbours of u after v in this order can close a triangle u->v->x, so the count
+    // kernels probe that suffix of u's row alone
+    uint32_t* colk = nullptr;     // m (+4 zero padding, 16-byte aligned like col)
+    uint32_t* origk = nullptr;    // m: position in col of colk[e]
+    uint32_t* in_posk = nullptr;  // m: position in colk of in-edge k's edge u->v (aligned with in_src / in_eid)
+
     ga_items light, heavy;        // degree-binned work lists of the hash-probe kernel
-    bool prepared = false;
+    bool index_ready = false;     // src, in-lists, colk / origk / in_posk built
+    bool prepared = false;        // ... and the work items for the current light_max_deg / item_work
     ga_loops* loops = nullptr;    // peeling / core loop state, allocated on first use
     // a batch: the graph is the disjoint union of seg_count graphs, graph s owning vertices [seg_off[s], seg_off[s+1])
     const unsigned long long* seg_off = nullptr;
@@ -115,7 +123,9 @@ struct ga_graph {
     int64_t opt_tc_kernel = 0, opt_loop_mode = 0, opt_max_rounds = 0, opt_update_mode = 0;
     int tuned_kernel = 0;          // count kernel chosen by the autotuner (1 plain, 2 hash; 0 not tuned yet)
     uint64_t tune_key = 0;         // degree-distribution signature it was chosen for
+    float tune_ms = 0;             // the chosen configuration's count time when it was measured (0: from the cache)
     uint32_t item_work = 4096, heavy_bits_cap = 0, light_max_deg = 128;
+    bool item_work_set = false, light_max_deg_set = false;   // set by the caller: the autotuner leaves them
 
     // every device allocation, freed by ga_graph_destroy
     std::vector<std::pair<void*, size_t>> allocations;
@@ -168,7 +178,7 @@ ga_status use_device(const ga_graph* g);
 // Frees the loop state (CUDA graphs, pinned buffers) of g.
 void destroy_loops(ga_graph* g);
 
-// Builds src, in-lists and work lists (idempotent).
+// Builds src, in-lists, the (degree, id)-ordered rows (once) and the work lists for the current options (idempotent).
 ga_status prepare(ga_graph* g);
 
 // Picks the count kernel for GA_OPT_TC_KERNEL = 0 from the graph's degree-distribution signature (cached per

@@ -3,6 +3,8 @@
 // Derived structures (built once per handle, on the device, kept resident):
 //   src[m]                 row owner of every edge (the reference builds it on the host, graph.h:64)
 //   in_ptr/in_src/in_eid   transpose of the oriented CSR: for every vertex v the edges u->v (source, edge index)
+//   colk/origk/in_posk     every row again in (degree, id) order, where each entry sits in it, and where each
+//                          in-edge u->v sits in u's reordered row (the start of its probe suffix)
 //   light / heavy items    degree-binned work lists of the hash-probe kernels: one item = a slice of v's in-edges
 //                          whose probe work (sum of out-degrees of the sources) is bounded; anchors with a large
 //                          out-degree go to the block-wide "heavy" bin, the rest to the per-warp "light" bin.
@@ -168,17 +170,71 @@ __global__ void k_in_scatter(const uint32_t* __restrict__ rowptr, const uint32_t
     if (bad) atomicOr(err, (unsigned long long)bad);
 }
 
-// work[k] = out-degree of the source of in-edge k (probe length of that in-edge).
-__global__ void k_in_work(const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ in_src, uint32_t m,
-                          unsigned long long* __restrict__ work) {
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
-        const uint32_t u = in_src[k];
-        work[k] = rowptr[u + 1] - rowptr[u];
+// key[e] = (degree << 32) | id of the endpoint col[e], degree = out + in: the orientation order of graph.h:43-45.
+__global__ void k_edge_keys(const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ col,
+                            const uint32_t* __restrict__ in_ptr, uint32_t m, unsigned long long* __restrict__ key) {
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
+        const uint32_t x = col[e];
+        const uint32_t deg = rowptr[x + 1] - rowptr[x] + in_ptr[x + 1] - in_ptr[x];
+        key[e] = ((unsigned long long)deg << 32) | x;
     }
 }
 
-// Items per anchor. prefix = inclusive scan of work over in-edges. An anchor with out-degree 0 or no in-edge has no
-// item; otherwise ceil(work / target) items (at least 1, at most one per in-edge), light or heavy by its out-degree
+constexpr int kOrderWarps = 4, kOrderStage = 1024;   // rows up to kOrderStage entries stage their keys in smem
+
+// One warp per row: every entry's place in the row's (degree, id) order is the number of entries with a smaller key
+// (keys are distinct), counted against the row's keys in shared memory (read by all lanes at once) or, for rows
+// longer than kOrderStage, in global memory. Writes colk/origk at that place and posk[e] = where entry e went.
+__global__ void __launch_bounds__(kOrderWarps * 32) k_order_rows(const uint32_t* __restrict__ rowptr,
+                                                                 const uint32_t* __restrict__ col,
+                                                                 const unsigned long long* __restrict__ key,
+                                                                 uint32_t n, uint32_t* __restrict__ colk,
+                                                                 uint32_t* __restrict__ origk,
+                                                                 uint32_t* __restrict__ posk) {
+    __shared__ unsigned long long s_key[kOrderWarps][kOrderStage];
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long* sk = s_key[w];
+    for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += nwarps) {
+        const uint32_t b = rowptr[u], d = rowptr[u + 1] - b;
+        if (d == 0) continue;
+        const bool staged = d <= kOrderStage;
+        if (staged) {
+            for (uint32_t i = lane; i < d; i += 32) sk[i] = key[b + i];
+            __syncwarp();
+        }
+        const unsigned long long* kr = staged ? sk : key + b;
+        for (uint32_t i = lane; i < d; i += 32) {
+            const unsigned long long ki = kr[i];
+            uint32_t r = 0;
+            for (uint32_t j = 0; j < d; j++) r += kr[j] < ki;
+            colk[b + r] = col[b + i];
+            origk[b + r] = b + i;
+            posk[b + i] = b + r;
+        }
+        __syncwarp();
+    }
+}
+
+// in_posk[k] = position in colk of in-edge k's edge (its position in col is in_eid[k]).
+__global__ void k_in_posk(const uint32_t* __restrict__ in_eid, const uint32_t* __restrict__ posk, uint32_t m,
+                          uint32_t* __restrict__ in_posk) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x)
+        in_posk[k] = posk[in_eid[k]];
+}
+
+// work[k] = probe length of in-edge k (u->v): the entries of u's (degree, id)-ordered row after v.
+__global__ void k_in_work(const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ in_src,
+                          const uint32_t* __restrict__ in_posk, uint32_t m, unsigned long long* __restrict__ work) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        const uint32_t u = in_src[k];
+        work[k] = rowptr[u + 1] - in_posk[k] - 1;
+    }
+}
+
+// Items per anchor. prefix = inclusive scan of work over in-edges. An anchor with out-degree 0, no in-edge or no
+// probe work has no item; otherwise ceil(work / target) items (at most one per in-edge), light or heavy by its
+// out-degree
 // (heavy items are `heavy_factor` times larger: the block-wide table is built once per item).
 __global__ void k_count_items(const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ in_ptr,
                               const unsigned long long* __restrict__ prefix, uint32_t n, uint32_t light_max_deg,
@@ -193,7 +249,7 @@ __global__ void k_count_items(const uint32_t* __restrict__ rowptr, const uint32_
         if (dv > 0 && e > b) {
             const unsigned long long w = prefix[e - 1] - (b ? prefix[b - 1] : 0ull);
             const unsigned long long t = heavy ? heavy_target : target;
-            c = (uint32_t)max(1ull, (w + t - 1) / t);
+            c = (uint32_t)((w + t - 1) / t);   // no item when no in-edge has anything to probe
             if (c > e - b) c = e - b;
         }
         cnt_light[v] = heavy ? 0 : c;
@@ -346,17 +402,25 @@ static ga_status build_items(ga_graph* g, const unsigned long long* prefix, uint
     return GA_OK;
 }
 
-ga_status prepare(ga_graph* g) {
-    if (g->prepared) return GA_OK;
-    GA_TRY(use_device(g));
+// The derived index (built once per handle): src, the in-lists, the (degree, id)-ordered rows and their in-edge
+// positions; checks the orientation on the way.
+static ga_status prepare_index(ga_graph* g) {
+    if (g->index_ready) return GA_OK;
     cudaStream_t st = g->stream;
     const uint32_t n = g->n, m = g->m;
     GA_CUDA(cudaStreamSynchronize(st));
-    for (uint32_t** p : {&g->src, &g->in_ptr, &g->in_src, &g->in_eid}) { dfree(g, *p); *p = nullptr; }
+    for (uint32_t** p : {&g->src, &g->in_ptr, &g->in_src, &g->in_eid, &g->colk, &g->origk, &g->in_posk}) {
+        dfree(g, *p);
+        *p = nullptr;
+    }
     GA_TRY(dalloc(g, &g->src, m));
     GA_TRY(dalloc(g, &g->in_ptr, (size_t)n + 1));
     GA_TRY(dalloc(g, &g->in_src, m));
     GA_TRY(dalloc(g, &g->in_eid, m));
+    GA_TRY(dalloc(g, &g->colk, (size_t)m + 4));   // padded like col: quad loads of the last row stay inside
+    GA_TRY(dalloc(g, &g->origk, m));
+    GA_TRY(dalloc(g, &g->in_posk, m));
+    GA_CUDA(cudaMemsetAsync(g->colk + m, 0, 16, st));
     uint32_t *indeg = nullptr, *fill = nullptr;
     GA_CUDA(pool_malloc((void**)&indeg, ((size_t)n + 1) * 4, st));
     GA_CUDA(pool_malloc((void**)&fill, ((size_t)n + 1) * 4, st));
@@ -373,12 +437,40 @@ ga_status prepare(ga_graph* g) {
     if (m) {
         k_in_scatter<<<ge, 256, 0, st>>>(g->rowptr, g->col, g->src, g->in_ptr, m, fill, g->in_src, g->in_eid, err);
         GA_CUDA(cudaGetLastError());
+        // rows in (degree, id) order, from one 64-bit key per edge
+        unsigned long long* key = nullptr;
+        uint32_t* posk = nullptr;
+        GA_CUDA(pool_malloc((void**)&key, (size_t)m * 8, st));
+        GA_CUDA(pool_malloc((void**)&posk, (size_t)m * 4, st));
+        k_edge_keys<<<ge, 256, 0, st>>>(g->rowptr, g->col, g->in_ptr, m, key);
+        k_order_rows<<<grid_for((uint64_t)n * 32, kOrderWarps * 32), kOrderWarps * 32, 0, st>>>(
+            g->rowptr, g->col, key, n, g->colk, g->origk, posk);
+        k_in_posk<<<ge, 256, 0, st>>>(g->in_eid, posk, m, g->in_posk);
+        GA_CUDA(cudaGetLastError());
+        cudaFreeAsync(key, st);
+        cudaFreeAsync(posk, st);
     }
-    // work prefix over in-edges (64-bit: the total probe count can exceed 2^32)
+    cudaFreeAsync(indeg, st);
+    cudaFreeAsync(fill, st);
+    unsigned long long herr = 0;
+    GA_CUDA(cudaMemcpyAsync(&herr, err, 8, cudaMemcpyDeviceToHost, st));
+    GA_CUDA(cudaStreamSynchronize(st));
+    if (herr & 16)
+        return fail(GA_ERR_INVALID_GRAPH, "CSR is not oriented by (degree, id) (graph.h:43-45): an edge points from "
+                                          "the larger to the smaller endpoint, or an undirected edge is stored twice");
+    g->index_ready = true;
+    return GA_OK;
+}
+
+// The work items of the hash kernel for the current light_max_deg / item_work (rebuilt when those change, e.g. by
+// the autotuner trying candidates): the probe work of every in-edge, its prefix, the items cut from it.
+static ga_status prepare_items(ga_graph* g) {
+    cudaStream_t st = g->stream;
+    const uint32_t n = g->n, m = g->m;
     unsigned long long* prefix = nullptr;
     GA_CUDA(pool_malloc((void**)&prefix, ((size_t)m + 1) * 8, st));
-    if (m) {
-        k_in_work<<<ge, 256, 0, st>>>(g->rowptr, g->in_src, m, prefix);
+    if (m) {   // work prefix over in-edges (64-bit: the total probe count can exceed 2^32)
+        k_in_work<<<grid_for(m, 256), 256, 0, st>>>(g->rowptr, g->in_src, g->in_posk, m, prefix);
         GA_CUDA(cudaGetLastError());
         GA_TRY(scan_impl<unsigned long long>(st, prefix, prefix, m, true));
     }
@@ -394,17 +486,15 @@ ga_status prepare(ga_graph* g) {
     cudaFreeAsync(cnt_h, st);
     cudaFreeAsync(off_l, st);
     cudaFreeAsync(off_h, st);
-    cudaFreeAsync(indeg, st);
-    cudaFreeAsync(fill, st);
-    GA_TRY(s);
-    unsigned long long herr = 0;
-    GA_CUDA(cudaMemcpyAsync(&herr, err, 8, cudaMemcpyDeviceToHost, st));
-    GA_CUDA(cudaStreamSynchronize(st));
-    if (herr & 16)
-        return fail(GA_ERR_INVALID_GRAPH, "CSR is not oriented by (degree, id) (graph.h:43-45): an edge points from "
-                                          "the larger to the smaller endpoint, or an undirected edge is stored twice");
+    return s;
+}
+
+ga_status prepare(ga_graph* g) {
+    if (g->prepared) return GA_OK;
+    GA_TRY(use_device(g));
+    GA_TRY(prepare_index(g));
+    GA_TRY(prepare_items(g));
     g->prepared = true;
-    g->tuned_kernel = 0;   // work lists changed: decide the kernel again (cached per signature)
     return GA_OK;
 }
 
@@ -584,9 +674,11 @@ ga_status ga_graph_set_option(ga_graph* g, ga_option opt, int64_t value) {
                 g->opt_update_mode = value;
             }
             return GA_OK;
-        case GA_OPT_ITEM_WORK: {
+        case GA_OPT_ITEM_WORK: {   // 0: the autotuner's choice (4096 until it has run)
             const uint32_t v = value ? (uint32_t)std::min<int64_t>(value, 1 << 30) : 4096;
+            g->item_work_set = value != 0;
             if (v != g->item_work) { g->item_work = v; g->prepared = false; }
+            g->tuned_kernel = 0;
             return GA_OK;
         }
         case GA_OPT_HEAVY_TABLE_BITS:
@@ -594,9 +686,11 @@ ga_status ga_graph_set_option(ga_graph* g, ga_option opt, int64_t value) {
                 return fail(GA_ERR_INVALID_ARGUMENT, "GA_OPT_HEAVY_TABLE_BITS is 0 or 3..13");
             g->heavy_bits_cap = (uint32_t)value;
             return GA_OK;
-        case GA_OPT_LIGHT_MAX_DEG: {
+        case GA_OPT_LIGHT_MAX_DEG: {   // 0: the autotuner's choice (128 until it has run)
             const uint32_t v = value ? (uint32_t)std::min<int64_t>(value, 256) : 128;
+            g->light_max_deg_set = value != 0;
             if (v != g->light_max_deg) { g->light_max_deg = v; g->prepared = false; }
+            g->tuned_kernel = 0;
             return GA_OK;
         }
     }

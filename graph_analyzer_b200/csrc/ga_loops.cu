@@ -24,6 +24,18 @@
 // the round is the body of a CUDA graph conditional WHILE node (cudaGraphSetConditional from the tail), so the
 // whole loop is one graph launch; mode 1 launches the same kernels round by round and reads the 100-byte round state
 // back after each (the reference's host loop with its one sync per round).
+//
+// Small core rounds: most of the thousands of core rounds of a power-law graph are small (R-MAT scale 22: 9,543
+// rounds, two thirds with at most 32K alive vertices, the median destroying some 20K incidence entries), and a grid
+// round of three dependent kernels costs tens of microseconds of launch and drain latency whatever its size. In graph
+// mode the core round's body therefore starts with k_core_small_rounds, ONE thread block cluster (16 CTAs of 1,024
+// threads, 8 where 16 cannot be co-scheduled) that runs consecutive rounds itself - minimum, frontier, update, close -
+// with cluster barriers between the phases instead of kernel boundaries, for as long as the alive list is at most
+// kSmallAlive and the next round destroys at most kSmallWork incidence entries. The first round that does not fit
+// is left untouched for the grid kernels that follow in the same body; the loop decisions and every result are the
+// grid round's, so the output is unchanged.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 
 #include "ga_device.cuh"
@@ -260,6 +272,7 @@ __global__ void __launch_bounds__(256) k_core_min(LoopScalars* sc, const uint32_
                                                   const uint32_t* alive0, const uint32_t* alive1,
                                                   uint8_t* __restrict__ state, const uint32_t* fr0,
                                                   const uint32_t* fr1) {
+    if (!sc->cont) return;   // the small-round cluster kernel ended the loop in this body
     const uint32_t p = sc->parity;
     retire_previous(sc, state, (sc->round & 1) ? fr0 : fr1);
     const uint32_t* in = p ? alive1 : alive0;
@@ -280,6 +293,7 @@ __global__ void __launch_bounds__(256) k_core_mark(LoopScalars* sc, const uint32
                                                    uint32_t* __restrict__ item_c, const uint32_t* __restrict__ rowptr,
                                                    const uint32_t* __restrict__ in_ptr,
                                                    const unsigned long long* __restrict__ inc_ptr) {
+    if (!sc->cont) return;
     const uint32_t p = sc->parity;
     uint32_t* frontier = (sc->round & 1) ? fr1 : fr0;
     const uint32_t* in = p ? alive1 : alive0;
@@ -410,6 +424,7 @@ __global__ void __launch_bounds__(kUpdWarps * 32) k_frontier_update(
     const uint32_t* __restrict__ item_c, const uint8_t* __restrict__ state, uint32_t* __restrict__ tri, Segs sg,
     int kind, cudaGraphConditionalHandle handle, int use_handle) {
     constexpr uint32_t kSlots = 2 * kChunk;   // 512 slots, load <= 1/2
+    if (!sc->cont) return;
     count_iteration(sc, handle, use_handle);
     constexpr uint32_t kBits = 9;
     __shared__ uint32_t s_key[kUpdWarps][kSlots];
@@ -522,6 +537,7 @@ __global__ void __launch_bounds__(256) k_frontier_update_list(LoopScalars* sc, c
                                                               uint32_t* __restrict__ tri, Segs sg, int kind,
                                                               cudaGraphConditionalHandle handle, int use_handle) {
     __shared__ unsigned long long s_red[8];
+    if (!sc->cont) return;
     count_iteration(sc, handle, use_handle);
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t nitems = sc->nitems;
@@ -555,6 +571,209 @@ __global__ void __launch_bounds__(256) k_frontier_update_list(LoopScalars* sc, c
         if (t) atomicAdd(&sc->destroyed, t);
     }
     close_round_if_last(sc, kind, handle, use_handle, sg);
+}
+
+// ---- small core rounds in one thread block cluster ----------------------------------------------------------------
+constexpr uint32_t kSmallThreads = 1024;     // threads per CTA of the cluster
+constexpr uint32_t kSmallAlive = 1u << 16;   // alive vertices up to which a round may run in the cluster
+constexpr uint32_t kSmallWork = 1u << 17;    // incidence entries a round may destroy in the cluster
+constexpr uint32_t kSmallChunk = 64;         // incidence entries per update item of the cluster
+
+// Cluster-wide sum / minimum of one value per thread: the CTA reduces through its warps into its own `slot`, and after
+// the cluster barrier every thread combines the slots of all CTAs (distributed shared memory reads).
+template <class T, bool MIN>
+__device__ __forceinline__ T cluster_reduce(cooperative_groups::cluster_group& cluster, T x, T* warp_part, T* slot) {
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const T y = __shfl_xor_sync(GA_FULL_MASK, x, o);
+        x = MIN ? (y < x ? y : x) : x + y;
+    }
+    if (lane == 0) warp_part[w] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        T t = warp_part[0];
+        for (uint32_t i = 1; i < blockDim.x / 32; i++) t = MIN ? (warp_part[i] < t ? warp_part[i] : t) : t + warp_part[i];
+        *slot = t;
+    }
+    cluster.sync();
+    T r = *cluster.map_shared_rank(slot, 0);
+    for (uint32_t c = 1; c < cluster.num_blocks(); c++) {
+        const T y = *cluster.map_shared_rank(slot, c);
+        r = MIN ? (y < r ? y : r) : r + y;
+    }
+    return r;
+}
+
+// Runs consecutive core rounds (the three grid kernels' work: k_core_min, k_core_mark, k_frontier_update_list and
+// close_round_if_last for LOOP_CORE) inside one cluster while the alive list has at most kSmallAlive vertices and
+// a round destroys at most kSmallWork incidence entries; returns at the first round that is larger (untouched, for
+// the grid kernels), when the loop ends (the WHILE condition is set to 0) or on a device check failure. Every
+// decision to leave is made from values all threads read after the same cluster barrier, so the cluster leaves
+// together. Mutable arrays are read with ld.global.cg (L2): other CTAs of the cluster write them between phases.
+__global__ void __launch_bounds__(kSmallThreads, 1) k_core_small_rounds(
+    LoopScalars* sc, uint32_t* __restrict__ tri, uint8_t* __restrict__ state, uint32_t* __restrict__ core,
+    uint32_t* alive0, uint32_t* alive1, uint32_t* fr0, uint32_t* fr1, uint32_t* __restrict__ item_x,
+    uint32_t* __restrict__ item_c, const uint2* __restrict__ inc, const unsigned long long* __restrict__ inc_ptr,
+    cudaGraphConditionalHandle handle) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    __shared__ uint32_t s_wu[32];
+    __shared__ unsigned long long s_wl[32];
+    __shared__ uint32_t s_min;
+    __shared__ unsigned long long s_work, s_des;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t tid = cluster.block_rank() * blockDim.x + threadIdx.x;
+    const uint32_t nthr = cluster.num_blocks() * blockDim.x;
+    const uint32_t gwarp = tid >> 5, nwarps = nthr >> 5;
+    volatile LoopScalars* vs = sc;
+    for (;;) {
+        // the round state, written by the previous close (or the grid kernels before this launch)
+        const uint32_t cont = vs->cont, p = vs->parity, round = vs->round, fprev = vs->fprev;
+        const uint32_t na = vs->alive_count[p], kcur = vs->kcur;
+        if (!cont || na > kSmallAlive) break;
+        uint32_t* in = p ? alive1 : alive0;
+        uint32_t* outl = p ? alive0 : alive1;
+        uint32_t* frontier = (round & 1) ? fr1 : fr0;
+        const uint32_t* prev = (round & 1) ? fr0 : fr1;
+        // retire the previous round's frontier (the grid kernels do it again if they take this round: idempotent)
+        for (uint32_t i = tid; i < fprev; i += nthr) state[__ldcg(prev + i)] = 0;
+        // k = max(k, min over alive of tri)
+        uint32_t mn = 0xFFFFFFFFu;
+        for (uint32_t i = tid; i < na; i += nthr) mn = min(mn, __ldcg(tri + __ldcg(in + i)));
+        mn = cluster_reduce<uint32_t, true>(cluster, mn, s_wu, &s_min);
+        const uint32_t k = max(kcur, mn);
+        // the round's size: incidence entries of the frontier {alive v : tri[v] <= k}
+        unsigned long long work = 0;
+        for (uint32_t i = tid; i < na; i += nthr) {
+            const uint32_t v = __ldcg(in + i);
+            if (__ldcg(tri + v) <= k) work += inc_ptr[v + 1] - inc_ptr[v];
+        }
+        work = cluster_reduce<unsigned long long, false>(cluster, work, s_wl, &s_work);
+        if (work > kSmallWork) break;   // the grid kernels take this round
+        // frontier and survivors (k_core_mark), with update items of kSmallChunk entries
+        for (uint32_t i0 = tid - lane; i0 < na; i0 += nthr) {
+            const uint32_t i = i0 + lane;
+            const bool valid = i < na;
+            const uint32_t v = valid ? __ldcg(in + i) : 0;
+            const bool rem = valid && __ldcg(tri + v) <= k;
+            if (rem) {
+                state[v] = 2;
+                core[v] = k;
+            }
+            uint32_t bal = __ballot_sync(GA_FULL_MASK, rem);
+            if (bal) {
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(&sc->fcount, (uint32_t)__popc(bal));
+                base = __shfl_sync(GA_FULL_MASK, base, 0);
+                const uint32_t nc = rem ? (uint32_t)((inc_ptr[v + 1] - inc_ptr[v] + kSmallChunk - 1) / kSmallChunk) : 0;
+                if (rem) frontier[base + __popc(bal & ((1u << lane) - 1))] = v;
+                const uint32_t incl = warp_incl_scan(nc, lane);
+                const uint32_t tot = __shfl_sync(GA_FULL_MASK, incl, 31);
+                uint32_t ib = 0;
+                if (lane == 31 && tot) ib = atomicAdd(&sc->nitems, tot);
+                ib = __shfl_sync(GA_FULL_MASK, ib, 31);
+                for (uint32_t c = 0; c < nc; c++) {
+                    item_x[ib + incl - nc + c] = v;
+                    item_c[ib + incl - nc + c] = c;
+                }
+            }
+            const bool keep = valid && !rem;
+            bal = __ballot_sync(GA_FULL_MASK, keep);
+            if (bal) {
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(&sc->alive_count[p ^ 1], (uint32_t)__popc(bal));
+                base = __shfl_sync(GA_FULL_MASK, base, 0);
+                if (keep) outl[base + __popc(bal & ((1u << lane) - 1))] = v;
+            }
+        }
+        __threadfence();
+        cluster.sync();
+        // update (k_frontier_update_list): each destroyed triangle once, by its smallest-id frontier corner
+        const uint32_t nitems = vs->nitems, F = vs->fcount;
+        unsigned long long destroyed = 0;
+        for (uint32_t it = gwarp; it < nitems; it += nwarps) {
+            const uint32_t x = __ldcg(item_x + it);
+            const unsigned long long b = inc_ptr[x] + (unsigned long long)__ldcg(item_c + it) * kSmallChunk;
+            const unsigned long long e = min(inc_ptr[x + 1], b + kSmallChunk);
+            for (unsigned long long i = b + lane; i < e; i += 32) {
+                const uint2 yw = inc[i];
+                const uint8_t sy = __ldcg(state + yw.x), sw = __ldcg(state + yw.y);
+                if (!sy || !sw) continue;
+                if ((sy == 2 && yw.x < x) || (sw == 2 && yw.y < x)) continue;
+                destroyed++;
+                if (sy == 1) atomicSub(&tri[yw.x], 1u);
+                if (sw == 1) atomicSub(&tri[yw.y], 1u);
+            }
+        }
+        destroyed = cluster_reduce<unsigned long long, false>(cluster, destroyed, s_wl, &s_des);
+        // close (close_round_if_last for LOOP_CORE, one thread)
+        if (tid == 0) {
+            uint32_t status = vs->status;
+            unsigned long long nalive = vs->nalive, T = vs->T;
+            if (F == 0 && nalive > 0) status = LS_NO_PROGRESS;
+            if (F > nalive) status = LS_OVER_REMOVED;
+            if (destroyed > T) status = LS_OVER_REMOVED;
+            if (k < kcur) status = LS_LEVEL_DOWN;
+            nalive -= min((unsigned long long)F, nalive);
+            T -= min(destroyed, T);
+            const uint32_t iters = vs->iters + 1, max_rounds = vs->max_rounds;
+            vs->nalive = nalive;
+            vs->T = T;
+            vs->kcur = k;
+            vs->kround = k;
+            vs->round = round + 1;
+            vs->parity = p ^ 1;
+            vs->alive_count[p] = 0;   // the list this round read is the next round's output
+            vs->fprev = F;
+            vs->fcount = 0;
+            vs->nitems = 0;
+            vs->destroyed = 0;
+            vs->done_blocks = 0;
+            vs->min_tri = 0xFFFFFFFFu;
+            vs->iters = iters;
+            if (iters > max_rounds + 1) status = LS_ROUND_LIMIT;   // count_iteration's bound
+            if (status == LS_OK && nalive > 0 && round + 1 >= max_rounds) status = LS_ROUND_LIMIT;
+            vs->status = status;
+            const uint32_t c = (status == LS_OK && nalive > 0 && iters <= max_rounds) ? 1u : 0u;
+            vs->cont = c;
+            if (!c) cudaGraphSetConditional(handle, 0);
+            __threadfence();
+        }
+        cluster.sync();
+    }
+    cluster.sync();   // no CTA leaves while another may still read its shared memory
+}
+
+// Cluster size for k_core_small_rounds: 16 CTAs where 16 can be co-scheduled, else 8 (0: neither).
+static int small_round_cluster(int device) {
+    static int cached[64] = {};
+    static std::mutex mu;
+    if (device < 0 || device >= 64) return 0;
+    std::lock_guard<std::mutex> lock(mu);
+    if (cached[device]) return cached[device] > 0 ? cached[device] : 0;
+    int best = -1;
+    cudaFuncSetAttribute(k_core_small_rounds, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    for (int c : {16, 8}) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = c;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(c);
+        cfg.blockDim = dim3(kSmallThreads);
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, k_core_small_rounds, &cfg) == cudaSuccess && clusters > 0) {
+            best = c;
+            break;
+        }
+    }
+    (void)cudaGetLastError();
+    cached[device] = best;
+    return best > 0 ? best : 0;
 }
 
 // Per graph: T0 = (sum of its vertices' triangle counts) / 3. One block per graph.
@@ -684,7 +903,8 @@ static ga_status build_lists(ga_graph* g, uint64_t T0) {
     cudaStream_t st = g->stream;
     const uint32_t n = g->n;
     const uint64_t entries = 3 * T0;
-    const uint64_t need_items = (uint64_t)n + entries / kListChunk + 1;
+    // the grid rounds' items (kListChunk entries) and a cluster round's (kSmallChunk entries, at most kSmallWork)
+    const uint64_t need_items = (uint64_t)n + std::max<uint64_t>(entries / kListChunk, kSmallWork / kSmallChunk) + 1;
     ga_status s = dalloc(g, &L->inc_ptr, (size_t)n + 1);
     if (s == GA_OK) s = dalloc(g, &L->inc, entries ? entries : 1);
     uint32_t *ix = nullptr, *ic = nullptr;
@@ -742,6 +962,23 @@ static ga_status enqueue_round(ga_graph* g, cudaStream_t st, cudaGraphConditiona
                                                   L->frontier[0], L->frontier[1], L->item_x, L->item_c, g->rowptr,
                                                   g->in_ptr, inc_ptr, sg);
     } else {
+        const int csize = use_h && L->lists == 1 ? small_round_cluster(g->device) : 0;
+        if (csize) {   // the small rounds first, in one cluster; the grid kernels below take the first large one
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = csize;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3(csize);
+            cfg.blockDim = dim3(kSmallThreads);
+            cfg.stream = st;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            GA_CUDA(cudaLaunchKernelEx(&cfg, k_core_small_rounds, L->sc, L->tri, L->state, L->out, L->alive[0],
+                                       L->alive[1], L->frontier[0], L->frontier[1], L->item_x, L->item_c,
+                                       (const uint2*)L->inc, (const unsigned long long*)L->inc_ptr, h));
+        }
         k_core_min<<<L->grid_scan, 256, 0, st>>>(L->sc, L->tri, L->alive[0], L->alive[1], L->state, L->frontier[0],
                                                  L->frontier[1]);
         k_core_mark<<<L->grid_scan, 256, 0, st>>>(L->sc, L->tri, L->state, L->out, L->alive[0], L->alive[1],
@@ -780,6 +1017,7 @@ static ga_status ensure_graph(ga_graph* g) {
     cudaGraphNode_t node;
     GA_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &params));
     cudaGraph_t body = params.conditional.phGraph_out[0];
+    if (KIND == LOOP_CORE) (void)small_round_cluster(g->device);   // decided before the capture starts
     cudaStream_t cap;
     GA_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     ga_status s = GA_OK;

@@ -53,6 +53,7 @@ struct Request {
     uint64_t gid = 0;
     ga_request_kind kind = GA_REQ_TC;
     uint64_t num = 0, den = 1;
+    uint32_t* out = nullptr;   // caller's host array of n entries: removed_round (peel) or core numbers (core)
     Clock::time_point submitted, started, finished;
     bool done = false;
     ga_request_result result{};
@@ -268,10 +269,10 @@ bool run_single(ga_server* s, cudaStream_t st, Work* w, Request& r, GraphEntry& 
                 rc = ga_tc_count(e.dev, &res.triangles);
                 break;
             case GA_REQ_PEEL:
-                rc = ga_batch_peel(e.dev, r.num, r.den, &res.peel, nullptr);
+                rc = ga_batch_peel(e.dev, r.num, r.den, &res.peel, r.out);
                 break;
             case GA_REQ_CORE:
-                rc = ga_core_decomposition(e.dev, nullptr, &res.core);
+                rc = ga_core_decomposition(e.dev, r.out, &res.core);
                 break;
         }
         // the graph's triangle count, known after its first request
@@ -301,14 +302,21 @@ void run_folded(ga_server* s, cudaStream_t st, std::vector<Request*>& rs, std::v
     std::vector<uint64_t> tri(G, 0);
     std::vector<ga_peel_result> peel(G);
     std::vector<uint32_t> status(G, GA_OK);
+    // removed_round of the whole batch when any folded request asked for its array
+    bool want = false;
+    for (const Request* r : rs) want |= r->out != nullptr;
+    std::vector<uint32_t> removed(want ? voff[G] + 1 : 0);
     ga_batch* b = nullptr;
     ga_status rc = ga_batch_create(G, voff.data(), eoff.data(), rowptr.data(), col.data(), s->cfg.device, st, &b);
     if (rc == GA_OK) {
         if (rs[0]->kind == GA_REQ_TC) rc = ga_batch_tc(b, tri.data());
-        else rc = ga_batch_tc_peel(b, rs[0]->num, rs[0]->den, tri.data(), peel.data(), status.data(), nullptr);
+        else rc = ga_batch_tc_peel(b, rs[0]->num, rs[0]->den, tri.data(), peel.data(), status.data(),
+                                   want ? removed.data() : nullptr);
     }
     if (b) ga_batch_destroy(b);
     for (uint32_t i = 0; i < G; i++) {
+        if (rc == GA_OK && rs[i]->out && rs[0]->kind == GA_REQ_PEEL)
+            std::copy(removed.begin() + voff[i], removed.begin() + voff[i + 1], rs[i]->out);
         ga_request_result& res = rs[i]->result;
         res.folded = G;
         res.resident_hit = 0;
@@ -492,6 +500,11 @@ ga_status ga_server_add_graph(ga_server* s, const uint32_t* rowptr, const uint32
 
 ga_status ga_server_submit(ga_server* s, uint64_t graph_id, ga_request_kind kind, uint64_t num, uint64_t den,
                            uint64_t* ticket) {
+    return ga_server_submit_out(s, graph_id, kind, num, den, nullptr, 0, ticket);
+}
+
+ga_status ga_server_submit_out(ga_server* s, uint64_t graph_id, ga_request_kind kind, uint64_t num, uint64_t den,
+                               uint32_t* out, uint64_t out_len, uint64_t* ticket) {
     if (!s || !ticket) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
     if (kind != GA_REQ_TC && kind != GA_REQ_PEEL && kind != GA_REQ_CORE)
         return fail(GA_ERR_INVALID_ARGUMENT, "unknown request kind");
@@ -499,12 +512,17 @@ ga_status ga_server_submit(ga_server* s, uint64_t graph_id, ga_request_kind kind
         return fail(GA_ERR_INVALID_ARGUMENT, "eps = num/den needs 1 <= den <= 2^20 and num <= 2^20");
     {
         std::lock_guard<std::mutex> lock(s->mu);
-        if (!s->graphs.count(graph_id)) return fail(GA_ERR_INVALID_ARGUMENT, "unknown graph id");
+        auto g = s->graphs.find(graph_id);
+        if (g == s->graphs.end()) return fail(GA_ERR_INVALID_ARGUMENT, "unknown graph id");
+        if (out && kind != GA_REQ_TC && out_len < g->second.n)
+            return fail(GA_ERR_INVALID_ARGUMENT, "out has %llu entries, the graph %u vertices",
+                        (unsigned long long)out_len, g->second.n);
         Request r;
         r.gid = graph_id;
         r.kind = kind;
         r.num = num;
         r.den = den;
+        r.out = kind == GA_REQ_TC ? nullptr : out;
         r.submitted = Clock::now();
         *ticket = s->next_ticket++;
         s->requests.emplace(*ticket, r);

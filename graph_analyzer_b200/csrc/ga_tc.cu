@@ -7,10 +7,12 @@
 //
 //     T = sum over anchors v of sum over in-edges u->v of |N+(u) ∩ N+(v)|
 //
-// N+(v) is loaded ONCE into a shared-memory hash set and every in-neighbour's list N+(u) is streamed past it (probe).
-// Probe work is sum_v sum_{u->v} d+(u) = sum_u d+(u)^2, the smaller of the two sides of the merge sum (the other
-// side, sum_{u->v} d+(v), is about twice as large on power-law graphs), and each probe is one or two shared-memory
-// loads instead of a merge step or a binary search in global memory.
+// N+(v) is loaded ONCE into a shared-memory hash set and the in-neighbours' lists are streamed past it (probe). A
+// common neighbour x of u and v has v->x, so it comes after v in the orientation order; with every row also kept in
+// (degree, id) order (colk, built by ga_graph.cu), the probe list of in-edge u->v is just the part of u's row after
+// v. Probe work is sum_u d+(u)(d+(u)-1)/2, half of sum_u d+(u)^2 and a quarter or less of the merge sum's
+// sum_{u->v} (d+(u) + d+(v)) on power-law graphs, and each probe is one shared-memory load instead of a merge step
+// or a binary search in global memory.
 //
 // Scheduler (degree-binned, one persistent launch):
 //   * work items = slices of an anchor's in-edge list with bounded probe work (built in ga_graph.cu);
@@ -92,12 +94,12 @@ __device__ __forceinline__ void on_hit(const TcArgs<CT>& a, uint32_t* cnt, uint3
         atomicAdd(&cnt[h], 1u);
         atomicAdd(&ecnt[owner], 1u);
     }
-    if (MODE == TC_ESUP) atomicAdd(&a.esup[e], 1u);
+    if (MODE == TC_ESUP) atomicAdd(&a.esup[a.origk[e]], 1u);
     if (MODE == TC_LIST) list_triangle(a, s_u[owner], anchor, x);
 }
 
-// Looks x (at col position e, probe list of in-edge `owner`) up in the hash set or, when `global`, by binary search in
-// the sorted row N+(v) = col[vb, vb + dv). Returns 1 on a hit and books the supports of the found triangle.
+// Looks x (at colk position e, probe list of in-edge `owner`) up in the hash set or, when `global`, by binary search
+// in the id-sorted row N+(v) = col[vb, vb + dv). Returns 1 on a hit and books the supports of the found triangle.
 template <int MODE, bool ALIVE, class CT>
 __device__ __forceinline__ uint32_t probe_one(const uint32_t* __restrict__ col, const TcArgs<CT>& a, uint32_t x,
                                               uint32_t e, uint32_t owner, const uint32_t* key, uint32_t* cnt,
@@ -126,7 +128,7 @@ __device__ __forceinline__ uint32_t probe_one(const uint32_t* __restrict__ col, 
         if (counters(MODE)) atomicAdd(&s_ecnt[owner], 1u);
         if (MODE == TC_VSUP) atomicAdd(&a.vsup[x], (CT)1);
         if (MODE == TC_ESUP) {
-            atomicAdd(&a.esup[e], 1u);
+            atomicAdd(&a.esup[a.origk[e]], 1u);
             atomicAdd(&a.esup[j], 1u);
         }
         if (MODE == TC_LIST) list_triangle(a, s_u[owner], anchor, x);
@@ -135,17 +137,17 @@ __device__ __forceinline__ uint32_t probe_one(const uint32_t* __restrict__ col, 
     return 0;
 }
 
-// Probes one batch of up to 32 in-edges [kb, kend) of anchor v (one warp). Lane l loads the l-th source u; each list
-// N+(u) = col[rb, re) is cut into 16-byte quads (col is 16-byte aligned and padded, so a quad never leaves the
-// allocation), a warp scan of the quad counts flattens the 32 lists into one sequence, and lane p takes quads
-// p, p+32, ...: one 128-bit load, then up to 4 probes of the elements inside [rb, re). Each lane advances its owner
-// index monotonically. Returns this lane's hits.
+// Probes one batch of up to 32 in-edges [kb, kend) of anchor v (one warp). Lane l loads the l-th source u; its probe
+// list, the part of u's (degree, id)-ordered row after v, colk[rb, re), is cut into 16-byte quads (colk is 16-byte
+// aligned and padded, so a quad never leaves the allocation), a warp scan of the quad counts flattens the 32 lists
+// into one sequence, and lane p takes quads p, p+32, ...: one 128-bit load, then up to 4 probes of the elements
+// inside [rb, re). Each lane advances its owner index monotonically. Returns this lane's hits.
 template <int MODE, bool ALIVE, class CT>
 __device__ __forceinline__ unsigned long long probe_batch(
-    const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ col, const uint32_t* __restrict__ in_src,
-    const uint32_t* __restrict__ in_eid, const TcArgs<CT>& a, uint32_t kb, uint32_t kend, const uint32_t* key,
-    uint32_t* cnt, uint32_t bits, bool global, uint32_t vb, uint32_t dv, uint32_t* s_incl, uint32_t* s_rb,
-    uint32_t* s_ecnt, uint32_t lane, uint32_t anchor) {
+    const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ col, const uint32_t* __restrict__ colk,
+    const uint32_t* __restrict__ in_src, const uint32_t* __restrict__ in_eid, const uint32_t* __restrict__ in_posk,
+    const TcArgs<CT>& a, uint32_t kb, uint32_t kend, const uint32_t* key, uint32_t* cnt, uint32_t bits, bool global,
+    uint32_t vb, uint32_t dv, uint32_t* s_incl, uint32_t* s_rb, uint32_t* s_ecnt, uint32_t lane, uint32_t anchor) {
     unsigned long long hits = 0;
     uint32_t* s_re = s_rb + 32;   // the caller's batch area: incl[32], rb[32], re[32], ecnt[32], u[32]
     uint32_t* s_u = s_rb + 96;
@@ -154,7 +156,7 @@ __device__ __forceinline__ unsigned long long probe_batch(
     if (k < kend) {
         u = in_src[k];
         if (!ALIVE || a.alive[u]) {
-            rb = rowptr[u];
+            rb = in_posk[k] + 1;
             re = rowptr[u + 1];
             if (re > rb) nq = ((re + 3) >> 2) - (rb >> 2);
         }
@@ -166,7 +168,7 @@ __device__ __forceinline__ unsigned long long probe_batch(
     s_re[lane] = re;
     if (MODE == TC_LIST) s_u[lane] = u;
     __syncwarp();
-    const uint4* __restrict__ col4 = reinterpret_cast<const uint4*>(col);
+    const uint4* __restrict__ col4 = reinterpret_cast<const uint4*>(colk);
     uint32_t owner = 0;
     for (uint32_t p = lane; p < tot; p += 32) {
         while (s_incl[owner] <= p) owner++;
@@ -251,19 +253,26 @@ __device__ __forceinline__ void flush_table(const TcArgs<CT>& a, uint32_t vb, co
     }
 }
 
+// bounds (optional, device): this launch's item ranges [bounds[0], bounds[1]) of the heavy and [bounds[2], bounds[3])
+// of the light bin (a shard); null means every item.
 template <int MODE, bool ALIVE, class CT>
 __global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const uint32_t* __restrict__ rowptr,
                                                       const uint32_t* __restrict__ col,
+                                                      const uint32_t* __restrict__ colk,
                                                       const uint32_t* __restrict__ in_src,
-                                                      const uint32_t* __restrict__ in_eid, ga_items heavy,
-                                                      ga_items light, uint32_t heavy_bits_max,
-                                                      uint32_t* __restrict__ queue, TcArgs<CT> a) {
+                                                      const uint32_t* __restrict__ in_eid,
+                                                      const uint32_t* __restrict__ in_posk, ga_items heavy,
+                                                      ga_items light, const uint32_t* __restrict__ bounds,
+                                                      uint32_t heavy_bits_max, uint32_t* __restrict__ queue,
+                                                      TcArgs<CT> a) {
     extern __shared__ uint32_t smem[];
     __shared__ uint32_t s_item, s_next;
     __shared__ unsigned long long s_red[kWarps];
     constexpr int W = SlotLayout<MODE>::words;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned long long hits = 0;
+    const uint32_t h0 = bounds ? bounds[0] : 0u, h1 = bounds ? bounds[1] : heavy.count;
+    const uint32_t l0 = bounds ? bounds[2] : 0u, l1 = bounds ? bounds[3] : light.count;
 
     // ---- heavy bin: the block shares one hash set of N+(v) per item; its warps pull 32-in-edge batches from a
     //      shared counter, so no warp waits for another until the item is exhausted ----
@@ -276,10 +285,10 @@ __global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const ui
         uint32_t *s_incl = wbase, *s_rb = wbase + 32, *s_ecnt = wbase + 96;
         s_ecnt[lane] = 0;
         for (;;) {
-            if (threadIdx.x == 0) s_item = atomicAdd(&queue[0], 1u);
+            if (threadIdx.x == 0) s_item = h0 + atomicAdd(&queue[0], 1u);
             __syncthreads();
             const uint32_t item = s_item;
-            if (item >= heavy.count) break;
+            if (item >= h1) break;
             const uint32_t v = heavy.v[item];
             if (ALIVE && !a.alive[v]) {
                 __syncthreads();          // everyone has read s_item before thread 0 overwrites it
@@ -298,8 +307,8 @@ __global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const ui
                 if (lane == 0) kb = atomicAdd(&s_next, 32u);
                 kb = __shfl_sync(GA_FULL_MASK, kb, 0);
                 if (kb >= k1) break;
-                h += probe_batch<MODE, ALIVE, CT>(rowptr, col, in_src, in_eid, a, kb, min(kb + 32, k1), key, cnt,
-                                                  bits, global, vb, dv, s_incl, s_rb, s_ecnt, lane, v);
+                h += probe_batch<MODE, ALIVE, CT>(rowptr, col, colk, in_src, in_eid, in_posk, a, kb, min(kb + 32, k1),
+                                                  key, cnt, bits, global, vb, dv, s_incl, s_rb, s_ecnt, lane, v);
             }
             hits += h;
             if (MODE == TC_VSUP) {
@@ -324,9 +333,9 @@ __global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const ui
         __syncwarp();
         for (;;) {
             uint32_t item = 0;
-            if (lane == 0) item = atomicAdd(&queue[1], 1u);
+            if (lane == 0) item = l0 + atomicAdd(&queue[1], 1u);
             item = __shfl_sync(GA_FULL_MASK, item, 0);
-            if (item >= light.count) break;
+            if (item >= l1) break;
             const uint32_t v = light.v[item];
             if (ALIVE && !a.alive[v]) continue;
             const uint32_t vb = rowptr[v], dv = rowptr[v + 1] - vb;
@@ -338,8 +347,8 @@ __global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const ui
             unsigned long long h = 0;
             const uint32_t k1 = light.k1[item];
             for (uint32_t kb = light.k0[item]; kb < k1; kb += 32)
-                h += probe_batch<MODE, ALIVE, CT>(rowptr, col, in_src, in_eid, a, kb, min(kb + 32, k1), key, cnt,
-                                                  bits, global, vb, dv, s_incl, s_rb, s_ecnt, lane, v);
+                h += probe_batch<MODE, ALIVE, CT>(rowptr, col, colk, in_src, in_eid, in_posk, a, kb, min(kb + 32, k1),
+                                                  key, cnt, bits, global, vb, dv, s_incl, s_rb, s_ecnt, lane, v);
             hits += h;
             if (MODE == TC_VSUP) {
                 const unsigned long long t = warp_sum_u64(h);
@@ -426,8 +435,33 @@ static uint32_t heavy_bits_for(const ga_graph* g, int mode) {
     return std::min(need, cap);
 }
 
+// Item ranges of shard `shard` of `nshards` in both bins (heavy then light, [lo, hi) each, into out[4]): equal parts
+// of each bin's items, every cut moved forward to the next anchor boundary (items are in ascending anchor order), so
+// that an anchor's items all fall into one shard. Items depend only on the graph and the options, not on the order
+// inside an in-list, so every GPU holding the graph cuts the same partition of the anchors - and of the triangles,
+// each counted at its middle vertex.
+__global__ void k_shard_bounds(const uint32_t* __restrict__ hv, uint32_t hcount, const uint32_t* __restrict__ lv,
+                               uint32_t lcount, uint32_t shard, uint32_t nshards, uint32_t* __restrict__ out) {
+    const uint32_t t = threadIdx.x;   // 4 threads: heavy lo, heavy hi, light lo, light hi
+    if (t >= 4) return;
+    const uint32_t* v = t < 2 ? hv : lv;
+    const uint32_t count = t < 2 ? hcount : lcount;
+    const uint32_t part = shard + (t & 1);
+    uint32_t cut = (uint32_t)((uint64_t)count * part / nshards);
+    if (cut > 0 && cut < count) {   // first item after `cut - 1` whose anchor differs: binary search (v ascending)
+        const uint32_t a = v[cut - 1];
+        uint32_t lo = cut, hi = count;
+        while (lo < hi) {
+            const uint32_t mid = lo + ((hi - lo) >> 1);
+            if (v[mid] <= a) lo = mid + 1; else hi = mid;
+        }
+        cut = lo;
+    }
+    out[t] = cut;
+}
+
 template <int MODE, bool ALIVE, class CT>
-static ga_status launch_hash(ga_graph* g, const TcArgs<CT>& a) {
+static ga_status launch_hash(ga_graph* g, const TcArgs<CT>& a0) {
     const uint32_t hb = heavy_bits_for(g, MODE);
     const size_t smem = hash_smem_bytes<MODE>(hb);
     auto kern = k_tc_hash<MODE, ALIVE, CT>;
@@ -435,24 +469,22 @@ static ga_status launch_hash(ga_graph* g, const TcArgs<CT>& a) {
     int occ = 0;
     GA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, smem));
     occ = std::max(occ, 1);
-    ga_items heavy = g->heavy, light = g->light;
-    if (a.nshards > 1) {   // this shard's equal part of each bin's item list (a view: offset pointers)
-        auto cut = [&](ga_items& it) {
-            const uint32_t lo = (uint32_t)((uint64_t)it.count * a.shard / a.nshards);
-            const uint32_t hi = (uint32_t)((uint64_t)it.count * (a.shard + 1) / a.nshards);
-            it.v += lo;
-            it.k0 += lo;
-            it.k1 += lo;
-            it.count = hi - lo;
-        };
-        cut(heavy);
-        cut(light);
+    TcArgs<CT> a = a0;
+    a.origk = g->origk;
+    const uint32_t* bounds = nullptr;
+    uint64_t want = std::max<uint64_t>(g->heavy.count, (g->light.count + kWarps - 1) / kWarps);
+    if (a.nshards > 1) {   // this shard's anchors (cut on the device; the queue counters sit in d_queue[0..1])
+        uint32_t* b = g->d_queue + 4;
+        k_shard_bounds<<<1, 32, 0, g->stream>>>(g->heavy.v, g->heavy.count, g->light.v, g->light.count, a.shard,
+                                                a.nshards, b);
+        GA_CUDA(cudaGetLastError());
+        bounds = b;
+        want = (want + a.nshards - 1) / a.nshards + 1;
     }
-    const uint64_t want = std::max<uint64_t>(heavy.count, (light.count + kWarps - 1) / kWarps);
     const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)g->sm_count * occ, want));
-    GA_CUDA(cudaMemsetAsync(g->d_queue, 0, 8 * sizeof(uint32_t), g->stream));
-    kern<<<grid, kThreads, smem, g->stream>>>(g->rowptr, g->col, g->in_src, g->in_eid, heavy, light, hb, g->d_queue,
-                                              a);
+    GA_CUDA(cudaMemsetAsync(g->d_queue, 0, 4 * sizeof(uint32_t), g->stream));
+    kern<<<grid, kThreads, smem, g->stream>>>(g->rowptr, g->col, g->colk, g->in_src, g->in_eid, g->in_posk, g->heavy,
+                                              g->light, bounds, hb, g->d_queue, a);
     GA_CUDA(cudaGetLastError());
     return GA_OK;
 }
@@ -496,12 +528,16 @@ ga_status run_tc(ga_graph* g, const TcArgs<CT>& a, bool zero_outputs) {
 }
 
 // ---- autotuner ----------------------------------------------------------------------------------------------------
-// The best count kernel depends on the degree distribution: on graphs whose out-lists are all short (Holme-Kim with a
-// handful of edges per vertex) the plain merge wins, on skewed graphs with long lists (R-MAT) the degree-binned hash
-// kernel wins by several times. The choice is cached per degree-distribution signature: log2 of n and m and the
-// fraction of edges whose source has out-degree in each log2 bucket, in sixteenths. A signature seen before is
-// answered from the cache (process-wide; also kept in the file named by GA_TUNE_CACHE when that is set); a new one
-// is decided by timing both kernels once on the graph (their code loaded beforehand).
+// What runs fastest depends on the degree distribution: on graphs whose out-lists are all short (Holme-Kim with a
+// handful of edges per vertex) the plain merge can win, on skewed graphs with long lists (R-MAT) the degree-binned
+// hash kernel wins by several times, and within the hash kernel the bin cutoff between per-warp and block-wide sets
+// (light_max_deg) and the probe work per item (item_work, which sets how many warps share an anchor) move the time
+// by some percent. The choice - kernel, cutoff, item work - is cached per degree-distribution signature: log2 of n
+// and m and the fraction of edges whose source has out-degree in each log2 bucket, in sixteenths. A signature seen
+// before is answered from the cache (process-wide; also kept in the file named by GA_TUNE_CACHE when that is set); a
+// new one is decided by timing candidates on the graph: the hash kernel and the plain kernel at the current options,
+// then the cutoffs {32, 64, 128, 256} and the item works {1024, 4096, 16384} (coordinate-wise; options the caller
+// set explicitly stay as set). Every candidate gives the same count.
 
 __global__ void k_degree_hist(const uint32_t* __restrict__ rowptr, uint32_t n, unsigned long long* hist) {
     __shared__ unsigned long long s_h[33];
@@ -515,8 +551,13 @@ __global__ void k_degree_hist(const uint32_t* __restrict__ rowptr, uint32_t n, u
     if (threadIdx.x < 33 && s_h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], s_h[threadIdx.x]);
 }
 
+struct TuneChoice {
+    int kernel = 2;
+    uint32_t light_max_deg = 128, item_work = 4096;
+};
+
 static std::mutex g_tune_mu;
-static std::map<uint64_t, int> g_tune_cache;
+static std::map<uint64_t, TuneChoice> g_tune_cache;
 static bool g_tune_loaded = false;
 
 static void tune_cache_load_locked() {
@@ -527,19 +568,20 @@ static void tune_cache_load_locked() {
     FILE* f = std::fopen(path, "r");
     if (!f) return;
     unsigned long long key;
-    int kernel;
-    while (std::fscanf(f, "%llx %d", &key, &kernel) == 2)
-        if (kernel == 1 || kernel == 2) g_tune_cache[key] = kernel;
+    TuneChoice c;
+    while (std::fscanf(f, "%llx %d %u %u", &key, &c.kernel, &c.light_max_deg, &c.item_work) == 4)
+        if ((c.kernel == 1 || c.kernel == 2) && c.light_max_deg >= 1 && c.light_max_deg <= 256 && c.item_work >= 1)
+            g_tune_cache[key] = c;
     std::fclose(f);
 }
 
-static void tune_cache_store_locked(uint64_t key, int kernel) {
-    g_tune_cache[key] = kernel;
+static void tune_cache_store_locked(uint64_t key, const TuneChoice& c) {
+    g_tune_cache[key] = c;
     const char* path = std::getenv("GA_TUNE_CACHE");
     if (!path) return;
     FILE* f = std::fopen(path, "a");
     if (!f) return;
-    std::fprintf(f, "%llx %d\n", (unsigned long long)key, kernel);
+    std::fprintf(f, "%llx %d %u %u\n", (unsigned long long)key, c.kernel, c.light_max_deg, c.item_work);
     std::fclose(f);
 }
 
@@ -547,6 +589,18 @@ ga_status ready(ga_graph* g) {
     GA_TRY(prepare(g));
     if (g->opt_tc_kernel == 0) GA_TRY(autotune(g));
     return GA_OK;
+}
+
+// Applies a choice (leaving options the caller set) and rebuilds the work items when the cutoff or item work moved.
+static ga_status apply_choice(ga_graph* g, const TuneChoice& c) {
+    const uint32_t light = g->light_max_deg_set ? g->light_max_deg : c.light_max_deg;
+    const uint32_t work = g->item_work_set ? g->item_work : c.item_work;
+    if (light != g->light_max_deg || work != g->item_work) {
+        g->light_max_deg = light;
+        g->item_work = work;
+        g->prepared = false;
+    }
+    return prepare(g);
 }
 
 ga_status autotune(ga_graph* g) {
@@ -563,7 +617,7 @@ ga_status autotune(ga_graph* g) {
     cudaMemcpyAsync(hist, d_hist, 33 * 8, cudaMemcpyDeviceToHost, st);
     cudaFreeAsync(d_hist, st);
     GA_CUDA(cudaStreamSynchronize(st));
-    uint64_t key = mix64(32 - __builtin_clz(n | 1)) ^ mix64(0x100 + 32 - __builtin_clz(g->m));
+    uint64_t key = mix64(32 - __builtin_clz(n | 1)) ^ mix64(0x100 + 32 - __builtin_clz(g->m)) ^ mix64(0x5e2);
     for (int b = 0; b < 33; b++) {
         const uint64_t q = (hist[b] * 16 + g->m / 2) / g->m;   // sixteenths of the edges
         key = mix64(key ^ (q << 8) ^ (uint64_t)b);
@@ -573,46 +627,83 @@ ga_status autotune(ga_graph* g) {
         tune_cache_load_locked();
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) {
-            g->tuned_kernel = it->second;
+            const TuneChoice c = it->second;
+            GA_TRY(apply_choice(g, c));
+            g->tuned_kernel = c.kernel;
             g->tune_key = key;
+            g->tune_ms = 0;
             return GA_OK;
         }
     }
-    // time both kernels once (count only) on this graph
+    // time the candidates on this graph (count only); every kernel's code is loaded first (lazy module loading
+    // would otherwise charge the load to the first candidate)
     cudaEvent_t e0, e1;
     GA_CUDA(cudaEventCreate(&e0));
     GA_CUDA(cudaEventCreate(&e1));
-    float ms[3] = {0, 0, 0};
     TcArgs<unsigned int> a{};
     a.total = g->d_scalars + 2;
-    ga_status s = GA_OK;
-    // a kernel's first launch in the process would also load its code (lazy module loading): load both first
     cudaFuncAttributes fa;
     cudaFuncGetAttributes(&fa, k_tc_hash<TC_COUNT, false, unsigned int>);
     cudaFuncGetAttributes(&fa, k_tc_plain<TC_COUNT, false, unsigned int>);
-    for (int k = 1; k <= 2 && s == GA_OK; k++) {
-        g->tuned_kernel = k;
-        cudaEventRecord(e0, st);
-        s = run_tc<TC_COUNT, false, unsigned int>(g, a, true);
-        cudaEventRecord(e1, st);
-        if (s == GA_OK && cudaEventSynchronize(e1) != cudaSuccess) s = fail(GA_ERR_CUDA, "autotune timing failed");
-        if (s == GA_OK) cudaEventElapsedTime(&ms[k], e0, e1);
+    ga_status s = GA_OK;
+    // best of two launches of candidate c
+    auto time_of = [&](const TuneChoice& c, float* ms) -> ga_status {
+        GA_TRY(apply_choice(g, c));
+        g->tuned_kernel = c.kernel;
+        float best = 1e30f;
+        for (int rep = 0; rep < 2; rep++) {
+            cudaEventRecord(e0, st);
+            GA_TRY((run_tc<TC_COUNT, false, unsigned int>(g, a, true)));
+            cudaEventRecord(e1, st);
+            if (cudaEventSynchronize(e1) != cudaSuccess) return fail(GA_ERR_CUDA, "autotune timing failed");
+            float t = 0;
+            cudaEventElapsedTime(&t, e0, e1);
+            best = std::min(best, t);
+        }
+        *ms = best;
+        return GA_OK;
+    };
+    TuneChoice hash{2, g->light_max_deg, g->item_work}, plain{1, g->light_max_deg, g->item_work};
+    float hash_ms = 0, plain_ms = 0;
+    s = time_of(hash, &hash_ms);
+    if (s == GA_OK) s = time_of(plain, &plain_ms);   // the plain kernel does not use the items
+    for (uint32_t light : {32u, 64u, 128u, 256u}) {   // the bin cutoff, at the current item work
+        if (s != GA_OK || g->light_max_deg_set || light == hash.light_max_deg) continue;
+        TuneChoice c = hash;
+        c.light_max_deg = light;
+        float t = 0;
+        s = time_of(c, &t);
+        if (s == GA_OK && t < hash_ms) { hash = c; hash_ms = t; }
     }
+    for (uint32_t work : {1024u, 4096u, 16384u}) {    // the item work, at the best cutoff
+        if (s != GA_OK || g->item_work_set || work == hash.item_work) continue;
+        TuneChoice c = hash;
+        c.item_work = work;
+        float t = 0;
+        s = time_of(c, &t);
+        if (s == GA_OK && t < hash_ms) { hash = c; hash_ms = t; }
+    }
+    // the items stay at the best hash configuration either way (supports and incidence lists use them)
+    TuneChoice best = hash;
+    float best_ms = hash_ms;
+    if (plain_ms < hash_ms) { best.kernel = 1; best_ms = plain_ms; }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     g->tuned_kernel = 0;
     GA_TRY(s);
-    const int best = ms[1] < ms[2] ? 1 : 2;
+    GA_TRY(apply_choice(g, best));
     {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         tune_cache_store_locked(key, best);
     }
-    g->tuned_kernel = best;
+    g->tuned_kernel = best.kernel;
     g->tune_key = key;
+    g->tune_ms = best_ms;
     return GA_OK;
 }
 
 template ga_status run_tc<TC_COUNT, false, unsigned int>(ga_graph*, const TcArgs<unsigned int>&, bool);
+template ga_status run_tc<TC_COUNT, true, unsigned int>(ga_graph*, const TcArgs<unsigned int>&, bool);
 template ga_status run_tc<TC_VSUP, false, unsigned long long>(ga_graph*, const TcArgs<unsigned long long>&, bool);
 template ga_status run_tc<TC_VSUP, false, unsigned int>(ga_graph*, const TcArgs<unsigned int>&, bool);
 template ga_status run_tc<TC_VSUP, true, unsigned int>(ga_graph*, const TcArgs<unsigned int>&, bool);
@@ -631,6 +722,19 @@ struct Scratch {
     cudaStream_t st = nullptr;
     ~Scratch() { if (p) cudaFreeAsync(p, st); }
 };
+
+// alive[v] = core[v] >= k; the number of such vertices is added to *cnt (one atomic per warp).
+__global__ void k_core_mask(const uint32_t* __restrict__ core, uint32_t n, uint32_t k, uint8_t* __restrict__ alive,
+                            unsigned long long* cnt) {
+    uint32_t c = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const uint8_t in = core[v] >= k;
+        alive[v] = in;
+        c += in;
+    }
+    c = __reduce_add_sync(GA_FULL_MASK, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(cnt, (unsigned long long)c);
+}
 
 ga_status read_total(ga_graph* g, const unsigned long long* d_total, uint64_t* out) {
     GA_CUDA(cudaMemcpyAsync(g->h_scalars, d_total, 8, cudaMemcpyDeviceToHost, g->stream));
@@ -752,6 +856,51 @@ ga_status ga_tc_participation(ga_graph* g, const uint8_t* alive, uint32_t* tri, 
     GA_TRY((run_tc<TC_VSUP, true, unsigned int>(g, a, true)));
     if (g->n) GA_CUDA(cudaMemcpyAsync(tri, d_tri, (size_t)g->n * 4, cudaMemcpyDeviceToHost, g->stream));
     return read_total(g, a.total, triangles);
+}
+
+ga_status ga_graph_tuning(ga_graph* g, ga_tuning* out) {
+    if (!g || !out) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    GA_GRAPH_LOCK(g);
+    GA_TRY(use_device(g));
+    GA_TRY(ready(g));
+    out->kernel = (uint32_t)(g->opt_tc_kernel ? g->opt_tc_kernel : g->tuned_kernel);
+    out->light_max_deg = g->light_max_deg;
+    out->item_work = g->item_work;
+    out->signature = g->tune_key;
+    out->measured_ms = g->opt_tc_kernel ? 0.0 : (double)g->tune_ms;
+    out->heavy_items = g->heavy.count;
+    out->light_items = g->light.count;
+    return GA_OK;
+}
+
+ga_status ga_core_level_density(ga_graph* g, const uint32_t* core, uint32_t k, uint64_t* triangles,
+                                uint64_t* vertices) {
+    if (!g || (!core && g->n) || !triangles || !vertices) return fail(GA_ERR_INVALID_ARGUMENT, "null argument");
+    GA_GRAPH_LOCK(g);
+    GA_TRY(use_device(g));
+    GA_TRY(ready(g));
+    Scratch s;
+    s.st = g->stream;
+    const size_t n = g->n;
+    GA_CUDA(pool_malloc(&s.p, (n + 1) * 5, g->stream));
+    uint32_t* d_core = (uint32_t*)s.p;
+    uint8_t* d_alive = (uint8_t*)(d_core + n + 1);
+    unsigned long long* d_cnt = g->d_scalars + 1;
+    GA_CUDA(cudaMemsetAsync(d_cnt, 0, 8, g->stream));
+    if (n) {
+        GA_CUDA(cudaMemcpyAsync(d_core, core, n * 4, cudaMemcpyHostToDevice, g->stream));
+        k_core_mask<<<grid_for(n, 256), 256, 0, g->stream>>>(d_core, g->n, k, d_alive, d_cnt);
+        GA_CUDA(cudaGetLastError());
+    }
+    TcArgs<unsigned int> a{};
+    a.total = g->d_scalars;
+    a.alive = d_alive;
+    GA_TRY((run_tc<TC_COUNT, true, unsigned int>(g, a, true)));
+    GA_CUDA(cudaMemcpyAsync(g->h_scalars, g->d_scalars, 16, cudaMemcpyDeviceToHost, g->stream));
+    GA_CUDA(cudaStreamSynchronize(g->stream));
+    *triangles = g->h_scalars[0];
+    *vertices = g->h_scalars[1];
+    return GA_OK;
 }
 
 }  // extern "C"

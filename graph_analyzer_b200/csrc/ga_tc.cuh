@@ -21,6 +21,7 @@ struct TcArgs {
     const unsigned long long* inc_ptr = nullptr;
     uint32_t* fill = nullptr;
     uint32_t* overflow = nullptr;   // TC_LIST: entries that found their list full (must stay 0)
+    const uint32_t* origk = nullptr;  // set by the launcher: position in col of each (degree, id)-ordered entry
     // shard `shard` of `nshards` (0 = the whole graph): equal parts of the work items (hash kernel) or of the edges
     // (plain kernel); the shards of a graph partition its triangles
     uint32_t shard = 0, nshards = 0;

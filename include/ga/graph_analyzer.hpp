@@ -14,6 +14,7 @@
 //   batch_peel_loop(n, T_full, num, den, DeviceGraph&)   batch_peel_loop (densest.h:279-303) + GpuBackend
 //   core_decomp_loop_inc(n, T_full, DeviceGraph&, core)  core_decomp_loop_inc (dsg.h:724-751) + GpuCoreBackendInc
 //   Dens, dens_cmp, dens_gt, dens_ceil, DsgResult        dsg.h:33-59
+//   core_level_density(DeviceGraph&, core, k)            dsg.h:169-174 (the count restricted to the k-core, on device)
 //   greedy, greedy_pp, core_exact, exact_densest         dsg.h:189-250, 463-627, 405-428 (device triangle lists)
 //   prune_to_core                                        dsg.h:638-645
 //   GreedyResult, greedy_peel                            cpu_greedy_peel, densest.h:193-252 (the same greedy)
@@ -319,6 +320,15 @@ class Server {
         check(ga_server_submit(h_, graph_id, kind, num, den, &t));
         return t;
     }
+    // Also returns the vertex array into `out` (resized to n here; keep it alive and unread until wait() on the
+    // ticket returns): removed_round for GA_REQ_PEEL, core numbers for GA_REQ_CORE.
+    uint64_t submit(uint64_t graph_id, ga_request_kind kind, uint64_t num, uint64_t den, uint32_t n,
+                    std::vector<uint32_t>& out) {
+        out.assign(n, UINT32_MAX);
+        uint64_t t = 0;
+        check(ga_server_submit_out(h_, graph_id, kind, num, den, out.data(), out.size(), &t));
+        return t;
+    }
     ga_request_result wait(uint64_t ticket) {
         ga_request_result r{};
         check(ga_server_wait(h_, ticket, &r));
@@ -342,6 +352,15 @@ inline int dens_cmp(Dens a, Dens b) {
 inline bool dens_gt(Dens a, Dens b) { return dens_cmp(a, b) > 0; }
 inline uint64_t dens_ceil(Dens d) { return d.den == 0 ? 0 : (d.num + d.den - 1) / d.den; }
 inline double dens_value(Dens d) { return density_value(d.num, d.den); }
+
+// Triangles / vertices of {v : core[v] >= k}, the (k, triangle)-core (core_level_density, dsg.h:169-174); the count
+// runs on the device over the induced subgraph.
+inline Dens core_level_density(DeviceGraph& d, const std::vector<uint32_t>& core, uint32_t k) {
+    if (core.size() != d.n()) throw Error(GA_ERR_INVALID_ARGUMENT, "core must have n entries");
+    Dens r;
+    check(ga_core_level_density(d.handle(), core.data(), k, &r.num, &r.den));
+    return r;
+}
 
 struct DsgResult {
     uint64_t tri = 0, verts = 0;          // best subgraph: triangles / vertices (0/0 = graph without triangles)
@@ -461,6 +480,7 @@ using ga::batch_peel_loop;
 using ga::build_graph_from_edges;
 using ga::core_decomp_loop_inc;
 using ga::core_exact;
+using ga::core_level_density;
 using ga::Dens;
 using ga::dens_ceil;
 using ga::dens_cmp;

@@ -200,19 +200,38 @@ ga_status ga_tc_count_shard_async(ga_graph* g, uint32_t shard, uint32_t nshards,
  * cannot call cudaMalloc: a process whose device memory is entirely claimed by another allocator (for example a
  * framework's caching pool that reserved the free HBM up front), or a latency-critical path that must not pay for
  * cudaMalloc's implicit device synchronisation. The caller passes the oriented CSR in device memory of `device`
- * (rowptr[n+1], col[m], the reference's layout) and receives the count in host memory; the only scratch the call
- * uses (row owners and a few status words, 4 * GA_NOALLOC_MAX_EDGES bytes) is a fixed array compiled into the
- * library, which every GPU that loads the library holds until the process exits.
- *  - m > GA_NOALLOC_MAX_EDGES gives GA_ERR_CAPACITY; an invalid CSR gives GA_ERR_INVALID_GRAPH (checked on the
- *    device before any row is followed).
- *  - The first call on a device looks up the array's device address; make that first call before starting any
- *    stream capture on that device.
+ * (rowptr[n+1], col[m], the reference's layout: rows sorted, every edge from the smaller (degree, id) endpoint,
+ * degree = out + in) and receives the count in host memory; the only scratch the call uses (one in-degree counter
+ * per vertex and a few status words, 4 * GA_NOALLOC_MAX_VERTICES bytes) is a fixed array compiled into the
+ * library, which a GPU holds from the first call on it until the process exits.
+ *  - m > GA_NOALLOC_MAX_EDGES or n > GA_NOALLOC_MAX_VERTICES gives GA_ERR_CAPACITY; an invalid CSR gives
+ *    GA_ERR_INVALID_GRAPH: bad rowptr, an endpoint >= n, a self loop, a row not strictly ascending, or an edge
+ *    against the (degree, id) orientation (so a cyclically oriented or symmetric CSR is refused, not miscounted).
+ *    All of it is checked on the device before any row is followed.
+ *  - The device memory of the array is taken when the library's code is loaded on the device, which (lazy module
+ *    loading, CUDA 12's default) happens at the first call on that device. Make one call (n = m = 0 will do) on each
+ *    device before another allocator claims its free memory, and before starting any stream capture on it: that
+ *    first call also looks up the array's device address (again after the device's context changes).
  *  - All calls share the one array per device: calls that overlap on the GPU (different streams or threads at the
  *    same time) race and give wrong counts. Serialise them.
  *  - Synchronous: returns after the count has been read back. */
 #define GA_NOALLOC_MAX_EDGES 4194304u
+#define GA_NOALLOC_MAX_VERTICES 4194304u
 ga_status ga_tc_count_noalloc(const uint32_t* d_rowptr, const uint32_t* d_col, uint32_t n, uint32_t m, int device,
                               void* stream, uint64_t* triangles);
+
+/* What the count of a graph runs with (after ga_graph_prepare; tunes first when GA_OPT_TC_KERNEL is 0): the kernel
+ * (1 plain, 2 degree-binned hash), the bin cutoff and item work of the hash kernel's work lists (chosen by the
+ * autotuner unless set with GA_OPT_LIGHT_MAX_DEG / GA_OPT_ITEM_WORK), the degree-distribution signature the choice
+ * is cached under, and the count time of the choice when the autotuner measured it (0 when it came from the cache
+ * or the kernel was forced). Replaces the compile-time knobs of kernels.cuh:23-34 (group size, bin cutoffs). */
+typedef struct ga_tuning {
+    uint32_t kernel, light_max_deg, item_work, reserved;
+    uint64_t signature;
+    double measured_ms;
+    uint64_t heavy_items, light_items;
+} ga_tuning;
+ga_status ga_graph_tuning(ga_graph* g, ga_tuning* out);
 
 /* Per-oriented-edge support, indexed like col: sup[e] = triangles containing edge e (for_each_triangle's
  * (e, i, j), dsg.h:67-79). `sup` is host memory of m entries. *triangles may be NULL. */
@@ -227,6 +246,13 @@ ga_status ga_tc_support_vertices(ga_graph* g, uint64_t* deg, uint64_t* triangles
  * cpu_triangle_participation (densest.h:81-101). alive and tri are host memory of n entries. Refuses T >= 2^32
  * (uint32 counters) with GA_ERR_ARITH. */
 ga_status ga_tc_participation(ga_graph* g, const uint8_t* alive, uint32_t* tri, uint64_t* triangles);
+
+/* Triangles and vertices of the (k, triangle)-core {v : core[v] >= k} = core_level_density (dsg.h:169-174): the
+ * subgraph's density is *triangles / *vertices (compare densities exactly with dens_cmp, dsg.h:40-45). `core` is
+ * host memory of n entries (for example from ga_core_decomposition); the count runs on the device restricted to the
+ * induced subgraph. */
+ga_status ga_core_level_density(ga_graph* g, const uint32_t* core, uint32_t k, uint64_t* triangles,
+                                uint64_t* vertices);
 
 /* ---- triangle-density batch peeling: replaces batch_peel_loop<GpuBackend> (densest.h:279-303,
  *      gpu_densest.cu:70-126) with a device-resident loop ---- */
@@ -255,6 +281,8 @@ ga_status ga_batch_destroy(ga_batch* b);
 /* Same options as ga_graph_set_option, applied to the batch's kernels and loop. */
 ga_status ga_batch_set_option(ga_batch* b, ga_option opt, int64_t value);
 ga_status ga_batch_device_bytes(const ga_batch* b, uint64_t* bytes);
+/* The count configuration of the batch's one launch over the union (ga_graph_tuning). */
+ga_status ga_batch_tuning(ga_batch* b, ga_tuning* out);
 /* Triangle count of every graph (triangles: host, G entries), one persistent launch over all graphs. */
 ga_status ga_batch_tc(ga_batch* b, uint64_t* triangles);
 /* Triangle count and triangle-density batch peeling (eps = num/den) of every graph: one count launch and one
@@ -387,6 +415,13 @@ ga_status ga_server_add_graph(ga_server* s, const uint32_t* rowptr, const uint32
 /* Queues a request; returns at once with a ticket. eps = num/den for GA_REQ_PEEL. */
 ga_status ga_server_submit(ga_server* s, uint64_t graph_id, ga_request_kind kind, uint64_t num, uint64_t den,
                            uint64_t* ticket);
+/* The same, and the request's vertex array is written to `out` (host memory of out_len >= n entries, owned by the
+ * caller and left untouched until the result is handed out by ga_server_poll / ga_server_wait): for GA_REQ_PEEL the
+ * removed_round of every vertex (UINT32_MAX = never removed; the peeled set is {v : removed_round[v] >= best_round},
+ * the set gpu_densest.cu:220-226 reads), for GA_REQ_CORE the core number of every vertex (gpu_dsg.cu:283-289's
+ * core[]); ignored for GA_REQ_TC. out = NULL is ga_server_submit. */
+ga_status ga_server_submit_out(ga_server* s, uint64_t graph_id, ga_request_kind kind, uint64_t num, uint64_t den,
+                               uint32_t* out, uint64_t out_len, uint64_t* ticket);
 /* GA_ERR_NOT_READY while the request is pending; otherwise fills *out (out->status is the request's own status).
  * A result is handed out once: after a successful poll or wait the ticket is forgotten (a second call on it gives
  * GA_ERR_INVALID_ARGUMENT), so a long-running server keeps no state for collected requests. One thread per ticket. */

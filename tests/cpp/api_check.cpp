@@ -28,6 +28,8 @@ int main(int argc, char** argv) {
         unsigned long long ch = 0;
         for (uint32_t v = 0; v < g.n; v++) ch = ch * 1000003ull + core[v];
         std::printf("cores %u %u %llx\n", c.kmax, c.rounds, ch);
+        const Dens kd = core_level_density(d, core, c.kmax);
+        std::printf("kcore %llu %llu\n", (unsigned long long)kd.num, (unsigned long long)kd.den);
         std::vector<uint32_t> sup;
         std::vector<uint64_t> deg;
         std::printf("supports %llu %llu\n", (unsigned long long)d.edge_support(sup),
@@ -59,13 +61,16 @@ int main(int argc, char** argv) {
                               b.triangles() == bt;
             ga::Server srv;
             const uint64_t id = srv.add_graph(g);
-            const uint64_t t_tc = srv.submit(id, GA_REQ_TC), t_peel = srv.submit(id, GA_REQ_PEEL, num, den),
-                           t_core = srv.submit(id, GA_REQ_CORE);
+            std::vector<uint32_t> served_rr, served_core;   // the served vertex arrays
+            const uint64_t t_tc = srv.submit(id, GA_REQ_TC),
+                           t_peel = srv.submit(id, GA_REQ_PEEL, num, den, g.n, served_rr),
+                           t_core = srv.submit(id, GA_REQ_CORE, 1, 1, g.n, served_core);
             const ga_request_result a = srv.wait(t_tc), p = srv.wait(t_peel), q = srv.wait(t_core);
             const bool served = a.status == GA_OK && a.triangles == T_full && p.status == GA_OK &&
                                 p.peel.best_num == r.best_num && p.peel.best_den == r.best_den &&
                                 p.peel.best_round == r.best_round && p.peel.rounds == r.rounds &&
-                                q.status == GA_OK && q.core.kmax == c.kmax && q.core.rounds == c.rounds;
+                                q.status == GA_OK && q.core.kmax == c.kmax && q.core.rounds == c.rounds &&
+                                served_rr == r.removed_round && served_core == core;
             std::printf("batch_serve %d %d\n", same ? 1 : 0, served ? 1 : 0);
         }
         // the refusals of batch_peel_loop (densest.h:65-78, 283-287): wrong T_full, eps out of range

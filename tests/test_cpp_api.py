@@ -48,6 +48,7 @@ def test_reference_names_match_golden(api_check, golden, cuda_ok, name):
     assert out["peel"].split() == [str(p["best_num"]), str(p["best_den"]), str(p["best_round"]), str(p["rounds"]),
                                    _hash(a["removed_round_1_10"])]
     assert out["cores"].split() == [str(w["kmax"]), str(w["core_rounds"]), _hash(a["core"])]
+    assert out["kcore"].split() == [str(x) for x in w["kmax_core_density"]]   # core_level_density, dsg.h:169
     assert out["supports"].split() == [str(w["triangles"])] * 2
     assert out["refusals"].split() == ["0", "0"]
     assert out["batch_serve"].split() == ["1", "1"]      # DeviceBatch and Server give the single-graph results

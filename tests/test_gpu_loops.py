@@ -212,3 +212,22 @@ def test_gpu_best_round_recomputed_from_removed_round(ga, cuda_ok, name, eps):
     with ga.DeviceGraph(g) as d:
         r = d.batch_peel(*eps)
     assert (r.best_num, r.best_den, r.best_round, r.rounds) == best_from_removed_round(g, r.removed_round)
+
+
+@pytest.mark.parametrize("kernel", [1, 2])
+def test_core_level_density_every_level(ga, oracle, golden, cuda_ok, kernel):
+    """core_level_density (dsg.h:169-174) on the device, at every core level of a Holme-Kim and an R-MAT graph and
+    the golden kmax-core of each fixture, for both count kernels."""
+    for name in FIXTURES:
+        g = ga.load_graph(fixture_path(name))
+        with ga.DeviceGraph(g) as d:
+            d.set_option(ga.OPT_TC_KERNEL, kernel)
+            got = d.core_level_density(golden_arrays(name)["core"], golden[name]["kmax"])
+            assert list(got) == golden[name]["kmax_core_density"]
+    for g in (ga.graph_from_pairs(2000, ga.gen_holme_kim(2000, 5, 6, 0.5, 0.5, seed=3)),
+              ga.graph_from_pairs(1 << 12, ga.gen_rmat(12, 10 << 12, seed=5))):
+        core, kmax, _ = oracle.core_levels(g)
+        with ga.DeviceGraph(g) as d:
+            d.set_option(ga.OPT_TC_KERNEL, kernel)
+            for k in sorted(set(core.tolist()) | {0, kmax + 1}):
+                assert d.core_level_density(core, k) == oracle.core_level_density(g, core, k), k

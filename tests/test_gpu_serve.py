@@ -1,8 +1,11 @@
 """GPU tests of the request loop (ga_server): every request served in a concurrent mix - folded into batch launches,
 run on resident graphs, after evictions - returns exactly what the same request returns alone, and what the oracle
-gives for that graph (triangle count, PeelResult fields (densest.h:46-59), kmax and rounds of CoreLoopResult
-(dsg.h:687-691))."""
+gives for that graph (triangle count, PeelResult fields (densest.h:46-59) with the whole removed_round array, kmax,
+rounds and every core number of CoreLoopResult (dsg.h:687-691), the sets gpu_densest.cu:220-226 and
+gpu_dsg.cu:283-289 read)."""
 from __future__ import annotations
+
+import ctypes as C
 
 import numpy as np
 import pytest
@@ -30,19 +33,30 @@ def _graphs(ga, seed):
 
 
 def _alone(ga, g):
-    """Each request kind on its own device graph, one at a time."""
+    """Each request kind on its own device graph, one at a time (with the vertex arrays)."""
     out = {}
     with ga.DeviceGraph(g) as d:
         T = d.tc_count()
         out["tc"] = T
         for num, den in EPS:
-            r = d.batch_peel(num, den, want_removed=False)
+            r = d.batch_peel(num, den)
             out[("peel", num, den)] = (T, r.best_num, r.best_den, r.best_round, r.rounds)
+            out[("peel_array", num, den)] = r.removed_round
     with ga.DeviceGraph(g) as d:
-        c = d.core_decomposition(want_core=False)
+        c = d.core_decomposition()
         out["core"] = (T, c.kmax, c.rounds)
+        out["core_array"] = c.core
         out["bytes"] = d.device_bytes()   # resident with loop state and incidence lists
     return out
+
+
+def _array_ok(ga, kind, num, den, r, a) -> bool:
+    """The served vertex array equals the one of the request run alone."""
+    if kind == ga.REQ_PEEL:
+        return np.array_equal(r.peel.removed_round, a[("peel_array", num, den)])
+    if kind == ga.REQ_CORE:
+        return np.array_equal(r.core_numbers, a["core_array"])
+    return True
 
 
 def _key(kind, num, den):
@@ -83,8 +97,10 @@ def test_alone_matches_oracle(ga, oracle, served):
         for num, den in EPS:
             o = oracle.batch_peel(g, num, den)
             assert a[("peel", num, den)][1:] == (o.best_num, o.best_den, o.best_round, o.rounds)
-        _, kmax, rounds = oracle.core_levels(g)
+            assert np.array_equal(a[("peel_array", num, den)], o.removed_round)
+        core, kmax, rounds = oracle.core_levels(g)
         assert a["core"][1:] == (kmax, rounds)
+        assert np.array_equal(a["core_array"], core)
 
 
 @pytest.mark.parametrize("slots,fold,small,pin", [(4, 64, 0, 0), (1, 64, 1, 1), (6, 1, 3, 0), (3, 5, 2, 1)])
@@ -95,11 +111,15 @@ def test_mix_equals_alone(ga, served, slots, fold, small, pin):
     reqs = _mix(rng, len(gs), 0.3)
     with ga.Server(slots=slots, fold_max_graphs=fold, small_slots=small, pin_min_edges=pin) as s:
         ids = [s.add_graph(g) for g in gs]
-        tickets = [s.submit(ids[i], kind, num, den) for i, kind, num, den in reqs]
-        for t, (i, kind, num, den) in zip(tickets, reqs):
+        # every other request also asks for its vertex array (removed_round / core numbers)
+        tickets = [s.submit(ids[i], kind, num, den, want_array=j % 2 == 0)
+                   for j, (i, kind, num, den) in enumerate(reqs)]
+        for j, (t, (i, kind, num, den)) in enumerate(zip(tickets, reqs)):
             r = s.wait(t)
             assert r.status == 0, (i, kind)
             assert _value(ga, kind, r) == alone[i][_key(kind, num, den)], (i, kind, num, den, r.folded)
+            if j % 2 == 0:
+                assert _array_ok(ga, kind, num, den, r, alone[i]), (i, kind, num, den, r.folded)
         st = s.stats()
     assert st["submitted"] == st["completed"] == len(reqs)
     if fold > 1:
@@ -132,11 +152,12 @@ def test_small_budget_evicts_and_still_matches(ga, served):
         ids = [s.add_graph(gs[big]), s.add_graph(gs[big])]
         reqs = [(c, kind) for _ in range(3) for c in (0, 1) for kind in (0, 1, 2)]
         reqs = [reqs[j] for j in rng.permutation(len(reqs))]
-        tickets = [s.submit(ids[c], kind, 1, 10) for c, kind in reqs]
+        tickets = [s.submit(ids[c], kind, 1, 10, want_array=True) for c, kind in reqs]
         for t, (c, kind) in zip(tickets, reqs):
             r = s.wait(t)
             assert r.status == 0, (c, kind)
             assert _value(ga, kind, r) == alone[big][_key(kind, 1, 10)]
+            assert _array_ok(ga, kind, 1, 10, r, alone[big])
         st = s.stats()
     assert st["peak_reserved_bytes"] <= budget
     assert st["evictions"] > 0
@@ -155,6 +176,11 @@ def test_refusals(ga, served):
             s.submit(gid, ga.REQ_PEEL, 1, 0)                 # eps denominator 0
         with pytest.raises(ga.GAError):
             s.wait(12345)                                    # unknown ticket
+        short = np.zeros(max(gs[0].n - 1, 0), np.uint32)
+        t = C.c_uint64(0)
+        rc = ga.lib().ga_server_submit_out(s._h, gid, ga.REQ_CORE, 1, 1, short.ctypes.data if short.size else None,
+                                           short.size, C.byref(t))
+        assert ga.STATUS[rc] == "GA_ERR_INVALID_ARGUMENT"    # vertex array shorter than n
         t = s.submit(gid, ga.REQ_TC)
         r = s.wait(t)
         assert r.status == 0 and r.triangles == 0

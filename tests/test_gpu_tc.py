@@ -207,3 +207,32 @@ def test_one_handle_from_many_threads(ga, oracle, cuda_ok):
         for t in threads:
             t.join()
     assert not errors, errors
+
+
+def test_autotuner_choices(ga, oracle, cuda_ok):
+    """The autotuner picks a kernel, bin cutoff and item work per degree-distribution signature; every candidate it
+    times gives the oracle's count, options set by the caller are kept, and a second graph with the same signature
+    takes the cached choice without timing."""
+    graphs = [ga.graph_from_pairs(1 << 15, ga.gen_rmat(15, 9 << 15, seed=21)),
+              ga.graph_from_pairs(50000, ga.gen_holme_kim(50000, 6, 7, 0.54, 0.3, seed=22))]
+    for g in graphs:
+        want = oracle.triangles_omp(g)
+        with ga.DeviceGraph(g) as d:
+            assert d.tc_count() == want
+            t = d.tuning()
+            assert t["kernel"] in ("plain", "hash") and t["light_max_deg"] in (32, 64, 128, 256)
+            assert t["item_work"] in (1024, 4096, 16384) and t["measured_ms"] >= 0   # 0: an earlier graph's choice
+            _, sup = d.support_edges()
+            assert np.array_equal(sup, oracle.edge_support(g)[1])
+        with ga.DeviceGraph(g) as d:                 # same signature: from the cache
+            assert d.tc_count() == want
+            t2 = d.tuning()
+            assert t2["measured_ms"] == 0 and t2["signature"] == t["signature"]
+            assert (t2["kernel"], t2["light_max_deg"], t2["item_work"]) == (t["kernel"], t["light_max_deg"],
+                                                                             t["item_work"])
+        with ga.DeviceGraph(g) as d:                 # caller's options stay
+            d.set_option(ga.OPT_LIGHT_MAX_DEG, 64)
+            d.set_option(ga.OPT_ITEM_WORK, 2048)
+            assert d.tc_count() == want
+            t3 = d.tuning()
+            assert (t3["light_max_deg"], t3["item_work"]) == (64, 2048)
