@@ -13,7 +13,14 @@ Reported (one JSON line, rank 0):
                validation), ga_graph_prepare, ga_tc_count (8-byte D2H) and ga_graph_destroy, every step;
   roofline     B_alg per launch / CUDA-event launch time vs the measured HBM copy bandwidth;
   cpu_baseline the reference's own cpu_triangles_omp (oracle/_ref, compiled from its sources) on the host cores.
-``--impl reference`` times the reference's CPU implementation alone with the same metric.
+``--impl reference`` times the reference's CPU implementation alone with the same metric (its graph built by the
+library's generator alone, libga_gen.so, and the reference's own build_graph_from_edges).
+
+After the headline (outside its timed region) the default run adds the secondary workloads to the same line under
+"workloads", each with parity against the reference's CPU code and its own CPU baseline: hk2 (Holme-Kim n 1.70M,
+count + batch peeling at three eps), rmat22-full (per-edge supports and (k, triangle)-cores of the headline graph),
+batch (4,096 graphs in one launch vs per-graph launches) and serve (Poisson arrivals into the request loop, p50/p99).
+``--workload NAME`` runs one of them alone as its own line; ``--legs`` picks which the default run adds.
 Multi-GPU (torchrun, one rank per GPU): replicas by default - every rank counts its own copy of the graph, no
 collective on the data path; the max over ranks of the device time gives the whole-job value (weak scaling). With
 --shard the ranks count ONE graph together, rank r its shard r of N (ga_tc_count_shard), summed by one 8-byte
@@ -52,6 +59,39 @@ def make_graph(ga, scale=SCALE, ef=EDGE_FACTOR, seed=SEED):
     log(f"graph: R-MAT scale {scale} ef {ef} seed {seed}: n={g.n} m={g.m} max_out_degree={g.max_out_degree} "
         f"({time.time() - t0:.1f} s on the host)")
     return g
+
+
+def reference_graph(scale=SCALE, ef=EDGE_FACTOR, seed=SEED):
+    """The same R-MAT graph as make_graph, built without the CUDA library: the samples come from libga_gen.so (the
+    library's generator alone), the clean-up (self loops dropped, (min, max), unique) is numpy's, and the oriented CSR
+    is the reference's own build_graph_from_edges (graph.h:38-67, oracle/_ref). Returns the reference's Graph fields."""
+    import ctypes as C
+    from oracle import Reference
+    lib = C.CDLL(os.path.join(ROOT, "graph_analyzer_b200", "_lib", "libga_gen.so"))
+    lib.ga_gen_rmat.argtypes = [C.c_uint32, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_void_p]
+    lib.ga_permute_ids.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint64]
+    t0 = time.time()
+    ns = int(ef * (1 << scale))
+    pairs = np.zeros(2 * ns, np.uint32)
+    if lib.ga_gen_rmat(scale, ns, *RMAT, seed, pairs.ctypes.data) or lib.ga_permute_ids(pairs.ctypes.data, ns,
+                                                                                          1 << scale, seed):
+        raise RuntimeError("libga_gen: generation failed")
+    p = pairs.reshape(-1, 2).astype(np.uint64)
+    lo, hi = np.minimum(p[:, 0], p[:, 1]), np.maximum(p[:, 0], p[:, 1])
+    keys = np.unique((lo << np.uint64(32) | hi)[lo != hi])
+    edges = np.stack([keys >> np.uint64(32), keys & np.uint64(0xFFFFFFFF)], 1).astype(np.uint32)
+    g = Reference().build_graph_from_edges(1 << scale, edges)
+    log(f"graph (reference build): R-MAT scale {scale} ef {ef} seed {seed}: n={g.n} m={g.m} "
+        f"max_out_degree={g.max_out_degree} ({time.time() - t0:.1f} s on the host)")
+    return g
+
+
+def headline_config(scale, g, triangles, b_alg, parallelism):
+    """The `config` of the headline line, identical in keys (and in everything but `parallelism`) in both arms."""
+    return {"workload": f"rmat{scale}_tc", "n": g.n, "m": g.m, "edge_factor": EDGE_FACTOR, "seed": SEED,
+            "rmat_abc": list(RMAT), "triangles": triangles, "b_alg_bytes": b_alg,
+            "l2": f"256 MiB written between timed steps (untimed); col alone is {4 * g.m / 1e6:.0f} MB",
+            "parallelism": parallelism}
 
 
 def algorithmic_bytes(g) -> int:
@@ -186,10 +226,9 @@ def run_reference_arm(args):
         if dist:
             dist.destroy_process_group()
         return 0
-    import graph_analyzer_b200 as ga
     from oracle import Reference
     ref = Reference()
-    g = make_graph(ga, args.scale)
+    g = reference_graph(args.scale)
     b_alg = algorithmic_bytes(g)
     rg = ref.resident(g)
     # one whole count (untimed) sizes the sample: every step counts the rows [0, u1), chosen so that the whole
@@ -225,9 +264,10 @@ def run_reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"rmat{args.scale}_tc", "n": g.n, "m": g.m, "edge_factor": EDGE_FACTOR, "seed": SEED,
-                   "triangles": T_full, "b_alg_bytes": b_alg, "step_triangles": T, "step_b_alg_bytes": b_step,
-                   "full_count_ms": t_full * 1e3, "parallelism": "host threads (OpenMP)"},
+        "config": headline_config(args.scale, g, T_full, b_alg,
+                                  f"host threads x{ref.num_threads()} (OpenMP)"),
+        "sample": {"step_triangles": T, "step_b_alg_bytes": b_step, "full_count_ms": t_full * 1e3,
+                   "graph_build": "libga_gen samples + the reference's build_graph_from_edges"},
         "cpu_baseline": {"value": value, "unit": "GB/s", "cores": ref.num_threads(), "kind": "reference",
                          "sample": f"{sample}, cpu_triangles_omp (graph.h:123), {args.steps} steps"},
         "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -259,6 +299,7 @@ def run_ours(args):
     torch.cuda.synchronize(dev)
     prep_ms = (time.perf_counter() - t0) * 1e3
     T = dg.tc_count()
+    tuning = dg.tuning()
     shard = dist is not None and args.shard   # strong scaling: rank r counts shard r of world, one sum at the end
     count_async = ((lambda p: dg.tc_count_shard_async(rank, world, p)) if shard else dg.tc_count_async)
     for _ in range(args.warmup):
@@ -336,11 +377,9 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "strong" if shard else "weak", "vs_baseline": None,
         "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"rmat{args.scale}_tc", "n": g.n, "m": g.m, "edge_factor": EDGE_FACTOR, "seed": SEED,
-                   "rmat_abc": list(RMAT), "triangles": T, "b_alg_bytes": b_alg, "prep_ms": prep_ms,
-                   "l2": f"256 MiB written between steps (untimed); col alone is {4 * g.m / 1e6:.0f} MB",
-                   "parallelism": f"shards x{world} (one 8-byte all-reduce)" if shard else f"replicas x{world}",
-                   "oriented_edges_per_s": (1 if shard else world) * g.m / (ms / 1e3)},
+        "config": headline_config(args.scale, g, T, b_alg,
+                                  f"shards x{world} (one 8-byte all-reduce)" if shard else f"replicas x{world}"),
+        "prep_ms": prep_ms, "oriented_edges_per_s": (1 if shard else world) * g.m / (ms / 1e3), "tuning": tuning,
         "e2e": {"value": e2e_value, "unit": "GB/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(rp_h.numel() * 4 + col_h.numel() * 4), "d2h_bytes_per_step": 8,
                 "path": "ga_graph_create + ga_graph_prepare + ga_tc_count + ga_graph_destroy"},
@@ -351,14 +390,26 @@ def run_ours(args):
         "clocks": clk.summary(),
         "gpu_launches": args.steps,
     }
-    print(json.dumps(line), flush=True)
     dg.close()
+    del flush, d_out
+    if world == 1 and args.legs:
+        # the secondary workloads, after the headline's timed region and with its graph released from the device
+        line["workloads"] = run_legs(args, g)
+    print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
     return 0
 
 
-# ---- secondary workloads (one JSON line each; the default line above is the headline) ---------------------------
+# ---- secondary workloads -----------------------------------------------------------------------------------------
+# Each leg returns one dict: its GPU times (plain launches vs the autotuned, graph-captured form), parity of the
+# device results with the reference's own CPU code (oracle/_ref) or with the full-size records that code made
+# (tests/golden/fullsize.json), and the reference's CPU times on this host. The default run adds every leg to the
+# headline line under "workloads" (after the headline is measured; nothing here is inside its timed region);
+# ``--workload NAME`` prints one leg as its own line.
+
+FULLSIZE = os.path.join(ROOT, "tests", "golden", "fullsize.json")
+
 
 def _timed(torch, fn, reps=1):
     """Device-synchronised wall time of fn() in ms (mean over reps) and its last result."""
@@ -371,16 +422,39 @@ def _timed(torch, fn, reps=1):
     return (time.perf_counter() - t0) * 1e3 / reps, r
 
 
+def _cpu_timed(fn):
+    t0 = time.perf_counter()
+    r = fn()
+    return (time.perf_counter() - t0) * 1e3, r
+
+
 def _peel_key(p):
-    return (p.best_num, p.best_den, p.best_round, p.rounds)
+    return (int(p.best_num), int(p.best_den), int(p.best_round), int(p.rounds))
 
 
-def run_hk2(args):
-    """Holme-Kim n = 1.70M, 6-7 edges per new vertex (mean 6.54), p = 0.3: (a) plain one-kernel-per-launch count and
-    host-driven peeling (one sync per round) vs (b) autotuned kernels with the peeling loop captured as a CUDA graph,
-    eps in {1/20, 1/10, 1/2}; results must be bit-identical between the two."""
+def _sha(a) -> str:
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def _fullsize(part: str):
+    try:
+        with open(FULLSIZE) as f:
+            return json.load(f).get(part)
+    except (OSError, ValueError):
+        return None
+
+
+def leg_hk2(args) -> dict:
+    """Holme-Kim n = 1.70M, 6-7 edges per new vertex (mean 6.54), p = 0.3: TC and batch peeling at eps 1/20, 1/10,
+    1/2. GPU: (a) plain one-kernel-per-launch count and host-driven peeling (one sync per round, re-enumeration
+    updates) vs (b) the autotuned kernel with the peeling loop captured as a CUDA graph. Parity: every PeelResult field
+    and the whole removed_round of both forms against the reference's cpu_batch_peel (densest.h:138-160), serial and
+    OpenMP, and the count against cpu_triangles_serial. CPU: those reference calls timed on this host."""
     import torch
     import graph_analyzer_b200 as ga
+    from oracle import Reference
+    ref = Reference()
     t0 = time.time()
     g = ga.graph_from_pairs(1_700_000, ga.gen_holme_kim(1_700_000, 6, 7, 0.54, 0.3, seed=SEED))
     log(f"graph: Holme-Kim n={g.n} m={g.m} ({time.time() - t0:.1f} s on the host)")
@@ -391,43 +465,75 @@ def run_hk2(args):
     tuned.set_option(ga.OPT_LOOP_MODE, 2)
     plain.prepare()
     tuned.prepare()
-    out = {"tc_ms": {}, "peel_ms": {}, "first_peel_ms_tuned": None}
+    out = {"workload": "hk1.7M_tc_peel", "n": g.n, "m": g.m, "tc_ms": {}, "peel_ms": {}}
     T = {}
     for name, d in (("plain", plain), ("tuned", tuned)):
         for _ in range(args.warmup):
             d.tc_count()
         out["tc_ms"][name], T[name] = _timed(torch, d.tc_count, args.steps)
-    assert T["plain"] == T["tuned"]
-    first, _ = _timed(torch, lambda: tuned.batch_peel(1, 10, want_removed=False))   # builds the incidence lists
-    out["first_peel_ms_tuned"] = first
-    identical = True
+    out["tuning"] = tuned.tuning()
+    out["first_peel_ms_tuned"], _ = _timed(torch, lambda: tuned.batch_peel(1, 10, want_removed=False))
+    gpu = {}
     for num, den in ((1, 20), (1, 10), (1, 2)):
-        res = {}
+        key = f"{num}/{den}"
         for name, d in (("plain", plain), ("tuned", tuned)):
-            res[name] = d.batch_peel(num, den)          # untimed: the full result, removed_round included
+            gpu[(key, name)] = d.batch_peel(num, den)        # untimed: the full result, removed_round included
             # timed like the reference's gpu_densest time_ms: the loop, without downloading removed_round
             ms, r = _timed(torch, lambda: d.batch_peel(num, den, want_removed=False), max(1, args.steps // 2))
-            identical &= _peel_key(r) == _peel_key(res[name])
-            out["peel_ms"].setdefault(f"{num}/{den}", {})[name] = ms
-        identical &= res["plain"] == res["tuned"]
-        out["peel_ms"][f"{num}/{den}"]["result"] = list(_peel_key(res["tuned"]))
+            out["peel_ms"].setdefault(key, {})[name] = ms
+            assert _peel_key(r) == _peel_key(gpu[(key, name)])
     plain.close()
     tuned.close()
+    # the reference's CPU code on the same graph: parity and baseline
+    cpu = {"serial": {}, "omp": {}}
+    cpu["serial"]["tc"], Ts = _cpu_timed(lambda: ref.triangles_serial(g))
+    cpu["omp"]["tc"], To = _cpu_timed(lambda: ref.triangles_omp(g))
+    parity = {"tc": T["plain"] == T["tuned"] == Ts == To}
+    for num, den in ((1, 20), (1, 10), (1, 2)):
+        key = f"{num}/{den}"
+        cpu["serial"][key], rs = _cpu_timed(lambda: ref.batch_peel(g, num, den, use_omp=False))
+        cpu["omp"][key], ro = _cpu_timed(lambda: ref.batch_peel(g, num, den, use_omp=True))
+        ok = rs.ok and ro.ok and _peel_key(rs) == _peel_key(ro) and np.array_equal(rs.removed_round, ro.removed_round)
+        for name in ("plain", "tuned"):
+            r = gpu[(key, name)]
+            ok &= _peel_key(r) == _peel_key(rs) and np.array_equal(r.removed_round, rs.removed_round)
+        parity[f"peel_{key}"] = bool(ok)
+        out["peel_ms"][key]["result"] = list(_peel_key(rs))
     tot = {k: out["tc_ms"][k] + sum(v[k] for v in out["peel_ms"].values()) for k in ("plain", "tuned")}
-    line = {"workload": "hk1.7M_tc_peel", "metric": "TC + batch peel (3 eps) ms, plain vs autotuned graph-captured",
-            "value": tot["tuned"], "unit": "ms", "higher_is_better": False, "plain_ms": tot["plain"],
-            "speedup": tot["plain"] / tot["tuned"], "bit_identical": bool(identical), "triangles": T["tuned"],
-            "n": g.n, "m": g.m, **out}
-    print(json.dumps(line), flush=True)
-    return 0 if identical else 1
+    cpu_tot = {k: sum(v.values()) for k, v in cpu.items()}
+    threads = ref.num_threads()
+    out.update({
+        "metric": "TC + batch peel (3 eps) ms, plain vs autotuned graph-captured", "value": tot["tuned"], "unit": "ms",
+        "higher_is_better": False, "plain_ms": tot["plain"], "speedup_vs_plain": tot["plain"] / tot["tuned"],
+        "triangles": T["tuned"],
+        "parity": {"against": "the reference's cpu_batch_peel (serial and OpenMP) and cpu_triangles_serial, every "
+                              "PeelResult field and the whole removed_round", **parity,
+                   "all": all(parity.values())},
+        "cpu_baseline": {"value": cpu_tot["omp"], "unit": "ms", "cores": threads, "kind": "reference",
+                         "sample": "whole graph: cpu_triangles_omp + cpu_batch_peel(OpenMP) at eps 1/20, 1/10, 1/2 "
+                                   "(graph.h:123, densest.h:138)", "per_call_ms": cpu["omp"]},
+        "cpu_serial": {"value": cpu_tot["serial"], "unit": "ms", "cores": 1, "kind": "reference",
+                       "sample": "whole graph: cpu_triangles_serial + cpu_batch_peel(serial) at the same eps "
+                                 "(graph.h:110, densest.h:138)", "per_call_ms": cpu["serial"]},
+        "speedup_vs_cpu_omp": cpu_tot["omp"] / tot["tuned"], "speedup_vs_cpu_serial": cpu_tot["serial"] / tot["tuned"],
+    })
+    return out
 
 
-def run_rmat22_full(args):
-    """R-MAT scale 22 (34.7M edges): TC, per-edge uint32 supports and the full (k, triangle)-core decomposition;
-    plain launches (one-thread-per-edge kernel, host-driven rounds) vs autotuned + graph-captured."""
+def leg_rmat22(args, g=None) -> dict:
+    """R-MAT scale 22 (34.7M edges): TC, per-edge uint32 supports and the full (k, triangle)-core decomposition.
+    GPU: plain launches (one-thread-per-edge kernel, host-driven rounds) vs autotuned + graph-captured. Parity: every
+    per-edge support against the oracle's for_each_triangle restatement (dsg.h:67-79, OpenMP) and the reference's
+    record (fullsize.json); every core number, kmax and the round count against the oracle's restatement of
+    core_decomp_loop_inc (dsg.h:724-751) and the reference's core_decomposition record (Alg 3, dsg.h:125-166).
+    CPU: cpu_triangles_serial on a bounded row sample and cpu_triangles_omp on the whole graph (the reference's),
+    the oracle's support and core passes."""
     import torch
     import graph_analyzer_b200 as ga
-    g = make_graph(ga, args.scale)
+    from oracle import Oracle, Reference
+    ref, orc = Reference(), Oracle()
+    g = g if g is not None else make_graph(ga, args.scale)
+    b_alg = algorithmic_bytes(g)
     plain = ga.DeviceGraph(g)
     for opt, v in ((ga.OPT_TC_KERNEL, 1), (ga.OPT_LOOP_MODE, 1)):
         plain.set_option(opt, v)
@@ -436,85 +542,184 @@ def run_rmat22_full(args):
     plain.prepare()
     tuned.prepare()
     d_sup = torch.zeros(g.m, dtype=torch.int32, device="cuda")
-    out = {}
+    out = {"workload": f"rmat{args.scale}_tc_esup_cores", "n": g.n, "m": g.m}
+    sup = {}
     for name, d in (("plain", plain), ("tuned", tuned)):
         d.tc_count()
         out[f"tc_ms_{name}"], T = _timed(torch, d.tc_count, args.steps)
         d.support_edges_device(d_sup.data_ptr())
         out[f"esup_ms_{name}"], _ = _timed(torch, lambda: d.support_edges_device(d_sup.data_ptr()), 2)
-    first, _ = _timed(torch, lambda: tuned.core_decomposition(want_core=False))   # lists built here
-    out["first_cores_ms_tuned"] = first
+        sup[name] = d_sup.cpu().numpy().view(np.uint32).copy()
+    out["tuning"] = tuned.tuning()
+    out["first_cores_ms_tuned"], _ = _timed(torch, lambda: tuned.core_decomposition(want_core=False))  # lists
     res = {}
-    for name, d in (("plain", plain), ("tuned", tuned)):
-        out[f"cores_ms_{name}"], res[name] = _timed(torch, lambda: d.core_decomposition(), 1)
-    identical = (res["plain"].kmax == res["tuned"].kmax and res["plain"].rounds == res["tuned"].rounds
-                 and np.array_equal(res["plain"].core, res["tuned"].core))
+    out["cores_ms_tuned_runs"] = []
+    for _ in range(3):
+        ms, res["tuned"] = _timed(torch, lambda: tuned.core_decomposition(), 1)
+        out["cores_ms_tuned_runs"].append(ms)
+    out["cores_ms_tuned"] = min(out["cores_ms_tuned_runs"])
+    out["cores_ms_plain"], res["plain"] = _timed(torch, lambda: plain.core_decomposition(), 1)
     plain.close()
     tuned.close()
-    line = {"workload": f"rmat{args.scale}_tc_esup_cores", "metric": "TC, per-edge supports, (k,triangle)-cores ms",
-            "value": out["tc_ms_tuned"] + out["esup_ms_tuned"] + out["cores_ms_tuned"], "unit": "ms",
-            "higher_is_better": False, "triangles": T, "kmax": res["tuned"].kmax, "rounds": res["tuned"].rounds,
-            "bit_identical": bool(identical), "n": g.n, "m": g.m, **out}
-    print(json.dumps(line), flush=True)
-    return 0 if identical else 1
+    del d_sup
+    # parity: the oracle now, the reference's own records (made offline by tests/golden/make_fullsize.py)
+    cpu = {}
+    cpu["esup_oracle_omp_ms"], (To, sup_o) = _cpu_timed(lambda: orc.edge_support(g, use_omp=True))
+    cpu["cores_oracle_ms"], (core_o, kmax_o, rounds_o) = _cpu_timed(lambda: orc.core_levels_inc(g))
+    parity = {
+        "tc": T == To,
+        "esup_vs_oracle": all(np.array_equal(sup[k], sup_o) for k in sup),
+        "cores_vs_oracle": all((r.kmax, r.rounds) == (kmax_o, rounds_o) and np.array_equal(r.core, core_o)
+                               for r in res.values()),
+    }
+    rec = _fullsize("rmat")
+    if rec and (rec["n"], rec["m"]) == (g.n, g.m) and args.scale == rec["config"]["scale"]:
+        parity["tc_vs_reference_record"] = T == rec["triangles"]
+        parity["esup_vs_reference_record"] = _sha(sup["tuned"]) == rec["edge_support_sha256"]
+        parity["cores_vs_reference_record"] = (_sha(res["tuned"].core) == rec["core_sha256"]
+                                               and res["tuned"].kmax == rec["kmax"])
+    # the reference's counters on this host: OpenMP on the whole graph, serial on a bounded row sample
+    with ref.resident(g) as rg:
+        cpu["tc_omp_ms"], T_omp = _cpu_timed(rg.triangles_omp)
+        parity["tc_vs_reference_omp"] = T_omp == T
+        d = np.diff(g.rowptr.astype(np.int64))
+        per_row = d * d + np.bincount(g.src.astype(np.int64), weights=d[g.col.astype(np.int64)], minlength=g.n)
+        # rows whose serial count takes about 10 s: the OpenMP time x threads x 10 s / (that product) of the work
+        frac = min(1.0, 10.0 / max(1e-3, cpu["tc_omp_ms"] / 1e3 * ref.num_threads()))
+        u1 = min(g.n, int(np.searchsorted(np.cumsum(per_row), frac * per_row.sum())) + 1)
+        cpu["tc_serial_sample_ms"], _ = _cpu_timed(lambda: rg.triangles_serial_rows(0, u1))
+    b_rows = algorithmic_bytes_rows(g, u1)
+    parity["all"] = all(parity.values())
+    out.update({
+        "metric": "TC, per-edge supports, (k,triangle)-cores ms",
+        "value": out["tc_ms_tuned"] + out["esup_ms_tuned"] + out["cores_ms_tuned"], "unit": "ms",
+        "higher_is_better": False, "triangles": T, "kmax": res["tuned"].kmax, "rounds": res["tuned"].rounds,
+        "parity": {"against": "oracle (for_each_triangle supports, core_decomp_loop_inc restated) now, and the "
+                              "reference's for_each_triangle / core_decomposition records", **parity},
+        "cpu_baseline": {"value": b_alg / (cpu["tc_omp_ms"] / 1e3) / 1e9, "unit": "GB/s",
+                         "cores": ref.num_threads(), "kind": "reference",
+                         "sample": f"whole graph, cpu_triangles_omp (graph.h:123): {cpu['tc_omp_ms']:.0f} ms"},
+        "cpu_serial": {"value": b_rows / (cpu["tc_serial_sample_ms"] / 1e3) / 1e9, "unit": "GB/s", "cores": 1,
+                       "kind": "reference",
+                       "sample": f"cpu_triangles_serial's loop (graph.h:110) on rows [0, {u1}) "
+                                 f"({100 * b_rows / b_alg:.1f}% of the algorithmic bytes): "
+                                 f"{cpu['tc_serial_sample_ms']:.0f} ms"},
+        "cpu_oracle": {"esup_omp_ms": cpu["esup_oracle_omp_ms"], "cores_ms": cpu["cores_oracle_ms"],
+                       "cores": ref.num_threads(), "kind": "port",
+                       "sample": "whole graph: or_edge_support_omp, or_core_levels_inc (incidence lists, OpenMP "
+                                 "listing and updates)"},
+    })
+    return out
 
 
-def run_batch(args):
+def leg_batch(args) -> dict:
     """4,096 Holme-Kim graphs (n log-uniform in [64, 262144], mean degree U[4, 32], p U[0.1, 0.7]) packed as one
-    concatenated CSR: TC + eps = 1/10 batch peeling of every graph by one count launch and one graph-captured
-    peeling loop, vs 4,096 plain per-graph launches (one-thread-per-edge count, host-driven rounds)."""
+    concatenated CSR: TC + eps = 1/10 batch peeling of every graph by one count launch and one graph-captured peeling
+    loop, against 4,096 per-graph runs of (a) the same kernels (autotuned count, graph-captured loop per graph) and
+    (b) plain launches (one-thread-per-edge count, host-driven rounds). Parity: every graph's count, PeelResult and
+    removed_round against the reference's records (fullsize.json, fullsize_batch.npz) and, on a sample of graphs, the
+    reference's cpu_triangles_serial + cpu_batch_peel run now on all host threads (the CPU baseline)."""
+    import concurrent.futures as cf
     import torch
     import graph_analyzer_b200 as ga
+    from oracle import Reference
+    ref = Reference()
     G = args.graphs
     t0 = time.time()
     b = ga.gen_holme_kim_batch(G, 64, 262144, 4.0, 32.0, 0.1, 0.7, seed=SEED)
     N, M = int(b.vtx_off[-1]), int(b.edge_off[-1])
     log(f"batch: {G} graphs, N={N} M={M} ({time.time() - t0:.1f} s on the host)")
+    out = {"workload": f"batch{G}_hk_tc_peel", "graphs": G, "N": N, "M": M}
     t0 = time.perf_counter()
     db = ga.DeviceBatch(b)
-    create_ms = (time.perf_counter() - t0) * 1e3
-    # timed without downloading removed_round (N entries), as the per-graph plain runs below
-    first_ms, r0 = _timed(torch, lambda: db.tc_peel(1, 10, want_removed=False))   # autotune + lists + run
-    steps = max(1, args.steps // 2)
-    batch_ms, r = _timed(torch, lambda: db.tc_peel(1, 10, want_removed=False), steps)
-    assert np.array_equal(r.triangles, r0.triangles)
-    db_bytes = db.device_bytes()
+    out["create_ms"] = (time.perf_counter() - t0) * 1e3
+    # timed without downloading removed_round (N entries), as the per-graph runs below
+    out["first_batch_ms"], r0 = _timed(torch, lambda: db.tc_peel(1, 10, want_removed=False))   # autotune, lists, capture
+    out["batch_ms"], r = _timed(torch, lambda: db.tc_peel(1, 10, want_removed=False), max(1, args.steps // 2))
+    full = db.tc_peel(1, 10)                                                  # untimed: with removed_round
+    out["device_bytes"] = db.device_bytes()
+    out["tuning"] = db.tuning()
     db.close()
-    # plain: every graph resident on its own, one count launch and a host-driven peeling loop per graph
+    ok_batch = np.array_equal(r.triangles, r0.triangles) and np.array_equal(full.best_num, r.best_num)
+    parity = {"status_ok": bool(np.all(full.status == 0)), "repeat_identical": bool(ok_batch)}
+    rec = _fullsize("batch")
+    if rec and G == rec["config"]["graphs"] and (N, M) == (rec["N"], rec["M"]):
+        with np.load(os.path.join(ROOT, "tests", "golden", rec["per_graph"])) as z:
+            want = {k: z[k] for k in z.files}
+        parity["vs_reference_record"] = bool(
+            np.array_equal(full.triangles, want["triangles"]) and np.array_equal(full.best_num, want["best_num"])
+            and np.array_equal(full.best_den, want["best_den"]) and np.array_equal(full.best_round, want["best_round"])
+            and np.array_equal(full.rounds, want["rounds"]) and _sha(full.removed_round) == rec["removed_round_sha256"])
     rp = torch.from_numpy(b.rowptr.view(np.int32)).cuda()
     cl = torch.from_numpy(b.col.view(np.int32)).cuda()
-    handles = []
-    for i in range(G):
-        v0, e0 = int(b.vtx_off[i]), int(b.edge_off[i])
-        n, m = int(b.vtx_off[i + 1]) - v0, int(b.edge_off[i + 1]) - e0
-        d = ga.DeviceGraph.from_device(rp.data_ptr() + 4 * (v0 + i), cl.data_ptr() + 4 * e0, n, m)
-        for opt, v in ((ga.OPT_TC_KERNEL, 1), (ga.OPT_LOOP_MODE, 1), (ga.OPT_UPDATE_MODE, 1)):
-            d.set_option(opt, v)
-        d.prepare()
-        handles.append(d)
-    del rp, cl
-    mismatches = 0
 
-    def plain_all():
-        nonlocal mismatches
+    def per_graph_arm(options):
+        handles = []
+        for i in range(G):
+            v0, e0 = int(b.vtx_off[i]), int(b.edge_off[i])
+            n, m = int(b.vtx_off[i + 1]) - v0, int(b.edge_off[i + 1]) - e0
+            d = ga.DeviceGraph.from_device(rp.data_ptr() + 4 * (v0 + i), cl.data_ptr() + 4 * e0, n, m)
+            for opt, v in options:
+                d.set_option(opt, v)
+            d.prepare()
+            handles.append(d)
         mismatches = 0
-        for i, d in enumerate(handles):
-            t = d.tc_count()
-            p = d.batch_peel(1, 10, want_removed=False)
-            if t != r.triangles[i] or _peel_key(p) != (r.best_num[i], r.best_den[i], r.best_round[i], r.rounds[i]):
-                mismatches += 1
-    plain_all()                                                       # warm-up (loop state per graph)
-    plain_ms, _ = _timed(torch, plain_all, 1)
-    for d in handles:
-        d.close()
-    line = {"workload": "batch4096_hk_tc_peel", "metric": "batched vs plain graphs/s (TC + eps=1/10 batch peel)",
-            "value": G / (batch_ms / 1e3), "unit": "graphs/s", "higher_is_better": True,
-            "plain_graphs_per_s": G / (plain_ms / 1e3), "speedup_vs_plain": plain_ms / batch_ms,
-            "batch_ms": batch_ms, "first_batch_ms": first_ms, "create_ms": create_ms, "plain_ms": plain_ms,
-            "graphs": G, "N": N, "M": M, "triangles": int(r.triangles.sum()), "device_bytes": db_bytes,
-            "bit_identical": mismatches == 0, "status_ok": bool(np.all(r.status == 0))}
-    print(json.dumps(line), flush=True)
-    return 0 if mismatches == 0 else 1
+
+        def run_all():
+            nonlocal mismatches
+            mismatches = 0
+            for i, d in enumerate(handles):
+                t = d.tc_count()
+                p = d.batch_peel(1, 10, want_removed=False)
+                if t != full.triangles[i] or _peel_key(p) != (full.best_num[i], full.best_den[i], full.best_round[i],
+                                                              full.rounds[i]):
+                    mismatches += 1
+        run_all()                                  # warm-up: loop state, lists and graph capture per graph
+        ms, _ = _timed(torch, run_all, 1)
+        for d in handles:
+            d.close()
+        return ms, mismatches
+
+    out["per_graph_same_kernels_ms"], mm1 = per_graph_arm([(ga.OPT_LOOP_MODE, 2)])
+    out["per_graph_plain_ms"], mm2 = per_graph_arm([(ga.OPT_TC_KERNEL, 1), (ga.OPT_LOOP_MODE, 1),
+                                                   (ga.OPT_UPDATE_MODE, 1)])
+    del rp, cl
+    parity["per_graph_same_kernels_identical"] = mm1 == 0
+    parity["per_graph_plain_identical"] = mm2 == 0
+    # the reference's CPU code on a sample of graphs (every 16th), all host threads, one graph per thread
+    sample = list(range(0, G, 16))
+    threads = os.cpu_count() or 1
+
+    def one(i):
+        gi = b.graph(i)
+        t = ref.triangles_serial(gi)
+        p = ref.batch_peel(gi, 1, 10)
+        v0, v1 = int(b.vtx_off[i]), int(b.vtx_off[i + 1])
+        return (t == full.triangles[i] and _peel_key(p) == (full.best_num[i], full.best_den[i], full.best_round[i],
+                                                             full.rounds[i])
+                and np.array_equal(p.removed_round, full.removed_round[v0:v1]))
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(threads) as ex:
+        oks = list(ex.map(one, sample))
+    cpu_s = time.perf_counter() - t0
+    parity["sample_vs_reference_now"] = all(oks)
+    parity["all"] = all(parity.values())
+    edges_sample = int(sum(int(b.edge_off[i + 1] - b.edge_off[i]) for i in sample))
+    out.update({
+        "metric": "batched vs plain graphs/s (TC + eps=1/10 batch peel)", "value": G / (out["batch_ms"] / 1e3),
+        "unit": "graphs/s", "higher_is_better": True,
+        "per_graph_same_kernels_graphs_per_s": G / (out["per_graph_same_kernels_ms"] / 1e3),
+        "per_graph_plain_graphs_per_s": G / (out["per_graph_plain_ms"] / 1e3),
+        "speedup_vs_per_graph_same_kernels": out["per_graph_same_kernels_ms"] / out["batch_ms"],
+        "speedup_vs_per_graph_plain": out["per_graph_plain_ms"] / out["batch_ms"],
+        "triangles": int(full.triangles.sum()),
+        "parity": {"against": "the reference's per-graph records (all graphs) and its CPU code now (sample)",
+                   **parity},
+        "cpu_baseline": {"value": len(sample) / cpu_s, "unit": "graphs/s", "cores": threads, "kind": "reference",
+                         "sample": f"every 16th graph ({len(sample)} graphs, {100 * edges_sample / M:.1f}% of the "
+                                   f"edges), cpu_triangles_serial + cpu_batch_peel per graph, one graph per thread"},
+    })
+    return out
 
 
 def _serve_trace(ga, R, rng):
@@ -579,7 +784,7 @@ def _fifo_latency(service_s, arrivals_s):
     return np.array(lat)
 
 
-def run_serve(args):
+def leg_serve(args) -> dict:
     """Serving: open-loop Poisson arrivals (rate swept) into the request loop (admission under a 150 GB HBM budget,
     resident graphs for re-queries, small requests folded into batch launches, 4 + 2 concurrent streams), against
     serial plain launches of the same library (one request at a time: uploaded, counted with the kernel the autotuner
@@ -662,8 +867,36 @@ def run_serve(args):
             "hbm_budget_gb": 150, "slots": args.slots or 4, "burst": burst, "sweep": sweep, "by_class": by_class,
             "bit_identical": bool(identical)}
     holder.close()
+    return line
+
+LEGS = {"hk2": leg_hk2, "rmat22-full": leg_rmat22, "batch": leg_batch, "serve": leg_serve}
+
+
+def run_legs(args, g_rmat=None) -> dict:
+    """Every secondary leg in turn (in the default run, after the headline), each under a wall-time budget and with
+    its failure recorded instead of raised, so that a leg can never cost the headline line."""
+    out, t_start = {}, time.time()
+    for name in args.legs:
+        if time.time() - t_start > args.legs_budget_s:
+            out[name] = {"skipped": f"wall-time budget of {args.legs_budget_s:.0f} s for the secondary legs spent"}
+            continue
+        t0 = time.time()
+        try:
+            out[name] = LEGS[name](args, g_rmat) if name == "rmat22-full" else LEGS[name](args)
+        except Exception as e:   # recorded in the line, never raised
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        out[name]["leg_wall_s"] = time.time() - t0
+        log(f"leg {name}: {out[name]['leg_wall_s']:.1f} s")
+    return out
+
+
+def run_leg(args) -> int:
+    """--workload NAME: one secondary leg as its own JSON line (exit 1 when its parity fails)."""
+    line = LEGS[args.workload](args)
     print(json.dumps(line), flush=True)
-    return 0 if identical else 1
+    par = line.get("parity", {})
+    ok = par.get("all", True) if isinstance(par, dict) else True
+    return 0 if ok and line.get("bit_identical", True) else 1
 
 
 def _write_edge_text(g, path):
@@ -795,20 +1028,19 @@ def main():
     ap.add_argument("--slots", type=int, default=0, help="serve workload: concurrent requests (0 = the default 4)")
     ap.add_argument("--rate-fracs", type=float, nargs="+", default=[0.25, 0.5, 0.75, 0.9],
                     help="serve workload: offered Poisson rates as fractions of the measured burst capacity")
+    ap.add_argument("--legs", nargs="*", choices=list(LEGS), default=list(LEGS),
+                    help="secondary workloads the default (headline) run adds to its line, after the headline "
+                         "(none: --legs with no names)")
+    ap.add_argument("--legs-budget-s", type=float, default=900.0,
+                    help="wall time after which the remaining secondary legs are skipped (recorded as skipped)")
     args = ap.parse_args()
     if args.warmup < 3:
         log("warm-up raised to 3 steps")
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
-    if args.workload == "hk2":
-        return run_hk2(args)
-    if args.workload == "rmat22-full":
-        return run_rmat22_full(args)
-    if args.workload == "batch":
-        return run_batch(args)
-    if args.workload == "serve":
-        return run_serve(args)
+    if args.workload in LEGS:
+        return run_leg(args)
     if args.workload == "reference-gpu":
         return run_reference_gpu(args)
     return run_ours(args)
