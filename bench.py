@@ -633,6 +633,7 @@ def leg_batch(args) -> dict:
     t0 = time.perf_counter()
     db = ga.DeviceBatch(b)
     out["create_ms"] = (time.perf_counter() - t0) * 1e3
+    t_leg = time.time()
     # timed without downloading removed_round (N entries), as the per-graph runs below
     out["first_batch_ms"], r0 = _timed(torch, lambda: db.tc_peel(1, 10, want_removed=False))   # autotune, lists, capture
     out["batch_ms"], r = _timed(torch, lambda: db.tc_peel(1, 10, want_removed=False), max(1, args.steps // 2))
@@ -650,10 +651,12 @@ def leg_batch(args) -> dict:
             np.array_equal(full.triangles, want["triangles"]) and np.array_equal(full.best_num, want["best_num"])
             and np.array_equal(full.best_den, want["best_den"]) and np.array_equal(full.best_round, want["best_round"])
             and np.array_equal(full.rounds, want["rounds"]) and _sha(full.removed_round) == rec["removed_round_sha256"])
+    log(f"batch: one-launch runs and records checked in {time.time() - t_leg:.1f} s")
     rp = torch.from_numpy(b.rowptr.view(np.int32)).cuda()
     cl = torch.from_numpy(b.col.view(np.int32)).cuda()
 
     def per_graph_arm(options):
+        t_arm = time.time()
         handles = []
         for i in range(G):
             v0, e0 = int(b.vtx_off[i]), int(b.edge_off[i])
@@ -674,10 +677,15 @@ def leg_batch(args) -> dict:
                 if t != full.triangles[i] or _peel_key(p) != (full.best_num[i], full.best_den[i], full.best_round[i],
                                                               full.rounds[i]):
                     mismatches += 1
+        log(f"batch per-graph arm {options}: {G} handles prepared in {time.time() - t_arm:.1f} s")
+        t0 = time.time()
         run_all()                                  # warm-up: loop state, lists and graph capture per graph
+        log(f"  warm-up {time.time() - t0:.1f} s")
         ms, _ = _timed(torch, run_all, 1)
+        t0 = time.time()
         for d in handles:
             d.close()
+        log(f"  timed {ms / 1e3:.2f} s, closed in {time.time() - t0:.1f} s")
         return ms, mismatches
 
     out["per_graph_same_kernels_ms"], mm1 = per_graph_arm([(ga.OPT_LOOP_MODE, 2)])
@@ -702,6 +710,7 @@ def leg_batch(args) -> dict:
     with cf.ThreadPoolExecutor(threads) as ex:
         oks = list(ex.map(one, sample))
     cpu_s = time.perf_counter() - t0
+    log(f"batch: reference on {len(sample)} graphs in {cpu_s:.1f} s")
     parity["sample_vs_reference_now"] = all(oks)
     parity["all"] = all(parity.values())
     edges_sample = int(sum(int(b.edge_off[i + 1] - b.edge_off[i]) for i in sample))
