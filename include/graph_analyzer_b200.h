@@ -188,11 +188,12 @@ ga_status ga_tc_count(ga_graph* g, uint64_t* triangles);
 ga_status ga_tc_count_async(ga_graph* g, uint64_t* d_triangles);
 
 /* Sharded count, for counting one graph on several GPUs (no counterpart in the reference, which runs on one GPU):
- * the triangles found by shard `shard` of `nshards` equal parts of the work items (hash kernel) or of the oriented
- * edges (plain kernel, when forced with GA_OPT_TC_KERNEL). The shards of a graph partition its triangles: with the
- * graph resident on every GPU, count one shard per GPU and sum the partial counts (one 8-byte all-reduce). Shards
- * use the hash kernel unless a kernel is forced, so every GPU cuts the same partition. The _async form writes the
- * partial count to device memory on the graph's stream. */
+ * the triangles found by shard `shard` of `nshards` (hash kernel: a range of middle vertices holding about 1/nshards
+ * of the probe work, cut from per-vertex work alone; plain kernel, when forced with GA_OPT_TC_KERNEL: an equal range
+ * of the oriented edges). The cut depends only on the graph, not on this copy's autotuned options, so with the graph
+ * resident on every GPU, count one shard per GPU and sum the partial counts (one 8-byte all-reduce). Shards use the
+ * hash kernel unless a kernel is forced, so every GPU cuts the same partition. The _async form writes the partial
+ * count to device memory on the graph's stream. */
 ga_status ga_tc_count_shard(ga_graph* g, uint32_t shard, uint32_t nshards, uint64_t* partial);
 ga_status ga_tc_count_shard_async(ga_graph* g, uint32_t shard, uint32_t nshards, uint64_t* d_partial);
 
