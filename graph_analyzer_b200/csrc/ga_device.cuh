@@ -106,6 +106,7 @@ struct ga_graph {
     uint32_t* origk = nullptr;    // m: position in col of colk[e]
     uint32_t* in_posk = nullptr;  // m: position in colk of in-edge k's edge u->v (aligned with in_src / in_eid)
 
+    unsigned long long* anchor_work = nullptr;   // n+1: probe work of the anchors below v (cuts shards)
     ga_items light, heavy;        // degree-binned work lists of the hash-probe kernel
     bool index_ready = false;     // src, in-lists, colk / origk / in_posk built
     bool prepared = false;        // ... and the work items for the current light_max_deg / item_work

@@ -182,38 +182,132 @@ __global__ void k_edge_keys(const uint32_t* __restrict__ rowptr, const uint32_t*
 
 constexpr int kOrderWarps = 4, kOrderStage = 1024;   // rows up to kOrderStage entries stage their keys in smem
 
-// One warp per row: every entry's place in the row's (degree, id) order is the number of entries with a smaller key
-// (keys are distinct), counted against the row's keys in shared memory (read by all lanes at once) or, for rows
-// longer than kOrderStage, in global memory. Writes colk/origk at that place and posk[e] = where entry e went.
-__global__ void __launch_bounds__(kOrderWarps * 32) k_order_rows(const uint32_t* __restrict__ rowptr,
-                                                                 const uint32_t* __restrict__ col,
-                                                                 const unsigned long long* __restrict__ key,
-                                                                 uint32_t n, uint32_t* __restrict__ colk,
-                                                                 uint32_t* __restrict__ origk,
-                                                                 uint32_t* __restrict__ posk) {
+// Sorting the rows' keys (degree << 32 | id: distinct, the id is the low word) with the entry positions alongside,
+// in two kernels. Each writes colk/origk in sorted order and posk[e] = where entry e went.
+//
+// k_order_rows_small: rows of at most 8 entries (most rows of a power-law graph), four rows per warp, one per 8-lane
+// group: a bitonic network across the group's registers (xor partners below 8 stay inside the group). Longer rows are
+// appended to `listed` (one atomic per warp) for k_order_rows_listed.
+__global__ void __launch_bounds__(256) k_order_rows_small(const uint32_t* __restrict__ rowptr,
+                                                          const unsigned long long* __restrict__ key, uint32_t n,
+                                                          uint32_t* __restrict__ colk, uint32_t* __restrict__ origk,
+                                                          uint32_t* __restrict__ posk, uint32_t* __restrict__ listed,
+                                                          uint32_t* __restrict__ nlisted) {
+    const uint32_t lane = threadIdx.x & 31, sub = lane & 7;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t t0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x - lane; t0 < (uint64_t)n * 8; t0 += stride) {
+        const uint64_t t = t0 + lane;
+        const uint32_t u = (uint32_t)(t >> 3);
+        uint32_t b = 0, d = 0;
+        if (u < n) {
+            b = rowptr[u];
+            d = rowptr[u + 1] - b;
+        }
+        const bool mine = d >= 1 && d <= 8;   // the whole group agrees (same row)
+        unsigned long long k = mine && sub < d ? key[b + sub] : ~0ull;
+        uint32_t idx = sub;
+#pragma unroll
+        for (uint32_t size = 2; size <= 8; size <<= 1) {
+#pragma unroll
+            for (uint32_t st = size >> 1; st > 0; st >>= 1) {
+                const unsigned long long ok = __shfl_xor_sync(GA_FULL_MASK, k, st);
+                const uint32_t oi = __shfl_xor_sync(GA_FULL_MASK, idx, st);
+                const bool up = (sub & size) == 0, lower = (sub & st) == 0;
+                if (lower == up ? ok < k : ok > k) { k = ok; idx = oi; }
+            }
+        }
+        if (mine && sub < d) {
+            colk[b + sub] = (uint32_t)k;
+            origk[b + sub] = b + idx;
+            posk[b + idx] = b + sub;
+        }
+        const bool longer = u < n && d > 8 && sub == 0;
+        const uint32_t bal = __ballot_sync(GA_FULL_MASK, longer);
+        if (bal) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(nlisted, (uint32_t)__popc(bal));
+            base = __shfl_sync(GA_FULL_MASK, base, 0);
+            if (longer) listed[base + __popc(bal & ((1u << lane) - 1))] = u;
+        }
+    }
+}
+
+// k_order_rows_listed: the rows k_order_rows_small listed, one warp per row. Up to 32 entries: a bitonic network
+// across the warp's registers. Longer: every entry's place is the number of entries with a smaller key, counted
+// against the row's keys staged in the warp's shared memory (read by all lanes at once; rows longer than
+// kOrderStage, rare since d+ is at most sqrt(2m) in this orientation, read them from global memory), four entries
+// per lane per pass over the row.
+__global__ void __launch_bounds__(kOrderWarps * 32) k_order_rows_listed(const uint32_t* __restrict__ rowptr,
+                                                                        const unsigned long long* __restrict__ key,
+                                                                        const uint32_t* __restrict__ listed,
+                                                                        const uint32_t* __restrict__ nlisted,
+                                                                        uint32_t* __restrict__ colk,
+                                                                        uint32_t* __restrict__ origk,
+                                                                        uint32_t* __restrict__ posk) {
     __shared__ unsigned long long s_key[kOrderWarps][kOrderStage];
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t count = *nlisted;
     unsigned long long* sk = s_key[w];
-    for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += nwarps) {
+    for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < count; r += nwarps) {
+        const uint32_t u = listed[r];
         const uint32_t b = rowptr[u], d = rowptr[u + 1] - b;
-        if (d == 0) continue;
+        if (d <= 32) {
+            unsigned long long k = lane < d ? key[b + lane] : ~0ull;
+            uint32_t idx = lane;
+#pragma unroll
+            for (uint32_t size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+                for (uint32_t st = size >> 1; st > 0; st >>= 1) {
+                    const unsigned long long ok = __shfl_xor_sync(GA_FULL_MASK, k, st);
+                    const uint32_t oi = __shfl_xor_sync(GA_FULL_MASK, idx, st);
+                    const bool up = (lane & size) == 0, lower = (lane & st) == 0;
+                    if (lower == up ? ok < k : ok > k) { k = ok; idx = oi; }
+                }
+            }
+            if (lane < d) {
+                colk[b + lane] = (uint32_t)k;
+                origk[b + lane] = b + idx;
+                posk[b + idx] = b + lane;
+            }
+            continue;
+        }
         const bool staged = d <= kOrderStage;
         if (staged) {
             for (uint32_t i = lane; i < d; i += 32) sk[i] = key[b + i];
             __syncwarp();
         }
         const unsigned long long* kr = staged ? sk : key + b;
-        for (uint32_t i = lane; i < d; i += 32) {
-            const unsigned long long ki = kr[i];
-            uint32_t r = 0;
-            for (uint32_t j = 0; j < d; j++) r += kr[j] < ki;
-            colk[b + r] = col[b + i];
-            origk[b + r] = b + i;
-            posk[b + i] = b + r;
+        for (uint32_t i0 = lane; i0 < d; i0 += 128) {
+            unsigned long long kq[4];
+            uint32_t rk[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int q = 0; q < 4; q++) kq[q] = i0 + 32 * q < d ? kr[i0 + 32 * q] : ~0ull;
+            for (uint32_t j = 0; j < d; j++) {
+                const unsigned long long kj = kr[j];
+#pragma unroll
+                for (int q = 0; q < 4; q++) rk[q] += kj < kq[q];
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const uint32_t i = i0 + 32 * q;
+                if (i < d) {
+                    colk[b + rk[q]] = (uint32_t)kq[q];
+                    origk[b + rk[q]] = b + i;
+                    posk[b + i] = b + rk[q];
+                }
+            }
         }
         __syncwarp();
     }
+}
+
+// anchor_work[v] = probe work of the anchors below v (prefix = inclusive scan of the work over in-edges, which are
+// laid out anchor by anchor); anchor_work[n] = the whole work.
+__global__ void k_anchor_work(const uint32_t* __restrict__ in_ptr, const unsigned long long* __restrict__ prefix,
+                              uint32_t n, unsigned long long* __restrict__ anchor_work) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v <= n; v += gridDim.x * blockDim.x)
+        anchor_work[v] = in_ptr[v] ? prefix[in_ptr[v] - 1] : 0ull;
 }
 
 // in_posk[k] = position in colk of in-edge k's edge (its position in col is in_eid[k]).
@@ -443,8 +537,15 @@ static ga_status prepare_index(ga_graph* g) {
         GA_CUDA(pool_malloc((void**)&key, (size_t)m * 8, st));
         GA_CUDA(pool_malloc((void**)&posk, (size_t)m * 4, st));
         k_edge_keys<<<ge, 256, 0, st>>>(g->rowptr, g->col, g->in_ptr, m, key);
-        k_order_rows<<<grid_for((uint64_t)n * 32, kOrderWarps * 32), kOrderWarps * 32, 0, st>>>(
-            g->rowptr, g->col, key, n, g->colk, g->origk, posk);
+        uint32_t* listed = nullptr;   // rows longer than 8, then their count
+        GA_CUDA(pool_malloc((void**)&listed, ((size_t)n + 1) * 4, st));
+        GA_CUDA(cudaMemsetAsync(listed + n, 0, 4, st));
+        k_order_rows_small<<<grid_for((uint64_t)n * 8, 256), 256, 0, st>>>(g->rowptr, key, n, g->colk, g->origk,
+                                                                            posk, listed, listed + n);
+        if (g->max_out_degree > 8)
+            k_order_rows_listed<<<(unsigned)g->sm_count * 6, kOrderWarps * 32, 0, st>>>(
+                g->rowptr, key, listed, listed + n, g->colk, g->origk, posk);
+        cudaFreeAsync(listed, st);
         k_in_posk<<<ge, 256, 0, st>>>(g->in_eid, posk, m, g->in_posk);
         GA_CUDA(cudaGetLastError());
         cudaFreeAsync(key, st);
@@ -474,6 +575,9 @@ static ga_status prepare_items(ga_graph* g) {
         GA_CUDA(cudaGetLastError());
         GA_TRY(scan_impl<unsigned long long>(st, prefix, prefix, m, true));
     }
+    if (!g->anchor_work) GA_TRY(dalloc(g, &g->anchor_work, (size_t)n + 1));
+    k_anchor_work<<<grid_for((uint64_t)n + 1, 256), 256, 0, st>>>(g->in_ptr, prefix, n, g->anchor_work);
+    GA_CUDA(cudaGetLastError());
     uint32_t *cnt_l = nullptr, *cnt_h = nullptr, *off_l = nullptr, *off_h = nullptr;
     GA_CUDA(pool_malloc((void**)&cnt_l, ((size_t)n + 1) * 4, st));
     GA_CUDA(pool_malloc((void**)&cnt_h, ((size_t)n + 1) * 4, st));

@@ -271,8 +271,12 @@ __global__ void __launch_bounds__(256) k_peel_mark(LoopScalars* sc, const uint32
 __global__ void __launch_bounds__(256) k_core_min(LoopScalars* sc, const uint32_t* __restrict__ tri,
                                                   const uint32_t* alive0, const uint32_t* alive1,
                                                   uint8_t* __restrict__ state, const uint32_t* fr0,
-                                                  const uint32_t* fr1) {
-    if (!sc->cont) return;   // the small-round cluster kernel ended the loop in this body
+                                                  const uint32_t* fr1, cudaGraphConditionalHandle handle,
+                                                  int use_handle) {
+    if (!sc->cont) {   // the small-round cluster kernel ended the loop in this body: the WHILE node stops
+        if (use_handle && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(handle, 0);
+        return;
+    }
     const uint32_t p = sc->parity;
     retire_previous(sc, state, (sc->round & 1) ? fr0 : fr1);
     const uint32_t* in = p ? alive1 : alive0;
@@ -621,17 +625,33 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_core_small_rounds(
     __shared__ uint32_t s_wu[32];
     __shared__ unsigned long long s_wl[32];
     __shared__ uint32_t s_min;
-    __shared__ unsigned long long s_work, s_des;
+    __shared__ unsigned long long s_work, s_des, s_counts;
+    __shared__ uint32_t s_hdr[6];   // rank 0's copy of the round state: cont, parity, round, fprev, alive, k
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t tid = cluster.block_rank() * blockDim.x + threadIdx.x;
     const uint32_t nthr = cluster.num_blocks() * blockDim.x;
     const uint32_t gwarp = tid >> 5, nwarps = nthr >> 5;
     volatile LoopScalars* vs = sc;
+    if (tid == 0) {   // the state the grid kernels (or the loop's set-up) left
+        const uint32_t p = vs->parity;
+        s_hdr[0] = vs->cont;
+        s_hdr[1] = p;
+        s_hdr[2] = vs->round;
+        s_hdr[3] = vs->fprev;
+        s_hdr[4] = vs->alive_count[p];
+        s_hdr[5] = vs->kcur;
+    }
+    cluster.sync();
+    const uint32_t* hdr = cluster.map_shared_rank(s_hdr, 0);
     for (;;) {
-        // the round state, written by the previous close (or the grid kernels before this launch)
-        const uint32_t cont = vs->cont, p = vs->parity, round = vs->round, fprev = vs->fprev;
-        const uint32_t na = vs->alive_count[p], kcur = vs->kcur;
-        if (!cont || na > kSmallAlive) break;
+        // every thread takes the round state from rank 0's shared copy (written by the close below before the
+        // cluster barrier), so every decision to stay or leave is the same in all CTAs
+        const uint32_t cont = hdr[0], p = hdr[1], round = hdr[2], fprev = hdr[3], na = hdr[4], kcur = hdr[5];
+        if (!cont) {   // the loop is over: the WHILE node must stop whoever cleared `cont`
+            if (tid == 0) cudaGraphSetConditional(handle, 0);
+            break;
+        }
+        if (na > kSmallAlive) break;
         uint32_t* in = p ? alive1 : alive0;
         uint32_t* outl = p ? alive0 : alive1;
         uint32_t* frontier = (round & 1) ? fr1 : fr0;
@@ -652,6 +672,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_core_small_rounds(
         work = cluster_reduce<unsigned long long, false>(cluster, work, s_wl, &s_work);
         if (work > kSmallWork) break;   // the grid kernels take this round
         // frontier and survivors (k_core_mark), with update items of kSmallChunk entries
+        unsigned long long appended = 0;   // this thread's share: frontier vertices (low word), items (high word)
         for (uint32_t i0 = tid - lane; i0 < na; i0 += nthr) {
             const uint32_t i = i0 + lane;
             const bool valid = i < na;
@@ -673,6 +694,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_core_small_rounds(
                 uint32_t ib = 0;
                 if (lane == 31 && tot) ib = atomicAdd(&sc->nitems, tot);
                 ib = __shfl_sync(GA_FULL_MASK, ib, 31);
+                if (lane == 0) appended += ((unsigned long long)tot << 32) | (uint32_t)__popc(bal);
                 for (uint32_t c = 0; c < nc; c++) {
                     item_x[ib + incl - nc + c] = v;
                     item_c[ib + incl - nc + c] = c;
@@ -688,9 +710,10 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_core_small_rounds(
             }
         }
         __threadfence();
-        cluster.sync();
+        // the round's frontier size and item count, summed over the cluster (the barrier inside also ends the mark)
+        appended = cluster_reduce<unsigned long long, false>(cluster, appended, s_wl, &s_counts);
+        const uint32_t F = (uint32_t)appended, nitems = (uint32_t)(appended >> 32);
         // update (k_frontier_update_list): each destroyed triangle once, by its smallest-id frontier corner
-        const uint32_t nitems = vs->nitems, F = vs->fcount;
         unsigned long long destroyed = 0;
         for (uint32_t it = gwarp; it < nitems; it += nwarps) {
             const uint32_t x = __ldcg(item_x + it);
@@ -738,6 +761,12 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_core_small_rounds(
             const uint32_t c = (status == LS_OK && nalive > 0 && iters <= max_rounds) ? 1u : 0u;
             vs->cont = c;
             if (!c) cudaGraphSetConditional(handle, 0);
+            s_hdr[0] = c;
+            s_hdr[1] = p ^ 1;
+            s_hdr[2] = round + 1;
+            s_hdr[3] = F;
+            s_hdr[4] = __ldcg(&sc->alive_count[p ^ 1]);   // the survivors this round appended (atomics, in L2)
+            s_hdr[5] = k;
             __threadfence();
         }
         cluster.sync();
@@ -980,7 +1009,7 @@ static ga_status enqueue_round(ga_graph* g, cudaStream_t st, cudaGraphConditiona
                                        (const uint2*)L->inc, (const unsigned long long*)L->inc_ptr, h));
         }
         k_core_min<<<L->grid_scan, 256, 0, st>>>(L->sc, L->tri, L->alive[0], L->alive[1], L->state, L->frontier[0],
-                                                 L->frontier[1]);
+                                                 L->frontier[1], h, use_h);
         k_core_mark<<<L->grid_scan, 256, 0, st>>>(L->sc, L->tri, L->state, L->out, L->alive[0], L->alive[1],
                                                   L->frontier[0], L->frontier[1], L->item_x, L->item_c, g->rowptr,
                                                   g->in_ptr, inc_ptr);

@@ -72,6 +72,29 @@ constexpr int kBatchWords = 160;
 template <int MODE>
 constexpr int light_warp_words() { return light_slots<MODE>() * SlotLayout<MODE>::words + kBatchWords; }
 
+// Slots per hash bucket. A table of 2^bits "units" holds 4 * 2^bits slots either way: 2^(bits+1) buckets of 2 slots
+// (counts and lists: one 64-bit shared load per lookup, half the shared-memory traffic of a 4-slot bucket; measured
+// 3.88 vs 4.24 ms on R-MAT 22) or 2^bits buckets of 4 slots (supports, whose slots carry counters: 11.9 vs 12.5 ms).
+template <int MODE>
+constexpr uint32_t bucket_slots() { return counters(MODE) ? 4u : 2u; }
+template <int MODE>
+constexpr uint32_t bucket_shift() { return bucket_slots<MODE>() == 4 ? 0u : 1u; }
+
+// Slots of bucket b that hold x (bit i = slot i); *open when its last slot is empty (a bucket fills its slots in
+// order, so the search for x can stop there).
+template <int MODE>
+__device__ __forceinline__ uint32_t bucket_match(const uint32_t* key, uint32_t b, uint32_t x, bool* open) {
+    if constexpr (bucket_slots<MODE>() == 4) {
+        const uint4 t = reinterpret_cast<const uint4*>(key)[b];
+        *open = t.w == GA_EMPTY;
+        return (t.x == x ? 1u : 0u) | (t.y == x ? 2u : 0u) | (t.z == x ? 4u : 0u) | (t.w == x ? 8u : 0u);
+    } else {
+        const uint2 t = reinterpret_cast<const uint2*>(key)[b];
+        *open = t.y == GA_EMPTY;
+        return (t.x == x ? 1u : 0u) | (t.y == x ? 2u : 0u);
+    }
+}
+
 // Writes the triangle (u lowest, v middle, x highest) into the incidence list of each corner. A list is sized by the
 // counting pass; an entry that would land past its list's end is dropped and counted in *overflow instead.
 template <class CT>
@@ -106,20 +129,19 @@ __device__ __forceinline__ uint32_t probe_one(const uint32_t* __restrict__ col, 
                                               uint32_t bits, bool global, uint32_t vb, uint32_t dv,
                                               uint32_t* s_ecnt, uint32_t anchor, const uint32_t* s_u) {
     if (!global) {
-        // bucketed set: 2^bits buckets of 4 slots; a bucket fills its slots in order, so an empty last slot ends
-        // the search. One 128-bit shared load resolves almost every lookup.
-        const uint4* key4 = reinterpret_cast<const uint4*>(key);
-        const uint32_t mask = (1u << bits) - 1;
-        uint32_t b = hash_slot(x, bits);
+        // bucketed set (bucket_slots<MODE>() slots per bucket); a bucket fills its slots in order, so an empty last
+        // slot ends the search. One shared load resolves almost every lookup.
+        const uint32_t nb = bits + bucket_shift<MODE>(), mask = (1u << nb) - 1;
+        uint32_t b = hash_slot(x, nb);
         for (;;) {
-            const uint4 t = key4[b];
-            const uint32_t m = (t.x == x ? 1u : 0u) | (t.y == x ? 2u : 0u) | (t.z == x ? 4u : 0u) |
-                               (t.w == x ? 8u : 0u);
+            bool open;
+            const uint32_t m = bucket_match<MODE>(key, b, x, &open);
             if (m) {
-                on_hit<MODE, ALIVE, CT>(a, cnt, 4 * b + (__ffs(m) - 1), s_ecnt, owner, e, anchor, x, s_u);
+                on_hit<MODE, ALIVE, CT>(a, cnt, bucket_slots<MODE>() * b + (__ffs(m) - 1), s_ecnt, owner, e, anchor,
+                                        x, s_u);
                 return 1;
             }
-            if (t.w == GA_EMPTY) return 0;
+            if (open) return 0;
             b = (b + 1) & mask;
         }
     }
@@ -170,6 +192,45 @@ __device__ __forceinline__ unsigned long long probe_batch(
     __syncwarp();
     const uint4* __restrict__ col4 = reinterpret_cast<const uint4*>(colk);
     uint32_t owner = 0;
+    if (MODE == TC_COUNT && !global) {
+        // counts in a table: the four lookups of a quad are issued without branches (elements outside the list
+        // still read a bucket, their result is masked), so they overlap; a bucket that is full without a match
+        // (rare at a load of at most 1/4 per bucket) continues in the next buckets afterwards
+        const uint32_t nb = bits + bucket_shift<MODE>(), bmask = (1u << nb) - 1;
+        for (uint32_t p = lane; p < tot; p += 32) {
+            while (s_incl[owner] <= p) owner++;
+            const uint32_t lo = s_rb[owner], span = s_re[owner] - lo;
+            const uint32_t q = (lo >> 2) + (p - (owner ? s_incl[owner - 1] : 0u));
+            const uint4 v = __ldg(col4 + q);
+            const uint32_t off = (q << 2) - lo;   // element i of the quad is in the list iff off + i < span
+            const uint32_t xs[4] = {v.x, v.y, v.z, v.w};
+            uint32_t found = 0, more = 0;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const uint32_t x = xs[i];
+                bool open;
+                const bool m = bucket_match<MODE>(key, hash_slot(x, nb), x, &open) != 0;
+                const bool in = off + i < span;
+                found |= (uint32_t)(in & m) << i;
+                more |= (uint32_t)(in & !m & !open) << i;
+            }
+            hits += __popc(found);
+            while (more) {
+                const int i = __ffs(more) - 1;
+                more &= more - 1;
+                const uint32_t x = xs[i];
+                uint32_t b = hash_slot(x, nb);
+                for (;;) {
+                    b = (b + 1) & bmask;
+                    bool open;
+                    if (bucket_match<MODE>(key, b, x, &open)) { hits++; break; }
+                    if (open) break;
+                }
+            }
+        }
+        __syncwarp();
+        return hits;
+    }
     for (uint32_t p = lane; p < tot; p += 32) {
         while (s_incl[owner] <= p) owner++;
         const uint32_t lo = s_rb[owner], hi = s_re[owner];
@@ -212,13 +273,14 @@ __device__ __forceinline__ uint32_t table_bits(uint32_t dv, uint32_t cap) {
     return (2u << cap) >= dv ? cap : 0;
 }
 
-// Clears 2^bits buckets (4 slots each) and inserts the (alive) members of N+(v): a key takes the first free slot of
-// its bucket, or of the next bucket when all four are taken. tid/nthr cover the cooperating threads.
+// Clears the table's 4 * 2^bits slots and inserts the (alive) members of N+(v): a key takes the first free slot of its
+// bucket, or of the next bucket when all of them are taken. tid/nthr cover the cooperating threads.
 template <int MODE, bool ALIVE, class CT>
 __device__ __forceinline__ void build_table(const uint32_t* __restrict__ col, const TcArgs<CT>& a, uint32_t vb,
                                             uint32_t dv, uint32_t* key, uint32_t* cnt, uint32_t* pos, uint32_t bits,
                                             uint32_t tid, uint32_t nthr, bool sync_block) {
-    const uint32_t S = 4u << bits, mask = (1u << bits) - 1;
+    constexpr uint32_t B = bucket_slots<MODE>();
+    const uint32_t S = 4u << bits, nb = bits + bucket_shift<MODE>(), mask = (1u << nb) - 1;
     for (uint32_t s = tid; s < S; s += nthr) {
         key[s] = GA_EMPTY;
         if (counters(MODE)) cnt[s] = 0;
@@ -227,10 +289,10 @@ __device__ __forceinline__ void build_table(const uint32_t* __restrict__ col, co
     for (uint32_t i = tid; i < dv; i += nthr) {
         const uint32_t x = col[vb + i];
         if (ALIVE && !a.alive[x]) continue;
-        uint32_t b = hash_slot(x, bits), slot = 4 * b;
+        uint32_t b = hash_slot(x, nb), slot = B * b;
         while (atomicCAS(&key[slot], GA_EMPTY, x) != GA_EMPTY) {
             slot++;
-            if ((slot & 3) == 0) { b = (b + 1) & mask; slot = 4 * b; }
+            if ((slot & (B - 1)) == 0) { b = (b + 1) & mask; slot = B * b; }
         }
         if (MODE == TC_ESUP) pos[slot] = i;
     }
@@ -435,29 +497,37 @@ static uint32_t heavy_bits_for(const ga_graph* g, int mode) {
     return std::min(need, cap);
 }
 
-// Item ranges of shard `shard` of `nshards` in both bins (heavy then light, [lo, hi) each, into out[4]): equal parts
-// of each bin's items, every cut moved forward to the next anchor boundary (items are in ascending anchor order), so
-// that an anchor's items all fall into one shard. Items depend only on the graph and the options, not on the order
-// inside an in-list, so every GPU holding the graph cuts the same partition of the anchors - and of the triangles,
-// each counted at its middle vertex.
-__global__ void k_shard_bounds(const uint32_t* __restrict__ hv, uint32_t hcount, const uint32_t* __restrict__ lv,
+// Item ranges of shard `shard` of `nshards` in both bins (heavy then light, [lo, hi) each, into out[4]). A shard is a
+// range of anchors cut by their cumulative probe work (anchor_work[v] = work of the anchors below v): anchor v goes
+// to the shard its work starts in. Per-anchor work depends only on the graph - not on the bin cutoff or item work the
+// autotuner picked for this copy, nor on the order a build left an in-list in - so copies of a graph prepared
+// independently on several GPUs cut the same anchors, and the shards partition the triangles (each is counted at its
+// middle vertex). The items of an anchor range are found by binary search (items are in ascending anchor order).
+__global__ void k_shard_bounds(const unsigned long long* __restrict__ anchor_work, uint32_t n,
+                               const uint32_t* __restrict__ hv, uint32_t hcount, const uint32_t* __restrict__ lv,
                                uint32_t lcount, uint32_t shard, uint32_t nshards, uint32_t* __restrict__ out) {
     const uint32_t t = threadIdx.x;   // 4 threads: heavy lo, heavy hi, light lo, light hi
     if (t >= 4) return;
-    const uint32_t* v = t < 2 ? hv : lv;
-    const uint32_t count = t < 2 ? hcount : lcount;
     const uint32_t part = shard + (t & 1);
-    uint32_t cut = (uint32_t)((uint64_t)count * part / nshards);
-    if (cut > 0 && cut < count) {   // first item after `cut - 1` whose anchor differs: binary search (v ascending)
-        const uint32_t a = v[cut - 1];
-        uint32_t lo = cut, hi = count;
+    uint32_t first = n;               // first anchor of shard `part` (n for the end)
+    if (part < nshards) {
+        const unsigned long long W = anchor_work[n];
+        const unsigned long long goal = (W * part + nshards - 1) / nshards;   // ceil(W * part / nshards)
+        uint32_t lo = 0, hi = n;      // first v with anchor_work[v] >= goal
         while (lo < hi) {
             const uint32_t mid = lo + ((hi - lo) >> 1);
-            if (v[mid] <= a) lo = mid + 1; else hi = mid;
+            if (anchor_work[mid] < goal) lo = mid + 1; else hi = mid;
         }
-        cut = lo;
+        first = part == 0 ? 0u : lo;
     }
-    out[t] = cut;
+    const uint32_t* v = t < 2 ? hv : lv;
+    const uint32_t count = t < 2 ? hcount : lcount;
+    uint32_t lo = 0, hi = count;      // first item whose anchor is >= first
+    while (lo < hi) {
+        const uint32_t mid = lo + ((hi - lo) >> 1);
+        if (v[mid] < first) lo = mid + 1; else hi = mid;
+    }
+    out[t] = lo;
 }
 
 template <int MODE, bool ALIVE, class CT>
@@ -475,8 +545,8 @@ static ga_status launch_hash(ga_graph* g, const TcArgs<CT>& a0) {
     uint64_t want = std::max<uint64_t>(g->heavy.count, (g->light.count + kWarps - 1) / kWarps);
     if (a.nshards > 1) {   // this shard's anchors (cut on the device; the queue counters sit in d_queue[0..1])
         uint32_t* b = g->d_queue + 4;
-        k_shard_bounds<<<1, 32, 0, g->stream>>>(g->heavy.v, g->heavy.count, g->light.v, g->light.count, a.shard,
-                                                a.nshards, b);
+        k_shard_bounds<<<1, 32, 0, g->stream>>>(g->anchor_work, g->n, g->heavy.v, g->heavy.count, g->light.v,
+                                                g->light.count, a.shard, a.nshards, b);
         GA_CUDA(cudaGetLastError());
         bounds = b;
         want = (want + a.nshards - 1) / a.nshards + 1;
@@ -585,7 +655,43 @@ static void tune_cache_store_locked(uint64_t key, const TuneChoice& c) {
     std::fclose(f);
 }
 
+// Degree-distribution signature of g (one small kernel and a sync).
+static ga_status tune_key(ga_graph* g, uint64_t* out) {
+    cudaStream_t st = g->stream;
+    const uint32_t n = g->n;
+    unsigned long long* d_hist = nullptr;
+    GA_CUDA(pool_malloc((void**)&d_hist, 33 * 8, st));
+    unsigned long long hist[33] = {};
+    cudaMemsetAsync(d_hist, 0, 33 * 8, st);
+    k_degree_hist<<<grid_for(n, 256, (unsigned)g->sm_count * 8), 256, 0, st>>>(g->rowptr, n, d_hist);
+    cudaMemcpyAsync(hist, d_hist, 33 * 8, cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(d_hist, st);
+    GA_CUDA(cudaStreamSynchronize(st));
+    uint64_t key = mix64(32 - __builtin_clz(n | 1)) ^ mix64(0x100 + 32 - __builtin_clz(g->m)) ^ mix64(0x5e2);
+    for (int b = 0; b < 33; b++) {
+        const uint64_t q = (hist[b] * 16 + g->m / 2) / g->m;   // sixteenths of the edges
+        key = mix64(key ^ (q << 8) ^ (uint64_t)b);
+    }
+    *out = key;
+    return GA_OK;
+}
+
 ga_status ready(ga_graph* g) {
+    // a signature seen before sets the options before the work items are built, so they are built once
+    if (g->opt_tc_kernel == 0 && !g->tuned_kernel && !g->prepared && g->m) {
+        uint64_t key = 0;
+        GA_TRY(tune_key(g, &key));
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        tune_cache_load_locked();
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            if (!g->light_max_deg_set) g->light_max_deg = it->second.light_max_deg;
+            if (!g->item_work_set) g->item_work = it->second.item_work;
+            g->tuned_kernel = it->second.kernel;
+            g->tune_key = key;
+            g->tune_ms = 0;
+        }
+    }
     GA_TRY(prepare(g));
     if (g->opt_tc_kernel == 0) GA_TRY(autotune(g));
     return GA_OK;
@@ -608,20 +714,8 @@ ga_status autotune(ga_graph* g) {
     cudaStream_t st = g->stream;
     const uint32_t n = g->n;
     if (g->m == 0) { g->tuned_kernel = 2; return GA_OK; }
-    // signature
-    unsigned long long* d_hist = nullptr;
-    GA_CUDA(pool_malloc((void**)&d_hist, 33 * 8, st));
-    unsigned long long hist[33] = {};
-    cudaMemsetAsync(d_hist, 0, 33 * 8, st);
-    k_degree_hist<<<grid_for(n, 256, (unsigned)g->sm_count * 8), 256, 0, st>>>(g->rowptr, n, d_hist);
-    cudaMemcpyAsync(hist, d_hist, 33 * 8, cudaMemcpyDeviceToHost, st);
-    cudaFreeAsync(d_hist, st);
-    GA_CUDA(cudaStreamSynchronize(st));
-    uint64_t key = mix64(32 - __builtin_clz(n | 1)) ^ mix64(0x100 + 32 - __builtin_clz(g->m)) ^ mix64(0x5e2);
-    for (int b = 0; b < 33; b++) {
-        const uint64_t q = (hist[b] * 16 + g->m / 2) / g->m;   // sixteenths of the edges
-        key = mix64(key ^ (q << 8) ^ (uint64_t)b);
-    }
+    uint64_t key = 0;
+    GA_TRY(tune_key(g, &key));
     {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         tune_cache_load_locked();
