@@ -232,11 +232,34 @@ __global__ void __launch_bounds__(256) k_order_rows_small(const uint32_t* __rest
     }
 }
 
-// k_order_rows_listed: the rows k_order_rows_small listed, one warp per row. Up to 32 entries: a bitonic network
-// across the warp's registers. Longer: every entry's place is the number of entries with a smaller key, counted
-// against the row's keys staged in the warp's shared memory (read by all lanes at once; rows longer than
-// kOrderStage, rare since d+ is at most sqrt(2m) in this orientation, read them from global memory), four entries
-// per lane per pass over the row.
+// Bitonic sort of 32 keys across a warp's registers, ascending by lane, the entry index carried along.
+__device__ __forceinline__ void warp_bitonic32(unsigned long long& k, uint32_t& idx, uint32_t lane) {
+#pragma unroll
+    for (uint32_t size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+        for (uint32_t st = size >> 1; st > 0; st >>= 1) {
+            const unsigned long long ok = __shfl_xor_sync(GA_FULL_MASK, k, st);
+            const uint32_t oi = __shfl_xor_sync(GA_FULL_MASK, idx, st);
+            const bool up = (lane & size) == 0, lower = (lane & st) == 0;
+            if (lower == up ? ok < k : ok > k) { k = ok; idx = oi; }
+        }
+    }
+}
+
+// Keys below k in 32 ascending keys.
+__device__ __forceinline__ uint32_t rank_in_run32(const unsigned long long* run, unsigned long long k) {
+    uint32_t pos = 0;
+#pragma unroll
+    for (uint32_t step = 16; step > 0; step >>= 1)
+        if (run[pos + step - 1] < k) pos += step;
+    return pos + (run[pos] < k ? 1u : 0u);
+}
+
+// k_order_rows_listed: the rows k_order_rows_small listed, one warp per row. Up to 32 entries: one bitonic network
+// across the warp's registers. Up to kOrderStage: runs of 32 sorted the same way into the warp's shared memory, then
+// every entry's place = its place in its run + the keys below it in each other run (binary searches). Longer rows
+// (none in R-MAT 22, whose longest oriented row has 685 entries; d+ is at most sqrt(2m) in this orientation): every
+// entry's place is the count of smaller keys in the row, read from global memory.
 __global__ void __launch_bounds__(kOrderWarps * 32) k_order_rows_listed(const uint32_t* __restrict__ rowptr,
                                                                         const unsigned long long* __restrict__ key,
                                                                         const uint32_t* __restrict__ listed,
@@ -245,26 +268,19 @@ __global__ void __launch_bounds__(kOrderWarps * 32) k_order_rows_listed(const ui
                                                                         uint32_t* __restrict__ origk,
                                                                         uint32_t* __restrict__ posk) {
     __shared__ unsigned long long s_key[kOrderWarps][kOrderStage];
+    __shared__ uint16_t s_idx[kOrderWarps][kOrderStage];
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t count = *nlisted;
     unsigned long long* sk = s_key[w];
+    uint16_t* si = s_idx[w];
     for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < count; r += nwarps) {
         const uint32_t u = listed[r];
         const uint32_t b = rowptr[u], d = rowptr[u + 1] - b;
         if (d <= 32) {
             unsigned long long k = lane < d ? key[b + lane] : ~0ull;
             uint32_t idx = lane;
-#pragma unroll
-            for (uint32_t size = 2; size <= 32; size <<= 1) {
-#pragma unroll
-                for (uint32_t st = size >> 1; st > 0; st >>= 1) {
-                    const unsigned long long ok = __shfl_xor_sync(GA_FULL_MASK, k, st);
-                    const uint32_t oi = __shfl_xor_sync(GA_FULL_MASK, idx, st);
-                    const bool up = (lane & size) == 0, lower = (lane & st) == 0;
-                    if (lower == up ? ok < k : ok > k) { k = ok; idx = oi; }
-                }
-            }
+            warp_bitonic32(k, idx, lane);
             if (lane < d) {
                 colk[b + lane] = (uint32_t)k;
                 origk[b + lane] = b + idx;
@@ -272,12 +288,34 @@ __global__ void __launch_bounds__(kOrderWarps * 32) k_order_rows_listed(const ui
             }
             continue;
         }
-        const bool staged = d <= kOrderStage;
-        if (staged) {
-            for (uint32_t i = lane; i < d; i += 32) sk[i] = key[b + i];
+        if (d <= kOrderStage) {
+            const uint32_t runs = (d + 31) >> 5;   // the last run is padded with keys above every real key
+            for (uint32_t c = 0; c < runs; c++) {
+                const uint32_t i = (c << 5) + lane;
+                unsigned long long k = i < d ? key[b + i] : ~0ull;
+                uint32_t idx = i;
+                warp_bitonic32(k, idx, lane);
+                sk[(c << 5) + lane] = k;
+                si[(c << 5) + lane] = (uint16_t)idx;
+            }
             __syncwarp();
+            for (uint32_t c = 0; c < runs; c++) {
+                const uint32_t at = (c << 5) + lane;
+                if (at < d) {   // the padding sorts to the end of the last run
+                    const unsigned long long k = sk[at];
+                    const uint32_t idx = si[at];
+                    uint32_t place = lane;
+                    for (uint32_t c2 = 0; c2 < runs; c2++)
+                        if (c2 != c) place += rank_in_run32(sk + (c2 << 5), k);
+                    colk[b + place] = (uint32_t)k;
+                    origk[b + place] = b + idx;
+                    posk[b + idx] = b + place;
+                }
+            }
+            __syncwarp();
+            continue;
         }
-        const unsigned long long* kr = staged ? sk : key + b;
+        const unsigned long long* kr = key + b;
         for (uint32_t i0 = lane; i0 < d; i0 += 128) {
             unsigned long long kq[4];
             uint32_t rk[4] = {0, 0, 0, 0};
@@ -298,7 +336,6 @@ __global__ void __launch_bounds__(kOrderWarps * 32) k_order_rows_listed(const ui
                 }
             }
         }
-        __syncwarp();
     }
 }
 

@@ -583,38 +583,75 @@ constexpr uint32_t kSmallAlive = 1u << 16;   // alive vertices up to which a rou
 constexpr uint32_t kSmallWork = 1u << 17;    // incidence entries a round may destroy in the cluster
 constexpr uint32_t kSmallChunk = 64;         // incidence entries per update item of the cluster
 
-// Cluster-wide sum / minimum of one value per thread: the CTA reduces through its warps into its own `slot`, and after
-// the cluster barrier every thread combines the slots of all CTAs (distributed shared memory reads).
-template <class T, bool MIN>
-__device__ __forceinline__ T cluster_reduce(cooperative_groups::cluster_group& cluster, T x, T* warp_part, T* slot) {
-    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const T y = __shfl_xor_sync(GA_FULL_MASK, x, o);
-        x = MIN ? (y < x ? y : x) : x + y;
-    }
-    if (lane == 0) warp_part[w] = x;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        T t = warp_part[0];
-        for (uint32_t i = 1; i < blockDim.x / 32; i++) t = MIN ? (warp_part[i] < t ? warp_part[i] : t) : t + warp_part[i];
-        *slot = t;
-    }
-    cluster.sync();
-    T r = *cluster.map_shared_rank(slot, 0);
-    for (uint32_t c = 1; c < cluster.num_blocks(); c++) {
-        const T y = *cluster.map_shared_rank(slot, c);
-        r = MIN ? (y < r ? y : r) : r + y;
-    }
+constexpr uint32_t kSmallPer = kSmallAlive / (8 * kSmallThreads);   // alive entries per thread (8-CTA cluster)
+static_assert(kSmallPer * 8 * kSmallThreads == kSmallAlive, "alive entries must split evenly over the threads");
+
+// The round's level and size in one reduction: the minimum triangle count over the alive list, the incidence entries
+// of the vertices at that minimum, and the incidence entries of the vertices at or below the current level.
+struct MinWork {
+    uint32_t mn;
+    unsigned long long at_min, at_level;
+};
+
+__device__ __forceinline__ MinWork combine(const MinWork& a, const MinWork& b) {
+    MinWork r;
+    r.mn = min(a.mn, b.mn);
+    r.at_min = (a.mn == r.mn ? a.at_min : 0ull) + (b.mn == r.mn ? b.at_min : 0ull);
+    r.at_level = a.at_level + b.at_level;
     return r;
 }
 
-// Runs consecutive core rounds (the three grid kernels' work: k_core_min, k_core_mark, k_frontier_update_list and
-// close_round_if_last for LOOP_CORE) inside one cluster while the alive list has at most kSmallAlive vertices and
-// a round destroys at most kSmallWork incidence entries; returns at the first round that is larger (untouched, for
-// the grid kernels), when the loop ends (the WHILE condition is set to 0) or on a device check failure. Every
-// decision to leave is made from values all threads read after the same cluster barrier, so the cluster leaves
-// together. Mutable arrays are read with ld.global.cg (L2): other CTAs of the cluster write them between phases.
+__device__ __forceinline__ MinWork shfl_xor(const MinWork& a, int o) {
+    MinWork r;
+    r.mn = __shfl_xor_sync(GA_FULL_MASK, a.mn, o);
+    r.at_min = __shfl_xor_sync(GA_FULL_MASK, a.at_min, o);
+    r.at_level = __shfl_xor_sync(GA_FULL_MASK, a.at_level, o);
+    return r;
+}
+
+__device__ __forceinline__ MinWork warp_combine(MinWork x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = combine(x, shfl_xor(x, o));
+    return x;
+}
+
+// Cluster-wide MinWork: warps -> the CTA's slot (warp 0 combines the warps' parts), then after the cluster barrier
+// every warp combines the CTAs' slots, one distributed shared memory load per lane.
+__device__ __forceinline__ MinWork cluster_combine(cooperative_groups::cluster_group& cluster, MinWork x,
+                                                   MinWork* part, MinWork* slot) {
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const MinWork none = {0xFFFFFFFFu, 0ull, 0ull};
+    x = warp_combine(x);
+    if (lane == 0) part[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        x = warp_combine(lane < blockDim.x / 32 ? part[lane] : none);
+        if (lane == 0) *slot = x;
+    }
+    cluster.sync();
+    x = lane < cluster.num_blocks() ? *cluster.map_shared_rank(slot, lane) : none;
+    return warp_combine(x);
+}
+
+// Counters of one cluster round, in rank 0's shared memory (two sets, alternating by round).
+struct SmallCounters {
+    uint32_t frontier, items, survivors, pad;
+    unsigned long long destroyed;
+};
+
+// Runs consecutive core rounds (the work of k_core_min, k_core_mark, k_frontier_update_list and close_round_if_last
+// for LOOP_CORE) inside one cluster while the alive list has at most kSmallAlive vertices and a round destroys at
+// most kSmallWork incidence entries; returns at the first round that is larger (untouched, for the grid kernels),
+// when the loop ends (the WHILE condition is set to 0) or at a status other than LS_OK.
+//
+// A round is one pass over the alive list, whose entries (vertex, triangle count, incidence length) each thread
+// keeps in registers from the level's reduction to the mark, and three cluster barriers: after the level reduction,
+// after the mark, after the update. Every thread carries the loop state (level, parity, alive and triangle totals,
+// status) in registers and computes the close itself from the same counters, so every decision to stay or leave is
+// the same in all CTAs; thread 0 of rank 0 writes the state back for the grid kernels. The round's counters live in
+// rank 0's shared memory in two sets by round parity; the set a round uses was last read before the round's first
+// barrier, after which rank 0 clears the other one. Arrays that other CTAs write between phases are read with
+// ld.global.cg (L2).
 __global__ void __launch_bounds__(kSmallThreads, 1) k_core_small_rounds(
     LoopScalars* sc, uint32_t* __restrict__ tri, uint8_t* __restrict__ state, uint32_t* __restrict__ core,
     uint32_t* alive0, uint32_t* alive1, uint32_t* fr0, uint32_t* fr1, uint32_t* __restrict__ item_x,
@@ -622,33 +659,26 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_core_small_rounds(
     cudaGraphConditionalHandle handle) {
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
-    __shared__ uint32_t s_wu[32];
-    __shared__ unsigned long long s_wl[32];
-    __shared__ uint32_t s_min;
-    __shared__ unsigned long long s_work, s_des, s_counts;
-    __shared__ uint32_t s_hdr[6];   // rank 0's copy of the round state: cont, parity, round, fprev, alive, k
+    __shared__ MinWork s_part[kSmallThreads / 32];
+    __shared__ MinWork s_slot;
+    __shared__ SmallCounters s_cnt[2];
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t tid = cluster.block_rank() * blockDim.x + threadIdx.x;
     const uint32_t nthr = cluster.num_blocks() * blockDim.x;
     const uint32_t gwarp = tid >> 5, nwarps = nthr >> 5;
+    const bool writer = tid == 0;
+    if (threadIdx.x < 2) s_cnt[threadIdx.x] = SmallCounters{0, 0, 0, 0, 0ull};
+    // the state the grid kernels (or the loop's set-up) left; nothing writes it until the first close
     volatile LoopScalars* vs = sc;
-    if (tid == 0) {   // the state the grid kernels (or the loop's set-up) left
-        const uint32_t p = vs->parity;
-        s_hdr[0] = vs->cont;
-        s_hdr[1] = p;
-        s_hdr[2] = vs->round;
-        s_hdr[3] = vs->fprev;
-        s_hdr[4] = vs->alive_count[p];
-        s_hdr[5] = vs->kcur;
-    }
+    uint32_t cont = vs->cont, p = vs->parity, round = vs->round, fprev = vs->fprev, kcur = vs->kcur;
+    uint32_t na = vs->alive_count[vs->parity], status = vs->status, iters = vs->iters;
+    const uint32_t max_rounds = vs->max_rounds;
+    unsigned long long nalive = vs->nalive, T = vs->T;
     cluster.sync();
-    const uint32_t* hdr = cluster.map_shared_rank(s_hdr, 0);
+    SmallCounters* cnt0 = cluster.map_shared_rank(s_cnt, 0);
     for (;;) {
-        // every thread takes the round state from rank 0's shared copy (written by the close below before the
-        // cluster barrier), so every decision to stay or leave is the same in all CTAs
-        const uint32_t cont = hdr[0], p = hdr[1], round = hdr[2], fprev = hdr[3], na = hdr[4], kcur = hdr[5];
         if (!cont) {   // the loop is over: the WHILE node must stop whoever cleared `cont`
-            if (tid == 0) cudaGraphSetConditional(handle, 0);
+            if (writer) cudaGraphSetConditional(handle, 0);
             break;
         }
         if (na > kSmallAlive) break;
@@ -656,47 +686,57 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_core_small_rounds(
         uint32_t* outl = p ? alive0 : alive1;
         uint32_t* frontier = (round & 1) ? fr1 : fr0;
         const uint32_t* prev = (round & 1) ? fr0 : fr1;
+        SmallCounters* cnt = cnt0 + (round & 1);
         // retire the previous round's frontier (the grid kernels do it again if they take this round: idempotent)
         for (uint32_t i = tid; i < fprev; i += nthr) state[__ldcg(prev + i)] = 0;
-        // k = max(k, min over alive of tri)
-        uint32_t mn = 0xFFFFFFFFu;
-        for (uint32_t i = tid; i < na; i += nthr) mn = min(mn, __ldcg(tri + __ldcg(in + i)));
-        mn = cluster_reduce<uint32_t, true>(cluster, mn, s_wu, &s_min);
-        const uint32_t k = max(kcur, mn);
-        // the round's size: incidence entries of the frontier {alive v : tri[v] <= k}
-        unsigned long long work = 0;
-        for (uint32_t i = tid; i < na; i += nthr) {
-            const uint32_t v = __ldcg(in + i);
-            if (__ldcg(tri + v) <= k) work += inc_ptr[v + 1] - inc_ptr[v];
+        // this thread's alive entries, all loads in flight together
+        uint32_t v[kSmallPer], t[kSmallPer], d[kSmallPer];
+#pragma unroll
+        for (uint32_t j = 0; j < kSmallPer; j++) {
+            const uint32_t i = tid + j * nthr;
+            v[j] = i < na ? __ldcg(in + i) : 0u;
         }
-        work = cluster_reduce<unsigned long long, false>(cluster, work, s_wl, &s_work);
+#pragma unroll
+        for (uint32_t j = 0; j < kSmallPer; j++) {
+            const bool valid = tid + j * nthr < na;
+            t[j] = valid ? __ldcg(tri + v[j]) : 0xFFFFFFFFu;
+            d[j] = valid ? (uint32_t)(inc_ptr[v[j] + 1] - inc_ptr[v[j]]) : 0u;
+        }
+        // k = max(k, min over alive of tri); the round's size = incidence entries of {alive v : tri[v] <= k}
+        MinWork mw = {0xFFFFFFFFu, 0ull, 0ull};
+#pragma unroll
+        for (uint32_t j = 0; j < kSmallPer; j++) {
+            mw = combine(mw, MinWork{t[j], d[j], t[j] <= kcur ? d[j] : 0u});
+        }
+        mw = cluster_combine(cluster, mw, s_part, &s_slot);
+        const uint32_t k = max(kcur, mw.mn);
+        const unsigned long long work = mw.mn >= kcur ? mw.at_min : mw.at_level;
         if (work > kSmallWork) break;   // the grid kernels take this round
+        if (writer) cnt0[(round & 1) ^ 1] = SmallCounters{0, 0, 0, 0, 0ull};   // the next round's set
         // frontier and survivors (k_core_mark), with update items of kSmallChunk entries
-        unsigned long long appended = 0;   // this thread's share: frontier vertices (low word), items (high word)
-        for (uint32_t i0 = tid - lane; i0 < na; i0 += nthr) {
-            const uint32_t i = i0 + lane;
-            const bool valid = i < na;
-            const uint32_t v = valid ? __ldcg(in + i) : 0;
-            const bool rem = valid && __ldcg(tri + v) <= k;
+#pragma unroll
+        for (uint32_t j = 0; j < kSmallPer; j++) {
+            if (tid - lane + j * nthr >= na) break;   // the warp's entries of this slice are all past the list
+            const bool valid = tid + j * nthr < na;
+            const bool rem = valid && t[j] <= k;
             if (rem) {
-                state[v] = 2;
-                core[v] = k;
+                state[v[j]] = 2;
+                core[v[j]] = k;
             }
             uint32_t bal = __ballot_sync(GA_FULL_MASK, rem);
             if (bal) {
                 uint32_t base = 0;
-                if (lane == 0) base = atomicAdd(&sc->fcount, (uint32_t)__popc(bal));
+                if (lane == 0) base = atomicAdd(&cnt->frontier, (uint32_t)__popc(bal));
                 base = __shfl_sync(GA_FULL_MASK, base, 0);
-                const uint32_t nc = rem ? (uint32_t)((inc_ptr[v + 1] - inc_ptr[v] + kSmallChunk - 1) / kSmallChunk) : 0;
-                if (rem) frontier[base + __popc(bal & ((1u << lane) - 1))] = v;
+                const uint32_t nc = rem ? (uint32_t)(((unsigned long long)d[j] + kSmallChunk - 1) / kSmallChunk) : 0u;
+                if (rem) frontier[base + __popc(bal & ((1u << lane) - 1))] = v[j];
                 const uint32_t incl = warp_incl_scan(nc, lane);
                 const uint32_t tot = __shfl_sync(GA_FULL_MASK, incl, 31);
                 uint32_t ib = 0;
-                if (lane == 31 && tot) ib = atomicAdd(&sc->nitems, tot);
+                if (lane == 31 && tot) ib = atomicAdd(&cnt->items, tot);
                 ib = __shfl_sync(GA_FULL_MASK, ib, 31);
-                if (lane == 0) appended += ((unsigned long long)tot << 32) | (uint32_t)__popc(bal);
                 for (uint32_t c = 0; c < nc; c++) {
-                    item_x[ib + incl - nc + c] = v;
+                    item_x[ib + incl - nc + c] = v[j];
                     item_c[ib + incl - nc + c] = c;
                 }
             }
@@ -704,15 +744,14 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_core_small_rounds(
             bal = __ballot_sync(GA_FULL_MASK, keep);
             if (bal) {
                 uint32_t base = 0;
-                if (lane == 0) base = atomicAdd(&sc->alive_count[p ^ 1], (uint32_t)__popc(bal));
+                if (lane == 0) base = atomicAdd(&cnt->survivors, (uint32_t)__popc(bal));
                 base = __shfl_sync(GA_FULL_MASK, base, 0);
-                if (keep) outl[base + __popc(bal & ((1u << lane) - 1))] = v;
+                if (keep) outl[base + __popc(bal & ((1u << lane) - 1))] = v[j];
             }
         }
         __threadfence();
-        // the round's frontier size and item count, summed over the cluster (the barrier inside also ends the mark)
-        appended = cluster_reduce<unsigned long long, false>(cluster, appended, s_wl, &s_counts);
-        const uint32_t F = (uint32_t)appended, nitems = (uint32_t)(appended >> 32);
+        cluster.sync();
+        const uint32_t F = cnt->frontier, nitems = cnt->items;
         // update (k_frontier_update_list): each destroyed triangle once, by its smallest-id frontier corner
         unsigned long long destroyed = 0;
         for (uint32_t it = gwarp; it < nitems; it += nwarps) {
@@ -729,47 +768,43 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_core_small_rounds(
                 if (sw == 1) atomicSub(&tri[yw.y], 1u);
             }
         }
-        destroyed = cluster_reduce<unsigned long long, false>(cluster, destroyed, s_wl, &s_des);
-        // close (close_round_if_last for LOOP_CORE, one thread)
-        if (tid == 0) {
-            uint32_t status = vs->status;
-            unsigned long long nalive = vs->nalive, T = vs->T;
-            if (F == 0 && nalive > 0) status = LS_NO_PROGRESS;
-            if (F > nalive) status = LS_OVER_REMOVED;
-            if (destroyed > T) status = LS_OVER_REMOVED;
-            if (k < kcur) status = LS_LEVEL_DOWN;
-            nalive -= min((unsigned long long)F, nalive);
-            T -= min(destroyed, T);
-            const uint32_t iters = vs->iters + 1, max_rounds = vs->max_rounds;
+        destroyed = warp_sum_u64(destroyed);
+        if (lane == 0 && destroyed) atomicAdd(&cnt->destroyed, destroyed);
+        __threadfence();
+        cluster.sync();
+        // close (close_round_if_last for LOOP_CORE), the same in every thread
+        const unsigned long long des = cnt->destroyed;
+        const uint32_t survivors = cnt->survivors;
+        if (F == 0 && nalive > 0) status = LS_NO_PROGRESS;
+        if (F > nalive) status = LS_OVER_REMOVED;
+        if (des > T) status = LS_OVER_REMOVED;
+        if (k < kcur) status = LS_LEVEL_DOWN;
+        nalive -= min((unsigned long long)F, nalive);
+        T -= min(des, T);
+        iters++;
+        if (iters > max_rounds + 1) status = LS_ROUND_LIMIT;   // count_iteration's bound
+        if (status == LS_OK && nalive > 0 && round + 1 >= max_rounds) status = LS_ROUND_LIMIT;
+        cont = (status == LS_OK && nalive > 0 && iters <= max_rounds) ? 1u : 0u;
+        if (writer) {   // the state the grid kernels read (their counters are untouched by the cluster: zero)
             vs->nalive = nalive;
             vs->T = T;
             vs->kcur = k;
             vs->kround = k;
             vs->round = round + 1;
             vs->parity = p ^ 1;
-            vs->alive_count[p] = 0;   // the list this round read is the next round's output
+            vs->alive_count[p] = 0;
+            vs->alive_count[p ^ 1] = survivors;
             vs->fprev = F;
-            vs->fcount = 0;
-            vs->nitems = 0;
-            vs->destroyed = 0;
-            vs->done_blocks = 0;
-            vs->min_tri = 0xFFFFFFFFu;
             vs->iters = iters;
-            if (iters > max_rounds + 1) status = LS_ROUND_LIMIT;   // count_iteration's bound
-            if (status == LS_OK && nalive > 0 && round + 1 >= max_rounds) status = LS_ROUND_LIMIT;
             vs->status = status;
-            const uint32_t c = (status == LS_OK && nalive > 0 && iters <= max_rounds) ? 1u : 0u;
-            vs->cont = c;
-            if (!c) cudaGraphSetConditional(handle, 0);
-            s_hdr[0] = c;
-            s_hdr[1] = p ^ 1;
-            s_hdr[2] = round + 1;
-            s_hdr[3] = F;
-            s_hdr[4] = __ldcg(&sc->alive_count[p ^ 1]);   // the survivors this round appended (atomics, in L2)
-            s_hdr[5] = k;
-            __threadfence();
+            vs->cont = cont;
+            if (!cont) cudaGraphSetConditional(handle, 0);
         }
-        cluster.sync();
+        kcur = k;
+        round++;
+        p ^= 1;
+        fprev = F;
+        na = survivors;
     }
     cluster.sync();   // no CTA leaves while another may still read its shared memory
 }

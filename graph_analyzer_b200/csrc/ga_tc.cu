@@ -49,9 +49,9 @@ namespace ga {
 
 constexpr int kWarps = 8;                 // warps per block of the hash kernel
 constexpr int kThreads = kWarps * 32;
-// Per-warp hash set of the light bin: 128 buckets of 4 slots for counts and lists; 64 buckets in the support modes,
-// whose slots carry counters too (2-3 words each): the smaller set keeps 7-8 blocks resident per SM instead of 4
-// (an anchor of up to 128 out-neighbours then has up to 2 keys per bucket).
+// Per-warp hash set of the light bin: 512 slots for counts and lists; 256 in the support modes, whose slots carry
+// counters too (2-3 words each): the smaller set keeps 7-8 blocks resident per SM instead of 4 (an anchor of up to
+// 128 out-neighbours then has up to 2 keys per 4-slot bucket).
 template <int MODE>
 constexpr int light_slots() { return (MODE == TC_VSUP || MODE == TC_ESUP) ? 256 : 512; }
 template <int MODE>
@@ -80,18 +80,30 @@ constexpr uint32_t bucket_slots() { return counters(MODE) ? 4u : 2u; }
 template <int MODE>
 constexpr uint32_t bucket_shift() { return bucket_slots<MODE>() == 4 ? 0u : 1u; }
 
-// Slots of bucket b that hold x (bit i = slot i); *open when its last slot is empty (a bucket fills its slots in
-// order, so the search for x can stop there).
+// Table slots hold vertex ids below kTabEmpty (the hash kernel takes graphs of at most kTabEmpty vertices; larger
+// ones count with the merge kernel). A bucket fills its slots in order, so a search can stop at a bucket whose last
+// slot is free. 2-slot buckets (counts, lists) are full often enough at a load of 1/2 key per bucket (about 9 % of
+// them) that a miss would go on to the next bucket for every tenth probe; there a key that found its bucket full while
+// the table was built set kTabSpill in the last slot of every bucket it passed, and a search goes past a bucket only
+// when that flag is set (R-MAT 22: count 3.55 vs 3.88 ms). 4-slot buckets are rarely full, and the flag's masking
+// costs more than it saves there (supports 12.2 vs 11.5 ms), so they keep the free-slot rule alone.
+constexpr uint32_t kTabEmpty = 0x7FFFFFFFu, kTabSpill = 0x80000000u;
+
+template <int MODE>
+constexpr bool spill_flags() { return bucket_slots<MODE>() == 2; }
+static_assert(!spill_flags<TC_VSUP>() && !spill_flags<TC_ESUP>(), "flush_table reads the support modes' keys as ids");
+
+// Slots of bucket b that hold x (bit i = slot i); *open when the search for x ends at this bucket.
 template <int MODE>
 __device__ __forceinline__ uint32_t bucket_match(const uint32_t* key, uint32_t b, uint32_t x, bool* open) {
     if constexpr (bucket_slots<MODE>() == 4) {
         const uint4 t = reinterpret_cast<const uint4*>(key)[b];
-        *open = t.w == GA_EMPTY;
+        *open = t.w == kTabEmpty;
         return (t.x == x ? 1u : 0u) | (t.y == x ? 2u : 0u) | (t.z == x ? 4u : 0u) | (t.w == x ? 8u : 0u);
     } else {
         const uint2 t = reinterpret_cast<const uint2*>(key)[b];
-        *open = t.y == GA_EMPTY;
-        return (t.x == x ? 1u : 0u) | (t.y == x ? 2u : 0u);
+        *open = (t.y & kTabSpill) == 0;
+        return (t.x == x ? 1u : 0u) | ((t.y & ~kTabSpill) == x ? 2u : 0u);
     }
 }
 
@@ -274,7 +286,8 @@ __device__ __forceinline__ uint32_t table_bits(uint32_t dv, uint32_t cap) {
 }
 
 // Clears the table's 4 * 2^bits slots and inserts the (alive) members of N+(v): a key takes the first free slot of its
-// bucket, or of the next bucket when all of them are taken. tid/nthr cover the cooperating threads.
+// bucket, or moves on to the next bucket when all of them are taken, flagging the full one where the mode keeps spill
+// flags (kTabSpill in its last slot, which holds a key by then). tid/nthr cover the cooperating threads.
 template <int MODE, bool ALIVE, class CT>
 __device__ __forceinline__ void build_table(const uint32_t* __restrict__ col, const TcArgs<CT>& a, uint32_t vb,
                                             uint32_t dv, uint32_t* key, uint32_t* cnt, uint32_t* pos, uint32_t bits,
@@ -282,7 +295,7 @@ __device__ __forceinline__ void build_table(const uint32_t* __restrict__ col, co
     constexpr uint32_t B = bucket_slots<MODE>();
     const uint32_t S = 4u << bits, nb = bits + bucket_shift<MODE>(), mask = (1u << nb) - 1;
     for (uint32_t s = tid; s < S; s += nthr) {
-        key[s] = GA_EMPTY;
+        key[s] = kTabEmpty;
         if (counters(MODE)) cnt[s] = 0;
     }
     if (sync_block) __syncthreads(); else __syncwarp();
@@ -290,9 +303,13 @@ __device__ __forceinline__ void build_table(const uint32_t* __restrict__ col, co
         const uint32_t x = col[vb + i];
         if (ALIVE && !a.alive[x]) continue;
         uint32_t b = hash_slot(x, nb), slot = B * b;
-        while (atomicCAS(&key[slot], GA_EMPTY, x) != GA_EMPTY) {
+        while (atomicCAS(&key[slot], kTabEmpty, x) != kTabEmpty) {
             slot++;
-            if ((slot & (B - 1)) == 0) { b = (b + 1) & mask; slot = B * b; }
+            if ((slot & (B - 1)) == 0) {
+                if (spill_flags<MODE>()) atomicOr(&key[slot - 1], kTabSpill);
+                b = (b + 1) & mask;
+                slot = B * b;
+            }
         }
         if (MODE == TC_ESUP) pos[slot] = i;
     }
@@ -309,7 +326,7 @@ __device__ __forceinline__ void flush_table(const TcArgs<CT>& a, uint32_t vb, co
     for (uint32_t s = tid; s < S; s += nthr) {
         const uint32_t c = cnt[s];
         if (c) {
-            if (MODE == TC_VSUP) atomicAdd(&a.vsup[key[s]], (CT)c);
+            if (MODE == TC_VSUP) atomicAdd(&a.vsup[key[s]], (CT)c);   // 4-slot buckets: no spill flags
             else atomicAdd(&a.esup[vb + pos[s]], c);
         }
     }
@@ -590,8 +607,9 @@ ga_status run_tc(ga_graph* g, const TcArgs<CT>& a, bool zero_outputs) {
     // Holme-Kim 1.7M graph: 154 ms plain vs 4 ms hash; first peel of the 4,096-graph batch: 3.2 s vs 1.1 s)
     // A sharded count always uses the hash kernel unless one is forced: every GPU must cut the same partition, and
     // an autotuned choice could differ between GPUs.
-    const int64_t kernel = g->opt_tc_kernel ? g->opt_tc_kernel
-                                            : (MODE == TC_COUNT && a.nshards <= 1 ? g->tuned_kernel : 2);
+    int64_t kernel = g->opt_tc_kernel ? g->opt_tc_kernel
+                                      : (MODE == TC_COUNT && a.nshards <= 1 ? g->tuned_kernel : 2);
+    if (g->n > kTabEmpty) kernel = 1;   // ids of kTabEmpty and above do not fit the hash kernel's table slots
     if (kernel == 1) return launch_plain<MODE, ALIVE, CT>(g, a);
     if (g->heavy.count == 0 && g->light.count == 0) return GA_OK;
     return launch_hash<MODE, ALIVE, CT>(g, a);
@@ -714,6 +732,7 @@ ga_status autotune(ga_graph* g) {
     cudaStream_t st = g->stream;
     const uint32_t n = g->n;
     if (g->m == 0) { g->tuned_kernel = 2; return GA_OK; }
+    if (n > kTabEmpty) { g->tuned_kernel = 1; return GA_OK; }   // beyond the hash kernel's ids
     uint64_t key = 0;
     GA_TRY(tune_key(g, &key));
     {

@@ -77,6 +77,45 @@ def test_hub_graphs(ga, oracle, cuda_ok, cfg):
         _check_all(ga, oracle, g, cfg, rng)
 
 
+def _hash_class(ids: np.ndarray, bits: int) -> np.ndarray:
+    """The table bucket of each id at 2^bits buckets (the multiplicative hash of the count kernel's tables)."""
+    return ((ids.astype(np.uint64) * 2654435761) & 0xFFFFFFFF) >> (32 - bits)
+
+
+def _colliding_graph(rng: np.random.Generator, bucket: int) -> tuple[int, np.ndarray]:
+    """An anchor v whose 100 out-neighbours X all hash to one bucket of its table (256 two-slot buckets for 100 keys,
+    so they fill a chain of 50 buckets, wrapping past the last bucket when `bucket` is 255), and 40 in-neighbours
+    whose probe lists mix members of X (hits at every chain position) with 60 ids Y of the same bucket that are not
+    in the table (misses that must walk the whole chain). Fillers give X and Y the higher degree, so v -> x and the
+    lists of u -> v reach them."""
+    n = 1 << 16
+    ids = np.arange(n, dtype=np.int64)
+    cls = ids[_hash_class(ids, 8) == bucket]
+    rng.shuffle(cls)
+    X, Y = cls[:100], cls[100:160]
+    rest = np.setdiff1d(ids, cls)
+    v, U, F = rest[0], rest[1:41], rest[41:241]
+    pairs = [(v, x) for x in X]
+    for u in U:
+        pairs.append((u, v))
+        pairs += [(u, x) for x in rng.choice(X, 30, replace=False)]
+        pairs += [(u, y) for y in rng.choice(Y, 30, replace=False)]
+    pairs += [(f, z) for f in F for z in np.concatenate([X, Y])]
+    return n, np.array(pairs, dtype=np.uint32)
+
+
+@pytest.mark.parametrize("cfg", list(CONFIGS))
+def test_colliding_keys(ga, oracle, cuda_ok, cfg):
+    """Table keys that all land in one bucket: the search must follow the chain of full buckets a key moved along
+    when the table was built (hits anywhere in it, misses to its end), also where it wraps past the last bucket."""
+    rng = np.random.default_rng(5)
+    for bucket in (5, 255):
+        n, raw = _colliding_graph(rng, bucket)
+        g = ga.build_graph_from_edges(n, ga.canonical_edges(raw))
+        assert oracle.triangles_serial(g) == 40 * 30
+        _check_all(ga, oracle, g, cfg, rng)
+
+
 @pytest.mark.parametrize("cfg", list(CONFIGS))
 def test_clique_uses_heavy_bin(ga, oracle, cuda_ok, cfg):
     n = 640                                                       # out-degrees up to 639 > 256: heavy anchors
