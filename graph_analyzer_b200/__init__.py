@@ -35,7 +35,7 @@ __all__ = [
     "canonical_edges", "gen_holme_kim", "gen_rmat", "permute_ids", "density_value", "peel_arith_ok",
     "peel_improves", "gpu_triangles", "gpu_batch_peel", "gpu_core_decomposition", "lib", "device_count",
     "OPT_TC_KERNEL", "OPT_LOOP_MODE", "OPT_MAX_ROUNDS", "OPT_ITEM_WORK", "OPT_HEAVY_TABLE_BITS",
-    "OPT_LIGHT_MAX_DEG", "OPT_UPDATE_MODE", "HostBatch", "DeviceBatch", "BatchPeel", "pack_batch",
+    "OPT_LIGHT_MAX_DEG", "OPT_UPDATE_MODE", "OPT_COUNT_BITMAP", "HostBatch", "DeviceBatch", "BatchPeel", "pack_batch",
     "gen_holme_kim_batch",
 ]
 
@@ -44,6 +44,7 @@ LIB_PATH = os.path.join(_PKG, "_lib", "libga_b200.so")
 
 OPT_TC_KERNEL, OPT_LOOP_MODE, OPT_MAX_ROUNDS, OPT_ITEM_WORK, OPT_HEAVY_TABLE_BITS, OPT_LIGHT_MAX_DEG = 1, 2, 3, 4, 5, 6
 OPT_UPDATE_MODE = 7
+OPT_COUNT_BITMAP = 8
 
 STATUS = {
     0: "GA_OK", 1: "GA_ERR_INVALID_ARGUMENT", 2: "GA_ERR_INVALID_GRAPH", 3: "GA_ERR_CUDA",

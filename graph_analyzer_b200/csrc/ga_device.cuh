@@ -105,10 +105,15 @@ struct ga_graph {
     uint32_t* colk = nullptr;     // m (+4 zero padding, 16-byte aligned like col)
     uint32_t* origk = nullptr;    // m: position in col of colk[e]
     uint32_t* in_posk = nullptr;  // m: position in colk of in-edge k's edge u->v (aligned with in_src / in_eid)
+    // every vertex's place in the (degree, id) order, and colk with each entry replaced by that place: an anchor's
+    // out-neighbours then lie in a short range of places just above the anchor's own (R-MAT 22: within 65,536 for
+    // every anchor of more than 128 out-neighbours), which the count kernel covers with a bitmap
+    uint32_t* vrank = nullptr;    // n
+    uint32_t* colr = nullptr;     // m (+4 zero padding, 16-byte aligned like colk)
 
     unsigned long long* anchor_work = nullptr;   // n+1: probe work of the anchors below v (cuts shards)
     ga_items light, heavy;        // degree-binned work lists of the hash-probe kernel
-    bool index_ready = false;     // src, in-lists, colk / origk / in_posk built
+    bool index_ready = false;     // src, in-lists, colk / origk / in_posk / vrank / colr built
     bool prepared = false;        // ... and the work items for the current light_max_deg / item_work
     ga_loops* loops = nullptr;    // peeling / core loop state, allocated on first use
     // a batch: the graph is the disjoint union of seg_count graphs, graph s owning vertices [seg_off[s], seg_off[s+1])
@@ -121,7 +126,7 @@ struct ga_graph {
     uint32_t* d_queue = nullptr;               // 8 work-queue counters
 
     // options (ga_option)
-    int64_t opt_tc_kernel = 0, opt_loop_mode = 0, opt_max_rounds = 0, opt_update_mode = 0;
+    int64_t opt_tc_kernel = 0, opt_loop_mode = 0, opt_max_rounds = 0, opt_update_mode = 0, opt_count_bitmap = 0;
     int tuned_kernel = 0;          // count kernel chosen by the autotuner (1 plain, 2 hash; 0 not tuned yet)
     uint64_t tune_key = 0;         // degree-distribution signature it was chosen for
     float tune_ms = 0;             // the chosen configuration's count time when it was measured (0: from the cache)

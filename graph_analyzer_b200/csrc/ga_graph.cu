@@ -5,6 +5,7 @@
 //   in_ptr/in_src/in_eid   transpose of the oriented CSR: for every vertex v the edges u->v (source, edge index)
 //   colk/origk/in_posk     every row again in (degree, id) order, where each entry sits in it, and where each
 //                          in-edge u->v sits in u's reordered row (the start of its probe suffix)
+//   vrank/colr             every vertex's place in the (degree, id) order, and colk with entries as places
 //   light / heavy items    degree-binned work lists of the hash-probe kernels: one item = a slice of v's in-edges
 //                          whose probe work (sum of out-degrees of the sources) is bounded; anchors with a large
 //                          out-degree go to the block-wide "heavy" bin, the rest to the per-warp "light" bin.
@@ -232,34 +233,11 @@ __global__ void __launch_bounds__(256) k_order_rows_small(const uint32_t* __rest
     }
 }
 
-// Bitonic sort of 32 keys across a warp's registers, ascending by lane, the entry index carried along.
-__device__ __forceinline__ void warp_bitonic32(unsigned long long& k, uint32_t& idx, uint32_t lane) {
-#pragma unroll
-    for (uint32_t size = 2; size <= 32; size <<= 1) {
-#pragma unroll
-        for (uint32_t st = size >> 1; st > 0; st >>= 1) {
-            const unsigned long long ok = __shfl_xor_sync(GA_FULL_MASK, k, st);
-            const uint32_t oi = __shfl_xor_sync(GA_FULL_MASK, idx, st);
-            const bool up = (lane & size) == 0, lower = (lane & st) == 0;
-            if (lower == up ? ok < k : ok > k) { k = ok; idx = oi; }
-        }
-    }
-}
-
-// Keys below k in 32 ascending keys.
-__device__ __forceinline__ uint32_t rank_in_run32(const unsigned long long* run, unsigned long long k) {
-    uint32_t pos = 0;
-#pragma unroll
-    for (uint32_t step = 16; step > 0; step >>= 1)
-        if (run[pos + step - 1] < k) pos += step;
-    return pos + (run[pos] < k ? 1u : 0u);
-}
-
-// k_order_rows_listed: the rows k_order_rows_small listed, one warp per row. Up to 32 entries: one bitonic network
-// across the warp's registers. Up to kOrderStage: runs of 32 sorted the same way into the warp's shared memory, then
-// every entry's place = its place in its run + the keys below it in each other run (binary searches). Longer rows
-// (none in R-MAT 22, whose longest oriented row has 685 entries; d+ is at most sqrt(2m) in this orientation): every
-// entry's place is the count of smaller keys in the row, read from global memory.
+// k_order_rows_listed: the rows k_order_rows_small listed, one warp per row. Up to 32 entries: a bitonic network
+// across the warp's registers. Longer: every entry's place is the number of entries with a smaller key, counted
+// against the row's keys staged in the warp's shared memory (read by all lanes at once; rows longer than
+// kOrderStage, rare since d+ is at most sqrt(2m) in this orientation, read them from global memory), four entries
+// per lane per pass over the row.
 __global__ void __launch_bounds__(kOrderWarps * 32) k_order_rows_listed(const uint32_t* __restrict__ rowptr,
                                                                         const unsigned long long* __restrict__ key,
                                                                         const uint32_t* __restrict__ listed,
@@ -268,19 +246,26 @@ __global__ void __launch_bounds__(kOrderWarps * 32) k_order_rows_listed(const ui
                                                                         uint32_t* __restrict__ origk,
                                                                         uint32_t* __restrict__ posk) {
     __shared__ unsigned long long s_key[kOrderWarps][kOrderStage];
-    __shared__ uint16_t s_idx[kOrderWarps][kOrderStage];
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t count = *nlisted;
     unsigned long long* sk = s_key[w];
-    uint16_t* si = s_idx[w];
     for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < count; r += nwarps) {
         const uint32_t u = listed[r];
         const uint32_t b = rowptr[u], d = rowptr[u + 1] - b;
         if (d <= 32) {
             unsigned long long k = lane < d ? key[b + lane] : ~0ull;
             uint32_t idx = lane;
-            warp_bitonic32(k, idx, lane);
+#pragma unroll
+            for (uint32_t size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+                for (uint32_t st = size >> 1; st > 0; st >>= 1) {
+                    const unsigned long long ok = __shfl_xor_sync(GA_FULL_MASK, k, st);
+                    const uint32_t oi = __shfl_xor_sync(GA_FULL_MASK, idx, st);
+                    const bool up = (lane & size) == 0, lower = (lane & st) == 0;
+                    if (lower == up ? ok < k : ok > k) { k = ok; idx = oi; }
+                }
+            }
             if (lane < d) {
                 colk[b + lane] = (uint32_t)k;
                 origk[b + lane] = b + idx;
@@ -288,34 +273,12 @@ __global__ void __launch_bounds__(kOrderWarps * 32) k_order_rows_listed(const ui
             }
             continue;
         }
-        if (d <= kOrderStage) {
-            const uint32_t runs = (d + 31) >> 5;   // the last run is padded with keys above every real key
-            for (uint32_t c = 0; c < runs; c++) {
-                const uint32_t i = (c << 5) + lane;
-                unsigned long long k = i < d ? key[b + i] : ~0ull;
-                uint32_t idx = i;
-                warp_bitonic32(k, idx, lane);
-                sk[(c << 5) + lane] = k;
-                si[(c << 5) + lane] = (uint16_t)idx;
-            }
+        const bool staged = d <= kOrderStage;
+        if (staged) {
+            for (uint32_t i = lane; i < d; i += 32) sk[i] = key[b + i];
             __syncwarp();
-            for (uint32_t c = 0; c < runs; c++) {
-                const uint32_t at = (c << 5) + lane;
-                if (at < d) {   // the padding sorts to the end of the last run
-                    const unsigned long long k = sk[at];
-                    const uint32_t idx = si[at];
-                    uint32_t place = lane;
-                    for (uint32_t c2 = 0; c2 < runs; c2++)
-                        if (c2 != c) place += rank_in_run32(sk + (c2 << 5), k);
-                    colk[b + place] = (uint32_t)k;
-                    origk[b + place] = b + idx;
-                    posk[b + idx] = b + place;
-                }
-            }
-            __syncwarp();
-            continue;
         }
-        const unsigned long long* kr = key + b;
+        const unsigned long long* kr = staged ? sk : key + b;
         for (uint32_t i0 = lane; i0 < d; i0 += 128) {
             unsigned long long kq[4];
             uint32_t rk[4] = {0, 0, 0, 0};
@@ -336,7 +299,93 @@ __global__ void __launch_bounds__(kOrderWarps * 32) k_order_rows_listed(const ui
                 }
             }
         }
+        __syncwarp();
     }
+}
+
+// ---- vertex places in the (degree, id) order ---------------------------------------------------------------------
+// A stable LSD radix sort of the vertices by degree (out + in), 9 bits per pass, starting from id order, so that
+// equal degrees stay in id order: the result is the (degree, id) order of graph.h:43-45. Each warp owns a chunk of
+// kRankChunk consecutive entries: k_rank_count counts the chunk's digits, an exclusive scan over (digit, chunk) gives
+// every chunk its start in each digit's range, and k_rank_scatter writes the chunk's entries in order (lanes with the
+// same digit ranked by __match_any_sync, a per-digit running count per warp in shared memory).
+constexpr uint32_t kRankBits = 9, kRankDigits = 1u << kRankBits, kRankChunk = 512, kRankWarps = 8;
+
+__global__ void k_vertex_degree(const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ in_ptr, uint32_t n,
+                                uint32_t* __restrict__ deg, unsigned long long* maxdeg) {
+    uint32_t mx = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const uint32_t d = rowptr[v + 1] - rowptr[v] + in_ptr[v + 1] - in_ptr[v];
+        deg[v] = d;
+        mx = max(mx, d);
+    }
+    mx = __reduce_max_sync(GA_FULL_MASK, mx);
+    if ((threadIdx.x & 31) == 0 && mx) atomicMax(maxdeg, (unsigned long long)mx);
+}
+
+// counts[d * nchunks + c] = entries of chunk c whose digit is d (cur == nullptr: the identity order).
+__global__ void __launch_bounds__(kRankWarps * 32) k_rank_count(const uint32_t* __restrict__ cur,
+                                                                const uint32_t* __restrict__ deg, uint32_t n,
+                                                                uint32_t shift, uint32_t nchunks,
+                                                                uint32_t* __restrict__ counts) {
+    __shared__ uint32_t s_h[kRankWarps][kRankDigits];
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t c = blockIdx.x * kRankWarps + w;
+    if (c >= nchunks) return;   // warp-uniform; no block barrier below
+    uint32_t* h = s_h[w];
+    for (uint32_t d = lane; d < kRankDigits; d += 32) h[d] = 0;
+    __syncwarp();
+    const uint32_t b = c * kRankChunk, e = min(n, b + kRankChunk);
+    for (uint32_t i = b + lane; i < e; i += 32) {
+        const uint32_t x = cur ? cur[i] : i;
+        atomicAdd(&h[(deg[x] >> shift) & (kRankDigits - 1)], 1u);
+    }
+    __syncwarp();
+    for (uint32_t d = lane; d < kRankDigits; d += 32) counts[(size_t)d * nchunks + c] = h[d];
+}
+
+// Writes the chunk's entries to next[] at their digit's place (offs = exclusive scan of counts), in chunk order.
+__global__ void __launch_bounds__(kRankWarps * 32) k_rank_scatter(const uint32_t* __restrict__ cur,
+                                                                  const uint32_t* __restrict__ deg, uint32_t n,
+                                                                  uint32_t shift, uint32_t nchunks,
+                                                                  const uint32_t* __restrict__ offs,
+                                                                  uint32_t* __restrict__ next) {
+    __shared__ uint32_t s_run[kRankWarps][kRankDigits];
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t c = blockIdx.x * kRankWarps + w;
+    if (c >= nchunks) return;   // warp-uniform; no block barrier below
+    uint32_t* run = s_run[w];
+    for (uint32_t d = lane; d < kRankDigits; d += 32) run[d] = 0;
+    __syncwarp();
+    const uint32_t b = c * kRankChunk, e = min(n, b + kRankChunk);
+    for (uint32_t i0 = b; i0 < e; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        const bool valid = i < e;
+        const uint32_t x = valid ? (cur ? cur[i] : i) : 0u;
+        // lanes past the chunk get distinct digits outside the digit range, so they match no one
+        const uint32_t d = valid ? (deg[x] >> shift) & (kRankDigits - 1) : kRankDigits + lane;
+        const uint32_t peers = __match_any_sync(GA_FULL_MASK, d);
+        const uint32_t leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if (lane == leader && valid) base = run[d];
+        base = __shfl_sync(GA_FULL_MASK, base, leader);
+        if (valid) next[offs[(size_t)d * nchunks + c] + base + __popc(peers & ((1u << lane) - 1))] = x;
+        __syncwarp();
+        if (lane == leader && valid) run[d] = base + __popc(peers);
+        __syncwarp();
+    }
+}
+
+// vrank[order[i]] = i.
+__global__ void k_rank_invert(const uint32_t* __restrict__ order, uint32_t n, uint32_t* __restrict__ vrank) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) vrank[order[i]] = i;
+}
+
+// colr[e] = vrank[colk[e]].
+__global__ void k_colr(const uint32_t* __restrict__ colk, const uint32_t* __restrict__ vrank, uint32_t m,
+                       uint32_t* __restrict__ colr) {
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x)
+        colr[e] = vrank[colk[e]];
 }
 
 // anchor_work[v] = probe work of the anchors below v (prefix = inclusive scan of the work over in-edges, which are
@@ -540,7 +589,8 @@ static ga_status prepare_index(ga_graph* g) {
     cudaStream_t st = g->stream;
     const uint32_t n = g->n, m = g->m;
     GA_CUDA(cudaStreamSynchronize(st));
-    for (uint32_t** p : {&g->src, &g->in_ptr, &g->in_src, &g->in_eid, &g->colk, &g->origk, &g->in_posk}) {
+    for (uint32_t** p : {&g->src, &g->in_ptr, &g->in_src, &g->in_eid, &g->colk, &g->origk, &g->in_posk, &g->vrank,
+                         &g->colr}) {
         dfree(g, *p);
         *p = nullptr;
     }
@@ -590,12 +640,59 @@ static ga_status prepare_index(ga_graph* g) {
     }
     cudaFreeAsync(indeg, st);
     cudaFreeAsync(fill, st);
-    unsigned long long herr = 0;
+    // every vertex's degree (out + in) and the largest, which sets the number of radix passes below
+    uint32_t* deg = nullptr;
+    unsigned long long* maxdeg = g->d_scalars + 61;
+    GA_CUDA(cudaMemsetAsync(maxdeg, 0, 8, st));
+    if (n) {
+        GA_CUDA(pool_malloc((void**)&deg, (size_t)n * 4, st));
+        k_vertex_degree<<<gv, 256, 0, st>>>(g->rowptr, g->in_ptr, n, deg, maxdeg);
+        GA_CUDA(cudaGetLastError());
+    }
+    unsigned long long herr = 0, hmax = 0;
     GA_CUDA(cudaMemcpyAsync(&herr, err, 8, cudaMemcpyDeviceToHost, st));
+    GA_CUDA(cudaMemcpyAsync(&hmax, maxdeg, 8, cudaMemcpyDeviceToHost, st));
     GA_CUDA(cudaStreamSynchronize(st));
-    if (herr & 16)
+    if (herr & 16) {
+        cudaFreeAsync(deg, st);
         return fail(GA_ERR_INVALID_GRAPH, "CSR is not oriented by (degree, id) (graph.h:43-45): an edge points from "
                                           "the larger to the smaller endpoint, or an undirected edge is stored twice");
+    }
+    if (n) {   // vertex places in the (degree, id) order, and colk as places
+        GA_TRY(dalloc(g, &g->vrank, n));
+        GA_TRY(dalloc(g, &g->colr, (size_t)m + 4));
+        GA_CUDA(cudaMemsetAsync(g->colr + m, 0, 16, st));
+        const uint32_t nchunks = (uint32_t)(((uint64_t)n + kRankChunk - 1) / kRankChunk);
+        const uint64_t ncounts = (uint64_t)kRankDigits * nchunks;
+        uint32_t *ord0 = nullptr, *ord1 = nullptr, *counts = nullptr;
+        GA_CUDA(pool_malloc((void**)&ord0, (size_t)n * 4, st));
+        GA_CUDA(pool_malloc((void**)&ord1, (size_t)n * 4, st));
+        GA_CUDA(pool_malloc((void**)&counts, ncounts * 4, st));
+        const unsigned gr = (nchunks + kRankWarps - 1) / kRankWarps;
+        const uint32_t* cur = nullptr;   // the identity (id order) before the first pass
+        uint32_t* next = ord0;
+        uint32_t shift = 0;
+        do {
+            k_rank_count<<<gr, kRankWarps * 32, 0, st>>>(cur, deg, n, shift, nchunks, counts);
+            GA_CUDA(cudaGetLastError());
+            GA_TRY(scan_impl<uint32_t>(st, counts, counts, ncounts, false));
+            k_rank_scatter<<<gr, kRankWarps * 32, 0, st>>>(cur, deg, n, shift, nchunks, counts, next);
+            GA_CUDA(cudaGetLastError());
+            cur = next;
+            next = next == ord0 ? ord1 : ord0;
+            shift += kRankBits;
+        } while (shift < 32 && (hmax >> shift) != 0);
+        k_rank_invert<<<gv, 256, 0, st>>>(cur, n, g->vrank);
+        GA_CUDA(cudaGetLastError());
+        if (m) {
+            k_colr<<<ge, 256, 0, st>>>(g->colk, g->vrank, m, g->colr);
+            GA_CUDA(cudaGetLastError());
+        }
+        cudaFreeAsync(ord0, st);
+        cudaFreeAsync(ord1, st);
+        cudaFreeAsync(counts, st);
+        cudaFreeAsync(deg, st);
+    }
     g->index_ready = true;
     return GA_OK;
 }
@@ -822,6 +919,10 @@ ga_status ga_graph_set_option(ga_graph* g, ga_option opt, int64_t value) {
             g->tuned_kernel = 0;
             return GA_OK;
         }
+        case GA_OPT_COUNT_BITMAP:
+            if (value > 1) return fail(GA_ERR_INVALID_ARGUMENT, "GA_OPT_COUNT_BITMAP is 0 or 1");
+            g->opt_count_bitmap = value;
+            return GA_OK;
         case GA_OPT_HEAVY_TABLE_BITS:
             if (value != 0 && (value < 3 || value > 13))
                 return fail(GA_ERR_INVALID_ARGUMENT, "GA_OPT_HEAVY_TABLE_BITS is 0 or 3..13");

@@ -316,6 +316,73 @@ __device__ __forceinline__ void build_table(const uint32_t* __restrict__ col, co
     if (sync_block) __syncthreads(); else __syncwarp();
 }
 
+// Heavy anchors of a count use a bitmap of N+(v) instead of a hash set when it fits the table's shared memory: in the
+// (degree, id) order every out-neighbour of v comes after v, and for the anchors of many out-neighbours (high degree)
+// they lie in a short range of places above v's own (R-MAT 22: under 65,536 places for every anchor of more than 128
+// out-neighbours, against 4.2M vertices). Bit o of the bitmap is set iff the vertex at place base + o is an (alive)
+// out-neighbour of v, base = v's place + 1; span = the largest out-neighbour's place - v's place bounds o. A probe is
+// then one shared 32-bit load and a bit test, with no collisions and nothing to continue.
+template <bool ALIVE, class CT>
+__device__ __forceinline__ void build_bitmap(const uint32_t* __restrict__ colk, const TcArgs<CT>& a, uint32_t vb,
+                                             uint32_t dv, uint32_t base, uint32_t span, uint32_t* bm) {
+    const uint32_t words = (span + 31) >> 5;
+    for (uint32_t w = threadIdx.x; w < words; w += kThreads) bm[w] = 0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < dv; i += kThreads) {
+        if (ALIVE && !a.alive[colk[vb + i]]) continue;
+        const uint32_t o = a.colr[vb + i] - base;
+        if (o < span) atomicOr(&bm[o >> 5], 1u << (o & 31));
+    }
+    __syncthreads();
+}
+
+// probe_batch for a count against the bitmap of a heavy anchor: the probe lists are read as quads of places (colr)
+// instead of ids; a place outside [base, base + span) is not an out-neighbour of v. Returns this lane's hits.
+template <bool ALIVE, class CT>
+__device__ __forceinline__ uint32_t probe_batch_bitmap(const uint32_t* __restrict__ rowptr,
+                                                       const uint32_t* __restrict__ in_src,
+                                                       const uint32_t* __restrict__ in_posk, const TcArgs<CT>& a,
+                                                       uint32_t kb, uint32_t kend, const uint32_t* bm, uint32_t base,
+                                                       uint32_t span, uint32_t* s_incl, uint32_t* s_rb,
+                                                       uint32_t lane) {
+    uint32_t* s_re = s_rb + 32;
+    const uint32_t k = kb + lane;
+    uint32_t nq = 0, rb = 0, re = 0;
+    if (k < kend) {
+        const uint32_t u = in_src[k];
+        if (!ALIVE || a.alive[u]) {
+            rb = in_posk[k] + 1;
+            re = rowptr[u + 1];
+            if (re > rb) nq = ((re + 3) >> 2) - (rb >> 2);
+        }
+    }
+    const uint32_t incl = warp_incl_scan(nq, lane);
+    const uint32_t tot = __shfl_sync(GA_FULL_MASK, incl, 31);
+    s_incl[lane] = incl;
+    s_rb[lane] = rb;
+    s_re[lane] = re;
+    __syncwarp();
+    const uint4* __restrict__ colr4 = reinterpret_cast<const uint4*>(a.colr);
+    uint32_t owner = 0, hits = 0;
+    for (uint32_t p = lane; p < tot; p += 32) {
+        while (s_incl[owner] <= p) owner++;
+        const uint32_t lo = s_rb[owner], len = s_re[owner] - lo;
+        const uint32_t q = (lo >> 2) + (p - (owner ? s_incl[owner - 1] : 0u));
+        const uint4 r4 = __ldg(colr4 + q);
+        const uint32_t off = (q << 2) - lo;   // element i of the quad is in the list iff off + i < len
+        const uint32_t rs[4] = {r4.x, r4.y, r4.z, r4.w};
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const uint32_t o = rs[i] - base;
+            const bool look = (off + i < len) & (o < span);
+            const uint32_t w = look ? bm[o >> 5] : 0u;
+            hits += (w >> (o & 31)) & 1u;
+        }
+    }
+    __syncwarp();
+    return hits;
+}
+
 // Adds the per-slot counters of an item to the outputs (x's vertex count or edge v->x's count).
 template <int MODE, class CT>
 __device__ __forceinline__ void flush_table(const TcArgs<CT>& a, uint32_t vb, const uint32_t* key,
@@ -375,10 +442,18 @@ __global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const ui
             }
             const uint32_t vb = rowptr[v], dv = rowptr[v + 1] - vb;
             const uint32_t k0 = heavy.k0[item], k1 = heavy.k1[item];
-            const uint32_t bits = table_bits(dv, heavy_bits_max);
-            const bool global = bits == 0;
+            uint32_t base = 0, span = 0;
+            if (MODE == TC_COUNT && a.vrank && dv) {
+                const uint32_t rv = a.vrank[v];
+                base = rv + 1;
+                span = a.colr[vb + dv - 1] - rv;   // the last entry of the ordered row has the largest place
+            }
+            const bool bitmap = MODE == TC_COUNT && a.vrank && dv && span <= (Smax << 5);
+            const uint32_t bits = bitmap ? 0u : table_bits(dv, heavy_bits_max);
+            const bool global = !bitmap && bits == 0;
             if (threadIdx.x == 0) s_next = k0;
-            if (!global) build_table<MODE, ALIVE, CT>(col, a, vb, dv, key, cnt, pos, bits, threadIdx.x, kThreads, true);
+            if (bitmap) build_bitmap<ALIVE, CT>(colk, a, vb, dv, base, span, key);
+            else if (!global) build_table<MODE, ALIVE, CT>(col, a, vb, dv, key, cnt, pos, bits, threadIdx.x, kThreads, true);
             else __syncthreads();
             unsigned long long h = 0;
             for (;;) {
@@ -386,8 +461,13 @@ __global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const ui
                 if (lane == 0) kb = atomicAdd(&s_next, 32u);
                 kb = __shfl_sync(GA_FULL_MASK, kb, 0);
                 if (kb >= k1) break;
-                h += probe_batch<MODE, ALIVE, CT>(rowptr, col, colk, in_src, in_eid, in_posk, a, kb, min(kb + 32, k1),
-                                                  key, cnt, bits, global, vb, dv, s_incl, s_rb, s_ecnt, lane, v);
+                if (MODE == TC_COUNT && bitmap)
+                    h += probe_batch_bitmap<ALIVE, CT>(rowptr, in_src, in_posk, a, kb, min(kb + 32, k1), key, base, span,
+                                                       s_incl, s_rb, lane);
+                else
+                    h += probe_batch<MODE, ALIVE, CT>(rowptr, col, colk, in_src, in_eid, in_posk, a, kb,
+                                                      min(kb + 32, k1), key, cnt, bits, global, vb, dv, s_incl, s_rb,
+                                                      s_ecnt, lane, v);
             }
             hits += h;
             if (MODE == TC_VSUP) {
@@ -395,7 +475,7 @@ __global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const ui
                 if (lane == 0 && t) atomicAdd(&a.vsup[v], (CT)t);
             }
             __syncthreads();
-            if (!global) flush_table<MODE, CT>(a, vb, key, cnt, pos, bits, threadIdx.x, kThreads);
+            if (!global && !bitmap) flush_table<MODE, CT>(a, vb, key, cnt, pos, bits, threadIdx.x, kThreads);
             __syncthreads();
         }
     }
@@ -558,6 +638,8 @@ static ga_status launch_hash(ga_graph* g, const TcArgs<CT>& a0) {
     occ = std::max(occ, 1);
     TcArgs<CT> a = a0;
     a.origk = g->origk;
+    a.colr = g->colr;
+    a.vrank = g->opt_count_bitmap ? nullptr : g->vrank;   // no place array: hash sets for every anchor
     const uint32_t* bounds = nullptr;
     uint64_t want = std::max<uint64_t>(g->heavy.count, (g->light.count + kWarps - 1) / kWarps);
     if (a.nshards > 1) {   // this shard's anchors (cut on the device; the queue counters sit in d_queue[0..1])

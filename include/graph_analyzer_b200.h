@@ -173,8 +173,11 @@ typedef enum ga_option {
     GA_OPT_HEAVY_TABLE_BITS = 5, /* log2 buckets (4 slots each) of the block-wide hash set; anchors that need more
                                     binary-search the global row (0 = as large as shared memory allows, 3..13)      */
     GA_OPT_LIGHT_MAX_DEG = 6, /* anchors with out-degree <= this use per-warp tables (0 = 128, at most 256)        */
-    GA_OPT_UPDATE_MODE = 7    /* peeling/core rounds: 0 auto (triangle incidence lists when their 24*T bytes fit,
+    GA_OPT_UPDATE_MODE = 7,   /* peeling/core rounds: 0 auto (triangle incidence lists when their 24*T bytes fit,
                                  else re-enumeration), 1 re-enumerate the frontier's triangles, 2 incidence lists   */
+    GA_OPT_COUNT_BITMAP = 8   /* counts in the hash kernel: 0 auto (a heavy anchor whose out-neighbours lie within
+                                 32 x the table's words of places above it in the (degree, id) order is probed
+                                 against a bitmap of them), 1 hash sets for every anchor                            */
 } ga_option;
 ga_status ga_graph_set_option(ga_graph* g, ga_option opt, int64_t value);
 

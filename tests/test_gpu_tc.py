@@ -10,12 +10,15 @@ from conftest import FIXTURES, fixture_path, golden_arrays, hub_pairs, random_pa
 pytestmark = pytest.mark.gpu
 
 # kernel configurations that force every path: default (light + heavy bins), plain merge kernel, tiny light bin with
-# a small heavy table (heavy anchors and the global binary-search fallback), small work items (many items/anchor)
+# a small heavy table (heavy anchors and the global binary-search fallback; option 8 keeps counts on hash sets),
+# small work items (many items/anchor)
 CONFIGS = {
     "auto": {},
     "plain": {1: 1},
-    "heavy_global": {6: 8, 5: 3},
-    "heavy_table": {6: 4, 5: 10},
+    "heavy_global": {6: 8, 5: 3, 8: 1},
+    "heavy_table": {6: 4, 5: 10, 8: 1},
+    # counts of heavy anchors against bitmaps of up to 1,024 places; wider anchors binary-search the global row
+    "heavy_bitmap": {6: 4, 5: 3},
     "small_items": {4: 16},
     # light bin up to out-degree 256: in the support modes anchors above 128 fall back to binary search
     "light_256": {6: 256, 1: 2},
