@@ -110,6 +110,9 @@ struct ga_graph {
     // every anchor of more than 128 out-neighbours), which the count kernel covers with a bitmap
     uint32_t* vrank = nullptr;    // n
     uint32_t* colr = nullptr;     // m (+4 zero padding, 16-byte aligned like colk)
+    // m: in-edge k's probe list [in_posk[k] + 1, end of its source's row) in colk; read by the count kernels in one
+    // 64-bit load instead of the source and then its row end (R-MAT 22 count: 2.58 vs 2.69 ms)
+    uint2* in_rng = nullptr;
 
     unsigned long long* anchor_work = nullptr;   // n+1: probe work of the anchors below v (cuts shards)
     ga_items light, heavy;        // degree-binned work lists of the hash-probe kernel

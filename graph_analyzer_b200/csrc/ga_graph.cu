@@ -381,6 +381,13 @@ __global__ void k_rank_invert(const uint32_t* __restrict__ order, uint32_t n, ui
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) vrank[order[i]] = i;
 }
 
+// in_rng[k] = [in_posk[k] + 1, rowptr[in_src[k] + 1]): where the probe list of in-edge k starts and ends in colk.
+__global__ void k_in_rng(const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ in_src,
+                         const uint32_t* __restrict__ in_posk, uint32_t m, uint2* __restrict__ in_rng) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x)
+        in_rng[k] = make_uint2(in_posk[k] + 1, rowptr[in_src[k] + 1]);
+}
+
 // colr[e] = vrank[colk[e]].
 __global__ void k_colr(const uint32_t* __restrict__ colk, const uint32_t* __restrict__ vrank, uint32_t m,
                        uint32_t* __restrict__ colr) {
@@ -634,6 +641,11 @@ static ga_status prepare_index(ga_graph* g) {
                 g->rowptr, key, listed, listed + n, g->colk, g->origk, posk);
         cudaFreeAsync(listed, st);
         k_in_posk<<<ge, 256, 0, st>>>(g->in_eid, posk, m, g->in_posk);
+        GA_CUDA(cudaGetLastError());
+        dfree(g, g->in_rng);
+        g->in_rng = nullptr;
+        GA_TRY(dalloc(g, &g->in_rng, m));
+        k_in_rng<<<ge, 256, 0, st>>>(g->rowptr, g->in_src, g->in_posk, m, g->in_rng);
         GA_CUDA(cudaGetLastError());
         cudaFreeAsync(key, st);
         cudaFreeAsync(posk, st);

@@ -171,11 +171,12 @@ __device__ __forceinline__ uint32_t probe_one(const uint32_t* __restrict__ col, 
     return 0;
 }
 
-// Probes one batch of up to 32 in-edges [kb, kend) of anchor v (one warp). Lane l loads the l-th source u; its probe
-// list, the part of u's (degree, id)-ordered row after v, colk[rb, re), is cut into 16-byte quads (colk is 16-byte
-// aligned and padded, so a quad never leaves the allocation), a warp scan of the quad counts flattens the 32 lists
-// into one sequence, and lane p takes quads p, p+32, ...: one 128-bit load, then up to 4 probes of the elements
-// inside [rb, re). Each lane advances its owner index monotonically. Returns this lane's hits.
+// Probes one batch of up to 32 in-edges [kb, kend) of anchor v (one warp). Lane l loads the l-th in-edge's probe
+// list, the part of its source u's (degree, id)-ordered row after v, colk[rb, re), from in_rng in one 64-bit load
+// (sources are read only where the mode needs them). The list is cut into 16-byte quads (colk is 16-byte aligned and
+// padded, so a quad never leaves the allocation), a warp scan of the quad counts flattens the 32 lists into one
+// sequence, and lane p takes quads p, p+32, ...: one 128-bit load, then up to 4 probes of the elements inside
+// [rb, re). Each lane advances its owner index monotonically. Returns this lane's hits.
 template <int MODE, bool ALIVE, class CT>
 __device__ __forceinline__ unsigned long long probe_batch(
     const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ col, const uint32_t* __restrict__ colk,
@@ -188,10 +189,11 @@ __device__ __forceinline__ unsigned long long probe_batch(
     const uint32_t k = kb + lane;
     uint32_t nq = 0, rb = 0, re = 0, u = 0;
     if (k < kend) {
-        u = in_src[k];
+        if (ALIVE || MODE == TC_LIST || MODE == TC_VSUP) u = in_src[k];   // the source's mask, list entry, count
         if (!ALIVE || a.alive[u]) {
-            rb = in_posk[k] + 1;
-            re = rowptr[u + 1];
+            const uint2 r = a.in_rng[k];
+            rb = r.x;
+            re = r.y;
             if (re > rb) nq = ((re + 3) >> 2) - (rb >> 2);
         }
     }
@@ -349,10 +351,10 @@ __device__ __forceinline__ uint32_t probe_batch_bitmap(const uint32_t* __restric
     const uint32_t k = kb + lane;
     uint32_t nq = 0, rb = 0, re = 0;
     if (k < kend) {
-        const uint32_t u = in_src[k];
-        if (!ALIVE || a.alive[u]) {
-            rb = in_posk[k] + 1;
-            re = rowptr[u + 1];
+        if (!ALIVE || a.alive[in_src[k]]) {
+            const uint2 r = a.in_rng[k];
+            rb = r.x;
+            re = r.y;
             if (re > rb) nq = ((re + 3) >> 2) - (rb >> 2);
         }
     }
@@ -639,6 +641,7 @@ static ga_status launch_hash(ga_graph* g, const TcArgs<CT>& a0) {
     TcArgs<CT> a = a0;
     a.origk = g->origk;
     a.colr = g->colr;
+    a.in_rng = g->in_rng;
     a.vrank = g->opt_count_bitmap ? nullptr : g->vrank;   // no place array: hash sets for every anchor
     const uint32_t* bounds = nullptr;
     uint64_t want = std::max<uint64_t>(g->heavy.count, (g->light.count + kWarps - 1) / kWarps);
