@@ -30,8 +30,8 @@
 // round of three dependent kernels costs tens of microseconds of launch and drain latency whatever its size. In graph
 // mode the core round's body therefore starts with k_core_small_rounds, ONE thread block cluster (16 CTAs of 1,024
 // threads, 8 where 16 cannot be co-scheduled) that runs consecutive rounds itself - minimum, frontier, update, close -
-// with cluster barriers between the phases instead of kernel boundaries, for as long as the alive list is at most
-// kSmallAlive and the next round destroys at most kSmallWork incidence entries. The first round that does not fit
+// with cluster barriers between the phases instead of kernel boundaries, for as long as the alive list holds at most
+// 8 vertices per cluster thread and the next round destroys at most kSmallWork incidence entries. The first round that does not fit
 // is left untouched for the grid kernels that follow in the same body; the loop decisions and every result are the
 // grid round's, so the output is unchanged.
 #include <cooperative_groups.h>
@@ -579,11 +579,14 @@ __global__ void __launch_bounds__(256) k_frontier_update_list(LoopScalars* sc, c
 
 // ---- small core rounds in one thread block cluster ----------------------------------------------------------------
 constexpr uint32_t kSmallThreads = 1024;     // threads per CTA of the cluster
-constexpr uint32_t kSmallAlive = 1u << 16;   // alive vertices up to which a round may run in the cluster
+constexpr uint32_t kSmallAlive = 1u << 16;   // alive vertices up to which a round may run in an 8-CTA cluster
 constexpr uint32_t kSmallWork = 1u << 17;    // incidence entries a round may destroy in the cluster
 constexpr uint32_t kSmallChunk = 64;         // incidence entries per update item of the cluster
 
-constexpr uint32_t kSmallPer = kSmallAlive / (8 * kSmallThreads);   // alive entries per thread (8-CTA cluster)
+// Alive entries per thread: a round runs in the cluster while its alive list fits 8 entries per thread, 65,536
+// vertices in an 8-CTA cluster and 131,072 in a 16-CTA one (R-MAT 22 cores: 233-236 ms against 245-248 ms with the
+// 65,536 limit for both sizes).
+constexpr uint32_t kSmallPer = kSmallAlive / (8 * kSmallThreads);
 static_assert(kSmallPer * 8 * kSmallThreads == kSmallAlive, "alive entries must split evenly over the threads");
 
 // The round's level and size in one reduction: the minimum triangle count over the alive list, the incidence entries
@@ -640,7 +643,7 @@ struct SmallCounters {
 };
 
 // Runs consecutive core rounds (the work of k_core_min, k_core_mark, k_frontier_update_list and close_round_if_last
-// for LOOP_CORE) inside one cluster while the alive list has at most kSmallAlive vertices and a round destroys at
+// for LOOP_CORE) inside one cluster while the alive list has at most kSmallPer vertices per thread and a round destroys at
 // most kSmallWork incidence entries; returns at the first round that is larger (untouched, for the grid kernels),
 // when the loop ends (the WHILE condition is set to 0) or at a status other than LS_OK.
 //
@@ -681,7 +684,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1) k_core_small_rounds(
             if (writer) cudaGraphSetConditional(handle, 0);
             break;
         }
-        if (na > kSmallAlive) break;
+        if (na > kSmallPer * nthr) break;   // kSmallAlive with 8 CTAs, twice that with 16
         uint32_t* in = p ? alive1 : alive0;
         uint32_t* outl = p ? alive0 : alive1;
         uint32_t* frontier = (round & 1) ? fr1 : fr0;
