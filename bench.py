@@ -886,6 +886,37 @@ def leg_serve(args) -> dict:
     holder.close()
     return line
 
+def leg_passes(args) -> dict:
+    """Each triangle pass of the hash kernel on R-MAT scale 22 timed alone (device-synchronised wall time, mean of
+    --steps calls after the warm-up): the count, per-edge supports (into device memory), per-vertex supports (with the
+    download of the n counters), and a batch peel at eps 1/2, whose first call builds the incidence lists with the
+    LIST pass (timed apart from the later, list-reusing calls). Checked against the count: both supports sum to 3T.
+    Also the short command the per-pass ncu captures run."""
+    import torch
+    import graph_analyzer_b200 as ga
+    g = make_graph(ga, args.scale)
+    d = ga.DeviceGraph(g)
+    d.set_option(ga.OPT_TC_KERNEL, 2)
+    d.prepare()
+    d_sup = torch.zeros(g.m, dtype=torch.int32, device="cuda")
+    T = d.tc_count()
+    out = {"workload": f"rmat{args.scale}_passes", "n": g.n, "m": g.m, "triangles": T}
+    for _ in range(args.warmup):
+        d.tc_count()
+        d.support_edges_device(d_sup.data_ptr())
+    out["count_ms"], _ = _timed(torch, d.tc_count, args.steps)
+    out["esup_ms"], Ts = _timed(torch, lambda: d.support_edges_device(d_sup.data_ptr()), args.steps)
+    out["vsup_ms"], (Tv, deg) = _timed(torch, d.support_vertices, args.steps)
+    out["first_peel_ms"], _ = _timed(torch, lambda: d.batch_peel(1, 2, want_removed=False))   # LIST pass + rounds
+    out["peel_ms"], _ = _timed(torch, lambda: d.batch_peel(1, 2, want_removed=False), args.steps)
+    sup_total = int(d_sup.cpu().numpy().view(np.uint32).astype(np.int64).sum())
+    d.close()
+    ok = Ts == T and Tv == T and sup_total == 3 * T and int(deg.astype(np.int64).sum()) == 3 * T
+    out.update({"metric": "triangle passes of the hash kernel, ms", "value": out["count_ms"], "unit": "ms",
+                "higher_is_better": False, "parity": {"against": "the count (supports sum to 3T)", "all": ok}})
+    return out
+
+
 LEGS = {"hk2": leg_hk2, "rmat22-full": leg_rmat22, "batch": leg_batch, "serve": leg_serve}
 
 
@@ -1031,7 +1062,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", choices=["rmat22", "hk2", "rmat22-full", "batch", "serve", "reference-gpu"],
+    ap.add_argument("--workload", choices=["rmat22", "hk2", "rmat22-full", "batch", "serve", "reference-gpu",
+                                           "passes"],
                     default="rmat22",
                     help="rmat22 (default, the headline line) or a secondary workload")
     ap.add_argument("--graphs", type=int, default=4096, help="graphs in the batch workload")
@@ -1061,6 +1093,10 @@ def main():
         args.per_graph_stride = 1 if args.workload == "batch" else 8
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "passes":
+        line = leg_passes(args)
+        print(json.dumps(line), flush=True)
+        return 0 if line["parity"]["all"] else 1
     if args.workload in LEGS:
         return run_leg(args)
     if args.workload == "reference-gpu":
