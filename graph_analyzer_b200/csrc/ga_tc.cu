@@ -129,7 +129,7 @@ __device__ __forceinline__ void on_hit(const TcArgs<CT>& a, uint32_t* cnt, uint3
         atomicAdd(&cnt[h], 1u);
         atomicAdd(&ecnt[owner], 1u);
     }
-    if (MODE == TC_ESUP) atomicAdd(&a.esup[a.origk[e]], 1u);
+    if (MODE == TC_ESUP) atomicAdd(&a.esupk[e], 1u);   // u->x at its probe position; folded into col order after
     if (MODE == TC_LIST) list_triangle(a, s_u[owner], anchor, x);
 }
 
@@ -162,7 +162,7 @@ __device__ __forceinline__ uint32_t probe_one(const uint32_t* __restrict__ col, 
         if (counters(MODE)) atomicAdd(&s_ecnt[owner], 1u);
         if (MODE == TC_VSUP) atomicAdd(&a.vsup[x], (CT)1);
         if (MODE == TC_ESUP) {
-            atomicAdd(&a.esup[a.origk[e]], 1u);
+            atomicAdd(&a.esupk[e], 1u);
             atomicAdd(&a.esup[j], 1u);
         }
         if (MODE == TC_LIST) list_triangle(a, s_u[owner], anchor, x);
@@ -398,6 +398,16 @@ __device__ __forceinline__ void flush_table(const TcArgs<CT>& a, uint32_t vb, co
             if (MODE == TC_VSUP) atomicAdd(&a.vsup[key[s]], (CT)c);   // 4-slot buckets: no spill flags
             else atomicAdd(&a.esup[vb + pos[s]], c);
         }
+    }
+}
+
+// esup[origk[e]] += esupk[e]: supports booked at colk positions moved to the caller's col order (origk is a
+// permutation within each row, so every target is written by one thread).
+__global__ void k_esup_fold(const uint32_t* __restrict__ esupk, const uint32_t* __restrict__ origk, uint32_t m,
+                            uint32_t* __restrict__ esup) {
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
+        const uint32_t c = esupk[e];
+        if (c) esup[origk[e]] += c;
     }
 }
 
@@ -655,9 +665,18 @@ static ga_status launch_hash(ga_graph* g, const TcArgs<CT>& a0) {
     }
     const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)g->sm_count * occ, want));
     GA_CUDA(cudaMemsetAsync(g->d_queue, 0, 4 * sizeof(uint32_t), g->stream));
+    if (MODE == TC_ESUP && g->m) {   // u->x supports by probe position (nearby addresses along a probe list)
+        GA_CUDA(pool_malloc((void**)&a.esupk, (size_t)g->m * 4, g->stream));
+        GA_CUDA(cudaMemsetAsync(a.esupk, 0, (size_t)g->m * 4, g->stream));
+    }
     kern<<<grid, kThreads, smem, g->stream>>>(g->rowptr, g->col, g->colk, g->in_src, g->in_eid, g->in_posk, g->heavy,
                                               g->light, bounds, hb, g->d_queue, a);
     GA_CUDA(cudaGetLastError());
+    if (MODE == TC_ESUP && g->m) {
+        k_esup_fold<<<grid_for(g->m, 256), 256, 0, g->stream>>>(a.esupk, g->origk, g->m, a.esup);
+        GA_CUDA(cudaGetLastError());
+        cudaFreeAsync(a.esupk, g->stream);
+    }
     return GA_OK;
 }
 

@@ -25,6 +25,7 @@ struct TcArgs {
     const uint32_t* colr = nullptr;   // set by the launcher: the (degree, id)-ordered rows as vertex places
     const uint32_t* vrank = nullptr;  // set by the launcher: every vertex's place in the (degree, id) order
     const uint2* in_rng = nullptr;    // set by the launcher: in-edge k's probe list [start, end) in colk / colr
+    uint32_t* esupk = nullptr;        // set by the launcher (ESUP, hash kernel): supports by colk position, m zeroed
     // shard `shard` of `nshards` (0 = the whole graph): equal parts of the work items (hash kernel) or of the edges
     // (plain kernel); the shards of a graph partition its triangles
     uint32_t shard = 0, nshards = 0;
