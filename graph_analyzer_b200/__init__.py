@@ -26,6 +26,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import time
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -105,7 +106,8 @@ class _RequestResult(C.Structure):
 
 class _ServerStats(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in ("submitted", "completed", "folded_launches", "evictions",
-                                          "resident_graphs", "resident_bytes", "peak_reserved_bytes")]
+                                          "resident_graphs", "resident_bytes", "peak_reserved_bytes", "queued",
+                                          "running", "reserved_bytes")]
 
 
 class _HostBatch(C.Structure):
@@ -893,6 +895,15 @@ class Server:
             return None
         _check(st)
         return self._result(ticket, r)
+
+    def wait_for(self, ticket: int, timeout_s: float) -> RequestResult | None:
+        """The result of `ticket` once ready, or None after `timeout_s` seconds (the request stays pending)."""
+        t_end = time.monotonic() + timeout_s
+        while True:
+            r = self.poll(ticket)
+            if r is not None or time.monotonic() >= t_end:
+                return r
+            time.sleep(0.01)
 
     def wait(self, ticket: int) -> RequestResult:
         r = _RequestResult()

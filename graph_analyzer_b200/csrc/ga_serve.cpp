@@ -568,6 +568,9 @@ ga_status ga_server_stats_get(ga_server* s, ga_server_stats* out) {
             out->resident_bytes += kv.second.dev_bytes;
         }
     out->peak_reserved_bytes = s->peak_reserved;
+    out->queued = s->queue.size();
+    out->running = s->running;
+    out->reserved_bytes = s->reserved;
     return GA_OK;
 }
 

@@ -407,6 +407,9 @@ typedef struct ga_request_result {
 typedef struct ga_server_stats {
     uint64_t submitted, completed, folded_launches, evictions, resident_graphs;
     uint64_t resident_bytes, peak_reserved_bytes;
+    uint64_t queued;   /* requests waiting for admission now */
+    uint64_t running;  /* work units a worker is running now (a folded batch counts once) */
+    uint64_t reserved_bytes;  /* the admission's current reservation */
 } ga_server_stats;
 
 ga_status ga_server_create(const ga_server_config* config, ga_server** out);

@@ -6,6 +6,7 @@ gpu_dsg.cu:283-289 read)."""
 from __future__ import annotations
 
 import ctypes as C
+import sys
 
 import numpy as np
 import pytest
@@ -127,14 +128,25 @@ def test_mix_equals_alone(ga, served, slots, fold, small, pin):
     assert st["resident_graphs"] > 0
 
 
+def _wait(s, ticket, what):
+    """The result within 300 s, or a failure that says where the request was: still queued (not admitted) or
+    running (on a worker) - with the admission's reservation."""
+    r = s.wait_for(ticket, 300.0)
+    if r is None:   # written past pytest's capture: closing the server waits for the request too
+        sys.__stderr__.write(f"{what}: not done after 300 s, server stats {s.stats()}\n")
+        sys.__stderr__.flush()
+    assert r is not None, (what, "not done after 300 s", s.stats())
+    return r
+
+
 def test_requery_hits_resident_graph(ga, served):
     gs, alone = served
     big = len(gs) - 1
     with ga.Server(slots=2) as s:
         gid = s.add_graph(gs[big])
-        first = s.wait(s.submit(gid, ga.REQ_TC))
-        again = s.wait(s.submit(gid, ga.REQ_PEEL, 1, 10))
-        core = s.wait(s.submit(gid, ga.REQ_CORE))
+        first = _wait(s, s.submit(gid, ga.REQ_TC), "count")
+        again = _wait(s, s.submit(gid, ga.REQ_PEEL, 1, 10), "peel")
+        core = _wait(s, s.submit(gid, ga.REQ_CORE), "cores")
     assert not first.resident_hit and again.resident_hit and core.resident_hit
     assert first.triangles == alone[big]["tc"]
     assert _value(ga, ga.REQ_PEEL, again) == alone[big][("peel", 1, 10)]
