@@ -104,19 +104,19 @@ struct ga_graph {
     // kernels probe that suffix of u's row alone
     uint32_t* colk = nullptr;     // m (+4 zero padding, 16-byte aligned like col)
     uint32_t* origk = nullptr;    // m: position in col of colk[e]
-    uint32_t* in_posk = nullptr;  // m: position in colk of in-edge k's edge u->v (aligned with in_src / in_eid)
     // every vertex's place in the (degree, id) order, and colk with each entry replaced by that place: an anchor's
     // out-neighbours then lie in a short range of places just above the anchor's own (R-MAT 22: within 65,536 for
     // every anchor of more than 128 out-neighbours), which the count kernel covers with a bitmap
     uint32_t* vrank = nullptr;    // n
     uint32_t* colr = nullptr;     // m (+4 zero padding, 16-byte aligned like colk)
-    // m: in-edge k's probe list [in_posk[k] + 1, end of its source's row) in colk; read by the count kernels in one
-    // 64-bit load instead of the source and then its row end (R-MAT 22 count: 2.58 vs 2.69 ms)
+    // m: in-edge k's probe list in colk, [the place of its edge u->v in u's reordered row + 1, end of u's row);
+    // read by the count kernels in one 64-bit load instead of the source and then its row end (R-MAT 22 count:
+    // 2.58 vs 2.69 ms)
     uint2* in_rng = nullptr;
 
     unsigned long long* anchor_work = nullptr;   // n+1: probe work of the anchors below v (cuts shards)
     ga_items light, heavy;        // degree-binned work lists of the hash-probe kernel
-    bool index_ready = false;     // src, in-lists, colk / origk / in_posk / vrank / colr built
+    bool index_ready = false;     // src, in-lists, colk / origk / in_rng / vrank / colr built
     bool prepared = false;        // ... and the work items for the current light_max_deg / item_work
     ga_loops* loops = nullptr;    // peeling / core loop state, allocated on first use
     // a batch: the graph is the disjoint union of seg_count graphs, graph s owning vertices [seg_off[s], seg_off[s+1])

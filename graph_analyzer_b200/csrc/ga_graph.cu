@@ -3,8 +3,8 @@
 // Derived structures (built once per handle, on the device, kept resident):
 //   src[m]                 row owner of every edge (the reference builds it on the host, graph.h:64)
 //   in_ptr/in_src/in_eid   transpose of the oriented CSR: for every vertex v the edges u->v (source, edge index)
-//   colk/origk/in_posk     every row again in (degree, id) order, where each entry sits in it, and where each
-//                          in-edge u->v sits in u's reordered row (the start of its probe suffix)
+//   colk/origk/in_rng      every row again in (degree, id) order, where each entry sits in it, and for each
+//                          in-edge u->v the part of u's reordered row after v (its probe suffix)
 //   vrank/colr             every vertex's place in the (degree, id) order, and colk with entries as places
 //   light / heavy items    degree-binned work lists of the hash-probe kernels: one item = a slice of v's in-edges
 //                          whose probe work (sum of out-degrees of the sources) is bounded; anchors with a large
@@ -381,11 +381,13 @@ __global__ void k_rank_invert(const uint32_t* __restrict__ order, uint32_t n, ui
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) vrank[order[i]] = i;
 }
 
-// in_rng[k] = [in_posk[k] + 1, rowptr[in_src[k] + 1]): where the probe list of in-edge k starts and ends in colk.
+// in_rng[k] = [posk[in_eid[k]] + 1, rowptr[in_src[k] + 1]): where the probe list of in-edge k (u->v) starts and ends
+// in colk, i.e. the part of u's (degree, id)-ordered row after v.
 __global__ void k_in_rng(const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ in_src,
-                         const uint32_t* __restrict__ in_posk, uint32_t m, uint2* __restrict__ in_rng) {
+                         const uint32_t* __restrict__ in_eid, const uint32_t* __restrict__ posk, uint32_t m,
+                         uint2* __restrict__ in_rng) {
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x)
-        in_rng[k] = make_uint2(in_posk[k] + 1, rowptr[in_src[k] + 1]);
+        in_rng[k] = make_uint2(posk[in_eid[k]] + 1, rowptr[in_src[k] + 1]);
 }
 
 // colr[e] = vrank[colk[e]].
@@ -403,19 +405,11 @@ __global__ void k_anchor_work(const uint32_t* __restrict__ in_ptr, const unsigne
         anchor_work[v] = in_ptr[v] ? prefix[in_ptr[v] - 1] : 0ull;
 }
 
-// in_posk[k] = position in colk of in-edge k's edge (its position in col is in_eid[k]).
-__global__ void k_in_posk(const uint32_t* __restrict__ in_eid, const uint32_t* __restrict__ posk, uint32_t m,
-                          uint32_t* __restrict__ in_posk) {
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x)
-        in_posk[k] = posk[in_eid[k]];
-}
-
 // work[k] = probe length of in-edge k (u->v): the entries of u's (degree, id)-ordered row after v.
-__global__ void k_in_work(const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ in_src,
-                          const uint32_t* __restrict__ in_posk, uint32_t m, unsigned long long* __restrict__ work) {
+__global__ void k_in_work(const uint2* __restrict__ in_rng, uint32_t m, unsigned long long* __restrict__ work) {
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
-        const uint32_t u = in_src[k];
-        work[k] = rowptr[u + 1] - in_posk[k] - 1;
+        const uint2 r = in_rng[k];
+        work[k] = r.y - r.x;
     }
 }
 
@@ -596,8 +590,7 @@ static ga_status prepare_index(ga_graph* g) {
     cudaStream_t st = g->stream;
     const uint32_t n = g->n, m = g->m;
     GA_CUDA(cudaStreamSynchronize(st));
-    for (uint32_t** p : {&g->src, &g->in_ptr, &g->in_src, &g->in_eid, &g->colk, &g->origk, &g->in_posk, &g->vrank,
-                         &g->colr}) {
+    for (uint32_t** p : {&g->src, &g->in_ptr, &g->in_src, &g->in_eid, &g->colk, &g->origk, &g->vrank, &g->colr}) {
         dfree(g, *p);
         *p = nullptr;
     }
@@ -607,7 +600,6 @@ static ga_status prepare_index(ga_graph* g) {
     GA_TRY(dalloc(g, &g->in_eid, m));
     GA_TRY(dalloc(g, &g->colk, (size_t)m + 4));   // padded like col: quad loads of the last row stay inside
     GA_TRY(dalloc(g, &g->origk, m));
-    GA_TRY(dalloc(g, &g->in_posk, m));
     GA_CUDA(cudaMemsetAsync(g->colk + m, 0, 16, st));
     uint32_t *indeg = nullptr, *fill = nullptr;
     GA_CUDA(pool_malloc((void**)&indeg, ((size_t)n + 1) * 4, st));
@@ -640,12 +632,10 @@ static ga_status prepare_index(ga_graph* g) {
             k_order_rows_listed<<<(unsigned)g->sm_count * 6, kOrderWarps * 32, 0, st>>>(
                 g->rowptr, key, listed, listed + n, g->colk, g->origk, posk);
         cudaFreeAsync(listed, st);
-        k_in_posk<<<ge, 256, 0, st>>>(g->in_eid, posk, m, g->in_posk);
-        GA_CUDA(cudaGetLastError());
         dfree(g, g->in_rng);
         g->in_rng = nullptr;
         GA_TRY(dalloc(g, &g->in_rng, m));
-        k_in_rng<<<ge, 256, 0, st>>>(g->rowptr, g->in_src, g->in_posk, m, g->in_rng);
+        k_in_rng<<<ge, 256, 0, st>>>(g->rowptr, g->in_src, g->in_eid, posk, m, g->in_rng);
         GA_CUDA(cudaGetLastError());
         cudaFreeAsync(key, st);
         cudaFreeAsync(posk, st);
@@ -717,7 +707,7 @@ static ga_status prepare_items(ga_graph* g) {
     unsigned long long* prefix = nullptr;
     GA_CUDA(pool_malloc((void**)&prefix, ((size_t)m + 1) * 8, st));
     if (m) {   // work prefix over in-edges (64-bit: the total probe count can exceed 2^32)
-        k_in_work<<<grid_for(m, 256), 256, 0, st>>>(g->rowptr, g->in_src, g->in_posk, m, prefix);
+        k_in_work<<<grid_for(m, 256), 256, 0, st>>>(g->in_rng, m, prefix);
         GA_CUDA(cudaGetLastError());
         GA_TRY(scan_impl<unsigned long long>(st, prefix, prefix, m, true));
     }

@@ -180,7 +180,7 @@ __device__ __forceinline__ uint32_t probe_one(const uint32_t* __restrict__ col, 
 template <int MODE, bool ALIVE, class CT>
 __device__ __forceinline__ unsigned long long probe_batch(
     const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ col, const uint32_t* __restrict__ colk,
-    const uint32_t* __restrict__ in_src, const uint32_t* __restrict__ in_eid, const uint32_t* __restrict__ in_posk,
+    const uint32_t* __restrict__ in_src, const uint32_t* __restrict__ in_eid,
     const TcArgs<CT>& a, uint32_t kb, uint32_t kend, const uint32_t* key, uint32_t* cnt, uint32_t bits, bool global,
     uint32_t vb, uint32_t dv, uint32_t* s_incl, uint32_t* s_rb, uint32_t* s_ecnt, uint32_t lane, uint32_t anchor) {
     unsigned long long hits = 0;
@@ -343,7 +343,7 @@ __device__ __forceinline__ void build_bitmap(const uint32_t* __restrict__ colk, 
 template <bool ALIVE, class CT>
 __device__ __forceinline__ uint32_t probe_batch_bitmap(const uint32_t* __restrict__ rowptr,
                                                        const uint32_t* __restrict__ in_src,
-                                                       const uint32_t* __restrict__ in_posk, const TcArgs<CT>& a,
+                                                       const TcArgs<CT>& a,
                                                        uint32_t kb, uint32_t kend, const uint32_t* bm, uint32_t base,
                                                        uint32_t span, uint32_t* s_incl, uint32_t* s_rb,
                                                        uint32_t lane) {
@@ -419,7 +419,7 @@ __global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const ui
                                                       const uint32_t* __restrict__ colk,
                                                       const uint32_t* __restrict__ in_src,
                                                       const uint32_t* __restrict__ in_eid,
-                                                      const uint32_t* __restrict__ in_posk, ga_items heavy,
+                                                      ga_items heavy,
                                                       ga_items light, const uint32_t* __restrict__ bounds,
                                                       uint32_t heavy_bits_max, uint32_t* __restrict__ queue,
                                                       TcArgs<CT> a) {
@@ -474,10 +474,10 @@ __global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const ui
                 kb = __shfl_sync(GA_FULL_MASK, kb, 0);
                 if (kb >= k1) break;
                 if (MODE == TC_COUNT && bitmap)
-                    h += probe_batch_bitmap<ALIVE, CT>(rowptr, in_src, in_posk, a, kb, min(kb + 32, k1), key, base, span,
+                    h += probe_batch_bitmap<ALIVE, CT>(rowptr, in_src, a, kb, min(kb + 32, k1), key, base, span,
                                                        s_incl, s_rb, lane);
                 else
-                    h += probe_batch<MODE, ALIVE, CT>(rowptr, col, colk, in_src, in_eid, in_posk, a, kb,
+                    h += probe_batch<MODE, ALIVE, CT>(rowptr, col, colk, in_src, in_eid, a, kb,
                                                       min(kb + 32, k1), key, cnt, bits, global, vb, dv, s_incl, s_rb,
                                                       s_ecnt, lane, v);
             }
@@ -518,7 +518,7 @@ __global__ void __launch_bounds__(kThreads, GA_TC_MIN_BLOCKS) k_tc_hash(const ui
             unsigned long long h = 0;
             const uint32_t k1 = light.k1[item];
             for (uint32_t kb = light.k0[item]; kb < k1; kb += 32)
-                h += probe_batch<MODE, ALIVE, CT>(rowptr, col, colk, in_src, in_eid, in_posk, a, kb, min(kb + 32, k1),
+                h += probe_batch<MODE, ALIVE, CT>(rowptr, col, colk, in_src, in_eid, a, kb, min(kb + 32, k1),
                                                   key, cnt, bits, global, vb, dv, s_incl, s_rb, s_ecnt, lane, v);
             hits += h;
             if (MODE == TC_VSUP) {
@@ -669,7 +669,7 @@ static ga_status launch_hash(ga_graph* g, const TcArgs<CT>& a0) {
         GA_CUDA(pool_malloc((void**)&a.esupk, (size_t)g->m * 4, g->stream));
         GA_CUDA(cudaMemsetAsync(a.esupk, 0, (size_t)g->m * 4, g->stream));
     }
-    kern<<<grid, kThreads, smem, g->stream>>>(g->rowptr, g->col, g->colk, g->in_src, g->in_eid, g->in_posk, g->heavy,
+    kern<<<grid, kThreads, smem, g->stream>>>(g->rowptr, g->col, g->colk, g->in_src, g->in_eid, g->heavy,
                                               g->light, bounds, hb, g->d_queue, a);
     GA_CUDA(cudaGetLastError());
     if (MODE == TC_ESUP && g->m) {
