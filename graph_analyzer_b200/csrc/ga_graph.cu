@@ -152,33 +152,33 @@ __global__ void k_src_and_indeg(const uint32_t* __restrict__ rowptr, const uint3
     }
 }
 
-// Scatter every edge u->v into v's in-list; checks the (degree, id) orientation rule of graph.h:43-45 with
-// deg = out + in (flag 16 in *err when an edge points the wrong way).
-__global__ void k_in_scatter(const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ col,
-                             const uint32_t* __restrict__ src, const uint32_t* __restrict__ in_ptr, uint32_t m,
-                             uint32_t* __restrict__ fill, uint32_t* __restrict__ in_src,
-                             uint32_t* __restrict__ in_eid, unsigned long long* err) {
-    uint32_t bad = 0;
+// Scatter every edge u->v into v's in-list.
+__global__ void k_in_scatter(const uint32_t* __restrict__ col, const uint32_t* __restrict__ src,
+                             const uint32_t* __restrict__ in_ptr, uint32_t m, uint32_t* __restrict__ fill,
+                             uint32_t* __restrict__ in_src, uint32_t* __restrict__ in_eid) {
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
         const uint32_t u = src[e], v = col[e];
-        const uint32_t du = rowptr[u + 1] - rowptr[u] + in_ptr[u + 1] - in_ptr[u];
-        const uint32_t dv = rowptr[v + 1] - rowptr[v] + in_ptr[v + 1] - in_ptr[v];
-        if (!(du != dv ? du < dv : u < v)) bad |= 16;
         const uint32_t p = in_ptr[v] + atomicAdd(&fill[v], 1u);
         in_src[p] = u;
         in_eid[p] = e;
     }
-    if (bad) atomicOr(err, (unsigned long long)bad);
 }
 
 // key[e] = (degree << 32) | id of the endpoint col[e], degree = out + in: the orientation order of graph.h:43-45.
+// Also checks that rule for the edge src[e] -> col[e] (flag 16 in *err when it points the wrong way); the owner's
+// degree is the same for a row's consecutive edges.
 __global__ void k_edge_keys(const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ col,
-                            const uint32_t* __restrict__ in_ptr, uint32_t m, unsigned long long* __restrict__ key) {
+                            const uint32_t* __restrict__ src, const uint32_t* __restrict__ in_ptr, uint32_t m,
+                            unsigned long long* __restrict__ key, unsigned long long* err) {
+    uint32_t bad = 0;
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
-        const uint32_t x = col[e];
+        const uint32_t x = col[e], u = src[e];
         const uint32_t deg = rowptr[x + 1] - rowptr[x] + in_ptr[x + 1] - in_ptr[x];
+        const uint32_t du = rowptr[u + 1] - rowptr[u] + in_ptr[u + 1] - in_ptr[u];
+        if (!(du != deg ? du < deg : u < x)) bad |= 16;
         key[e] = ((unsigned long long)deg << 32) | x;
     }
+    if (bad) atomicOr(err, (unsigned long long)bad);
 }
 
 constexpr int kOrderWarps = 4, kOrderStage = 1024;   // rows up to kOrderStage entries stage their keys in smem
@@ -615,14 +615,14 @@ static ga_status prepare_index(ga_graph* g) {
     }
     GA_TRY(scan_impl<uint32_t>(st, indeg, g->in_ptr, (uint64_t)n + 1, false));   // indeg[n] = 0 -> in_ptr[n] = m
     if (m) {
-        k_in_scatter<<<ge, 256, 0, st>>>(g->rowptr, g->col, g->src, g->in_ptr, m, fill, g->in_src, g->in_eid, err);
+        k_in_scatter<<<ge, 256, 0, st>>>(g->col, g->src, g->in_ptr, m, fill, g->in_src, g->in_eid);
         GA_CUDA(cudaGetLastError());
         // rows in (degree, id) order, from one 64-bit key per edge
         unsigned long long* key = nullptr;
         uint32_t* posk = nullptr;
         GA_CUDA(pool_malloc((void**)&key, (size_t)m * 8, st));
         GA_CUDA(pool_malloc((void**)&posk, (size_t)m * 4, st));
-        k_edge_keys<<<ge, 256, 0, st>>>(g->rowptr, g->col, g->in_ptr, m, key);
+        k_edge_keys<<<ge, 256, 0, st>>>(g->rowptr, g->col, g->src, g->in_ptr, m, key, err);
         uint32_t* listed = nullptr;   // rows longer than 8, then their count
         GA_CUDA(pool_malloc((void**)&listed, ((size_t)n + 1) * 4, st));
         GA_CUDA(cudaMemsetAsync(listed + n, 0, 4, st));
