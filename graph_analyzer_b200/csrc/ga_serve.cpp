@@ -63,7 +63,10 @@ struct Request {
 // triangle incidence lists): the sizes ga_graph.cu / ga_loops.cu allocate, with the item lists bounded generously.
 uint64_t estimate_bytes(const GraphEntry& e, ga_request_kind kind) {
     const uint64_t n = e.n, m = e.m;
-    uint64_t b = 4 * (n + 1) + 4 * (m + 4) + 4 * m + 4 * (n + 1) + 8 * m + 12 * (n + m / 64 + 1) + 1024;
+    // CSR, src, in-lists, the ordered rows (colk, origk, in_rng) and vertex places (vrank, colr), per-anchor work,
+    // work items
+    uint64_t b = 4 * (n + 1) + 4 * (m + 4) + 4 * m + 4 * (n + 1) + 8 * m;
+    b += 4 * (m + 4) + 4 * m + 8 * m + 4 * n + 4 * (m + 4) + 8 * (n + 1) + 12 * (n + m / 64 + 1) + 1024;
     if (kind != GA_REQ_TC) {
         const uint64_t T = e.triangles != UINT64_MAX ? e.triangles : e.tri_bound;
         b += 25 * n + 8 * (n + 3 * T / 1024 + 1) + 24 * T + 8 * (n + 1);
