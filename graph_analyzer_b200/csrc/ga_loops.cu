@@ -922,15 +922,26 @@ static ga_status ensure_loops(ga_graph* g) {
     return GA_OK;
 }
 
-void destroy_loops(ga_graph* g) {
-    ga_loops* L = g->loops;
-    if (!L) return;
+// Releases the captured loop graphs. A captured round holds the addresses of the buffers it was captured with, so
+// this runs whenever one of them is replaced (the next loop captures again). An executable graph still running is
+// freed by CUDA when it completes.
+static void drop_captured(ga_loops* L) {
     for (int k = 0; k < 2; k++) {
         if (L->exec[k]) cudaGraphExecDestroy(L->exec[k]);
         if (L->graph[k]) cudaGraphDestroy(L->graph[k]);
+        L->exec[k] = nullptr;
+        L->graph[k] = nullptr;
     }
     if (L->exec_seg) cudaGraphExecDestroy(L->exec_seg);
     if (L->graph_seg) cudaGraphDestroy(L->graph_seg);
+    L->exec_seg = nullptr;
+    L->graph_seg = nullptr;
+}
+
+void destroy_loops(ga_graph* g) {
+    ga_loops* L = g->loops;
+    if (!L) return;
+    drop_captured(L);
     delete L;   // device buffers belong to g->allocations
     g->loops = nullptr;
 }
@@ -993,6 +1004,9 @@ static ga_status build_lists(ga_graph* g, uint64_t T0) {
         return GA_OK;
     }
     if (ix) {
+        // a loop captured before (its update then enumerated: incidence_lists builds the lists later, for the
+        // densest-subgraph stages) points at the old item buffers
+        drop_captured(L);
         dfree(g, L->item_x); dfree(g, L->item_c);
         L->item_x = ix; L->item_c = ic; L->item_cap = need_items;
     }
